@@ -1,0 +1,362 @@
+"""Benchmark of the helical WFBP path on B200.
+
+One step = one full reconstruction (rebin -> filter -> backprojection ->
+thickening) of one synthetic scan of the `rows64` workload (888 channels x 64
+rows, 984 views/rotation, 10 rotations, 512 x 512 x 300 slices @ 1 mm),
+through the C ABI. Metric: contributing backprojection voxel-view updates per
+second over the whole step (whole job over all ranks), with s/volume beside
+it. Inputs (2.2 GB raw frames) are larger than L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp32|mixed] [--workload rows64|small]
+
+Under torchrun each rank reconstructs its own independently seeded scan
+(weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed vs FP32"
+UNIT = "voxel-view updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--workload", default="rows64")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-slices", type=int, default=1)
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(spec, raw_host_fn, n_slices=1):
+    """The reference's path on the host cores (the oracle's FP32 transcript,
+    all threads): rebin+filter of the view window one slice needs, and the
+    backprojection of n_slices slices at full resolution; scaled to the full
+    volume linearly in views and slices."""
+    import numpy as np
+    from freect_b200 import scans  # noqa: F401
+    from oracle import oracle as O
+    nthreads = os.cpu_count() or 1
+    O.set_threads(nthreads)
+    tube, table = spec.views()
+    cg, gp = O.configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    zn, zr = O.slice_locations(cg, rp)
+    mid = zn.size // 2
+    zs = zn[mid:mid + n_slices]
+    # views that pass the z cull for these slices, plus the rebin's view reach
+    sel = np.nonzero(np.abs(table - zs.mean()) <= cg.z_rot + 1.0)[0]
+    reach = int(math.ceil(0.5 * spec.nch * spec.dbeta / (2 * math.pi / spec.P))) + 2
+    v0 = max(0, sel[0] - reach)
+    v0 -= v0 % (spec.P // 2)  # keep half-turn alignment of theta~
+    v1 = min(spec.V, sel[-1] + reach + 1)
+    sub = scans.ScanSpec(**{**spec.__dict__})
+    sub.rotations = (v1 - v0) / spec.P
+    raw = raw_host_fn(v0, v1)
+    stube, stable = tube[v0:v1], table[v0:v1]
+    scg, sgp = O.configure_geometry(sub.meta(), stable)
+    scg.z_rot = cg.z_rot
+    sgp.z_rot_over_2_pi = gp.z_rot_over_2_pi
+    t0 = time.perf_counter()
+    taps = O.taps_fft_from_half(scg, O.taps_f64(scg, spec.window).astype(np.float32))
+    filt = O.rebin_filter_ref32(scg, raw, taps, q8=True)
+    t1 = time.perf_counter()
+    vn = O.backproject_ref32(scg, rp, sgp, filt, stube, stable, zs)
+    t2 = time.perf_counter()
+    # updates in the sample (FP64 oracle's count on the same views and slices)
+    _, n_sample = O.backproject_f64(scg, rp, filt.astype(np.float64), stube.astype(np.float64),
+                                    stable.astype(np.float64), zs.astype(np.float64))
+    t_rf_full = (t1 - t0) * spec.V / float(v1 - v0)
+    t_bp_full = (t2 - t1) * zn.size / float(zs.size)
+    return {"t_rf_sample": t1 - t0, "t_bp_sample": t2 - t1, "views": int(v1 - v0), "slices": int(zs.size),
+            "updates_sample": int(n_sample), "t_full_est": t_rf_full + t_bp_full, "cores": nthreads,
+            "bp_updates_per_s": n_sample / (t2 - t1)}
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's path on host cores, bounded sample per step."""
+    import numpy as np
+    from freect_b200 import scans
+    from oracle import oracle as O
+    spec = scans.WORKLOADS[args.workload]()
+    cache = {}
+
+    def raw_host(v0, v1):
+        if (v0, v1) not in cache:
+            sub = scans.ScanSpec(**{**spec.__dict__})
+            s = spec.synth()
+            s.n_readings = v1 - v0
+            s.angle0 = s.angle0 + v0 * s.dangle
+            s.z0 = s.z0 + v0 * s.dz
+            cache[(v0, v1)] = O.synth_project(s, spec.ellipsoids())
+        return cache[(v0, v1)]
+
+    full_updates = None
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(spec, raw_host, n_slices=args.cpu_slices)
+        if i >= args.warmup:
+            times.append(r)
+    est = sorted(t["t_full_est"] for t in times)[len(times) // 2]
+    # updates of the full volume: per-slice sample count x slices
+    tube, table = spec.views()
+    cg, _ = O.configure_geometry(spec.meta(), table)
+    zn, _ = O.slice_locations(cg, spec.recon_config())
+    full_updates = times[0]["updates_sample"] * zn.size / times[0]["slices"]
+    value = full_updates / est
+    sample = ("oracle FP32 transcript (q8 texture weights) on %d host threads: rebin+filter of %d of %d views and "
+              "backprojection of %d of %d native slices at %dx%d, scaled linearly to the full volume"
+              % (times[0]["cores"], times[0]["views"], spec.V, times[0]["slices"], zn.size, spec.nx, spec.ny))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": est * 1000.0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom)",
+            "config": {"workload": spec.name, "channels": spec.nch, "rows": spec.nr, "views": spec.V,
+                       "volume": [spec.n_slices, spec.ny, spec.nx], "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": times[0]["cores"], "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "s_per_volume": est}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    from freect_b200 import abi_types as T
+    from freect_b200 import scans, wfbp
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    spec = scans.WORKLOADS[args.workload](seed=rank)
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    prec = T.PRECISION_MIXED if args.precision == "mixed" else T.PRECISION_FP32
+    ext = wfbp.make_ext(precision=prec, filter_window=spec.window, tex_weights=1 if prec == T.PRECISION_FP32 else 0)
+    ctx = wfbp.Context(cg, rp, ext, device=local)
+    ctx.set_views(tube, table)
+    d = ctx.dims
+
+    raw = ctx.alloc("raw")
+    wfbp.synth_project(spec.synth(), spec.ellipsoids(), raw)
+    reb = ctx.alloc("rebinned")
+    filt = ctx.alloc("filtered")
+    scales = ctx.alloc("row_scales")
+    vn = ctx.alloc("native")
+    vol = ctx.alloc("volume")
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def step(count=None):
+        ctx.rebin(raw, reb)
+        ctx.filter(reb, filt, scales)
+        ctx.backproject(filt, vn, scales, update_count=count)
+        ctx.thicken(vn, vol)
+
+    step(cnt)  # counts the contributing updates once, outside the timed region
+    torch.cuda.synchronize()
+    updates = int(cnt.item())
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    ev = {k: [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)] for k in
+          ("s", "reb", "flt", "bp", "th")}
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    for i in range(args.steps):
+        ev["s"][i].record(stream)
+        ctx.rebin(raw, reb)
+        ev["reb"][i].record(stream)
+        ctx.filter(reb, filt, scales)
+        ev["flt"][i].record(stream)
+        ctx.backproject(filt, vn, scales)
+        ev["bp"][i].record(stream)
+        ctx.thicken(vn, vol)
+        ev["th"][i].record(stream)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = start.elapsed_time(stop)
+    stage = {"rebin": 0.0, "filter": 0.0, "backproject": 0.0, "thicken": 0.0}
+    for i in range(args.steps):
+        stage["rebin"] += ev["s"][i].elapsed_time(ev["reb"][i])
+        stage["filter"] += ev["reb"][i].elapsed_time(ev["flt"][i])
+        stage["backproject"] += ev["flt"][i].elapsed_time(ev["bp"][i])
+        stage["thicken"] += ev["bp"][i].elapsed_time(ev["th"][i])
+    stage = {k: v / args.steps for k, v in stage.items()}
+    ms = total_ms / args.steps
+    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
+    u_all = torch.tensor([float(updates)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u_all, op=dist.ReduceOp.SUM)
+    ms = float(t_max.item())
+    value = float(u_all.item()) / (ms / 1000.0)
+
+    # end to end through the public API with host buffers (pinned)
+    e2e = None
+    if not args.no_e2e:
+        raw_h = torch.empty(raw.shape, dtype=torch.float32, pin_memory=True)
+        raw_h.copy_(raw.cpu())
+        vol_h = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
+        ctx.run_host(raw_h, vol_h)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.run_host(raw_h, vol_h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.steps
+        te = torch.tensor([ems], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        ems = float(te.item())
+        e2e = {"value": float(u_all.item()) / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": int(d.raw_bytes), "d2h_bytes_per_step": int(d.volume_bytes)}
+
+    hbm, bf16, peak_src = load_peaks()
+    elem = 4 if prec == T.PRECISION_FP32 else 2
+    bp_bytes = updates * 4 * elem
+    achieved = bp_bytes / (stage["backproject"] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": "backproject", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_source": peak_src,
+                "algorithmic_bytes_per_update": 4 * elem,
+                "note": "4 bilinear taps per contributing update, read through L1/shared memory"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == T.PRECISION_FP32 else "f16-storage/f32-accumulate",
+            "data": "synthetic (seeded ellipsoid phantom, Poisson noise)",
+            "config": {"workload": spec.name, "channels": spec.nch, "rows": spec.nr, "views": spec.V,
+                       "volume": [d.n_slices_requested, d.ny, d.nx], "native_slices": d.n_slices_native,
+                       "precision": args.precision, "parallelism": "independent scan per GPU",
+                       "l2": "inputs larger than L2 (2.2 GB raw frames)"},
+            "s_per_volume": ms / 1000.0, "updates_per_volume": updates, "stage_ms": stage,
+            "roofline": roofline, "gpu_launches": 4 * args.steps, "e2e": e2e, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_baseline(spec, lambda v0, v1: raw[v0:v1].cpu().numpy(), n_slices=args.cpu_slices)
+            full = updates / cb["t_full_est"]
+            line["cpu_baseline"] = {
+                "value": full, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                "sample": "oracle FP32 transcript: rebin+filter of %d of %d views, backprojection of %d of %d native "
+                          "slices (%d updates) in %.1f s + %.1f s; scaled linearly to the full volume"
+                          % (cb["views"], spec.V, cb["slices"], d.n_slices_native, cb["updates_sample"],
+                             cb["t_rf_sample"], cb["t_bp_sample"]),
+                "s_per_volume_est": cb["t_full_est"]}
+        except Exception as ex:  # reported, not fatal
+            line["cpu_baseline"] = {"error": repr(ex)}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

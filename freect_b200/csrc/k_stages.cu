@@ -1,0 +1,244 @@
+// Rebin, FP32 Toeplitz filter, thickening and table kernels (sm_100a).
+#include "wfbp_internal.h"
+
+#include <math.h>
+
+// ---------------------------------------------------------------------------
+// tables
+// ---------------------------------------------------------------------------
+
+// Per-view sin/cos of the tube angle, evaluated with the accurate sinf/cosf
+// the reference calls per voxel (cuda_kernels.cuh:235-238).
+__global__ void k_view_tables(const float* __restrict__ tube, const float* __restrict__ table,
+                              float2* __restrict__ sc, float* __restrict__ z, int V) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= V) return;
+  float th = tube[j];
+  sc[j] = make_float2(sinf(th), cosf(th));
+  z[j] = table[j];
+}
+
+cudaError_t launch_view_tables(const float* d_tube, const float* d_table, float2* d_sc, float* d_z, int V,
+                               cudaStream_t s) {
+  k_view_tables<<<(V + 255) / 256, 256, 0, s>>>(d_tube, d_table, d_sc, d_z, V);
+  return cudaGetLastError();
+}
+
+// Per-channel rebin geometry of rebin_kernel (cuda_kernels.cuh:17-22): the
+// fan angle beta of output channel c and the source channel index; NaN marks
+// channels the reference writes as zero (cuda_kernels.cuh:32-34).
+__global__ void k_rebin_tables(float* __restrict__ beta_t, float* __restrict__ bidx_t, int nch, float c0,
+                               float dcol, float sdd) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  float p = ((float)c - c0) * dcol;
+  float beta = asinf(p / sdd);
+  float bidx = (beta * sdd / dcol) + c0;
+  if (bidx < 0 || bidx >= (float)nch || isnan(bidx)) bidx = __int_as_float(0x7fc00000);
+  beta_t[c] = beta;
+  bidx_t[c] = bidx;
+}
+
+cudaError_t launch_rebin_tables(float* d_beta, float* d_bidx, int nch, float c0, float dcol, float sdd,
+                                cudaStream_t s) {
+  k_rebin_tables<<<(nch + 127) / 128, 128, 0, s>>>(d_beta, d_bidx, nch, c0, dcol, sdd);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// rebin
+// ---------------------------------------------------------------------------
+//
+// One output sample (v, i, c) of the reference's rebin of row sheet i
+// (cuda_kernels.cuh:11-39) read straight from the raw [reading][row][channel]
+// frames: the host reshape of ReconstructionMachine.cu:153-162 is folded into
+// the index math (sheet row i <- raw row nr-1-i, sheet column b <- raw
+// channel nch-1-b). The bilinear sample follows the texture unit's linear
+// filter with clamp addressing and texel centres at +0.5 (RM.cu:176-180).
+__device__ __forceinline__ float rebin_sample(const float* __restrict__ rawrow, size_t view_stride, int V,
+                                              int nch, float bidx, float beta, int v, float dth, int q8) {
+  if (isnan(bidx)) return 0.0f;
+  float theta = (float)v * dth;
+  float alpha = theta - beta;
+  float aidx = alpha / dth;
+  float xb = (bidx + 0.5f) - 0.5f;
+  float yb = (aidx + 0.5f) - 0.5f;
+  float fx = floorf(xb), fy = floorf(yb);
+  float ax = xb - fx, ay = yb - fy;
+  if (q8) {
+    ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
+    ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
+  }
+  int x0 = (int)fx, y0 = (int)fy;
+  int x1 = min(max(x0 + 1, 0), nch - 1), y1 = min(max(y0 + 1, 0), V - 1);
+  x0 = min(max(x0, 0), nch - 1);
+  y0 = min(max(y0, 0), V - 1);
+  const float* r0 = rawrow + (size_t)y0 * view_stride;
+  const float* r1 = rawrow + (size_t)y1 * view_stride;
+  float t00 = __ldg(r0 + (nch - 1 - x0)), t10 = __ldg(r0 + (nch - 1 - x1));
+  float t01 = __ldg(r1 + (nch - 1 - x0)), t11 = __ldg(r1 + (nch - 1 - x1));
+  return (1.0f - ax) * (1.0f - ay) * t00 + ax * (1.0f - ay) * t10 + (1.0f - ax) * ay * t01 + ax * ay * t11;
+}
+
+// grid.x covers [V*nr] output rows (REB_ROWS per block), grid.y covers
+// channel quads; each thread writes 4 consecutive channels with one float4.
+constexpr int REB_ROWS = 4;
+constexpr int REB_QUADS = 64;
+
+__global__ void __launch_bounds__(REB_ROWS * REB_QUADS)
+k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float* __restrict__ beta_t,
+            const float* __restrict__ bidx_t, RebinParams p) {
+  __shared__ float s_beta[REB_QUADS * 4], s_bidx[REB_QUADS * 4];
+  const int tq = threadIdx.x % REB_QUADS, tr = threadIdx.x / REB_QUADS;
+  const int c_base = blockIdx.y * REB_QUADS * 4;
+  for (int t = threadIdx.x; t < REB_QUADS * 4; t += blockDim.x) {
+    int c = c_base + t;
+    s_beta[t] = c < p.nch ? beta_t[c] : 0.0f;
+    s_bidx[t] = c < p.nch ? bidx_t[c] : __int_as_float(0x7fc00000);
+  }
+  __syncthreads();
+  const long row = (long)blockIdx.x * REB_ROWS + tr;
+  if (row >= (long)p.V * p.nr) return;
+  const int v = (int)(row / p.nr), i = (int)(row % p.nr);
+  const float* rawrow = raw + (size_t)(p.nr - 1 - i) * p.nch;
+  const size_t vs = (size_t)p.nr * p.nch;
+  const int c = c_base + tq * 4;
+  float* o = out + (size_t)row * p.nch;
+  if (c + 3 < p.nch && (p.nch & 3) == 0) {
+    float4 r;
+    r.x = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 0], s_beta[tq * 4 + 0], v, p.dth, p.q8);
+    r.y = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 1], s_beta[tq * 4 + 1], v, p.dth, p.q8);
+    r.z = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 2], s_beta[tq * 4 + 2], v, p.dth, p.q8);
+    r.w = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 3], s_beta[tq * 4 + 3], v, p.dth, p.q8);
+    *reinterpret_cast<float4*>(o + c) = r;
+  } else {
+    for (int u = 0; u < 4; u++)
+      if (c + u < p.nch)
+        o[c + u] = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + u], s_beta[tq * 4 + u], v, p.dth, p.q8);
+  }
+}
+
+cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, const float* d_bidx,
+                             const RebinParams& p, cudaStream_t s) {
+  long rows = (long)p.V * p.nr;
+  dim3 grid((unsigned)((rows + REB_ROWS - 1) / REB_ROWS), (unsigned)((p.nch + REB_QUADS * 4 - 1) / (REB_QUADS * 4)));
+  k_rebin_f32<<<grid, REB_ROWS * REB_QUADS, 0, s>>>(raw, out, d_beta, d_bidx, p);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FP32 Toeplitz filter
+// ---------------------------------------------------------------------------
+//
+// The reference filters each zero-padded row with cuFFT (R2C, multiply by the
+// spectrum of the fftshifted taps and 1/N, C2R; ReconstructionMachine.cu:
+// 206-290, cuda_kernels.cuh:41-58). Because the zero padding is at least
+// nch-1 on each side, the data window of that circular convolution equals the
+// linear convolution y[n] = sum_k h[|n-k|] x[k] over the nch channels: a
+// [rows x nch] x [nch x nch] product with a symmetric Toeplitz matrix. This
+// kernel evaluates it in FP32 on the CUDA cores: 128x128 output tiles, 8x8
+// per thread, the Toeplitz operand read from a shared-memory tap line
+// htab[d + NTAB] = h[|d|] so the inner loop needs no index arithmetic.
+constexpr int TF_BM = 128, TF_BN = 128, TF_BK = 16;
+
+__global__ void __launch_bounds__(256)
+k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* __restrict__ taps, long M,
+               int nch) {
+  extern __shared__ float smem[];
+  float* As = smem;                          // [TF_BK][TF_BM + 4]
+  float* htab = smem + TF_BK * (TF_BM + 4);  // [2*nch + 1], htab[d + nch] = h[|d|]
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const long m0 = (long)blockIdx.x * TF_BM;
+  const int n0 = blockIdx.y * TF_BN;
+  for (int d = tid; d < 2 * nch + 1; d += 256) {
+    int a = d - nch;
+    a = a < 0 ? -a : a;
+    htab[d] = a < nch ? taps[a] : 0.0f;
+  }
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+
+  // column n_j = n0 + tx + 16 j; output columns >= nch are discarded
+  for (int k0 = 0; k0 < nch; k0 += TF_BK) {
+    __syncthreads();
+    // A tile: 128 rows x 16 k, stored k-major
+    for (int e = tid; e < TF_BM * TF_BK; e += 256) {
+      int mm = e / TF_BK, kk = e % TF_BK;
+      long m = m0 + mm;
+      int k = k0 + kk;
+      As[kk * (TF_BM + 4) + mm] = (m < M && k < nch) ? X[m * nch + k] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TF_BK; kk++) {
+      float a[8], b[8];
+      float4 a0 = *reinterpret_cast<const float4*>(&As[kk * (TF_BM + 4) + ty * 8]);
+      float4 a1 = *reinterpret_cast<const float4*>(&As[kk * (TF_BM + 4) + ty * 8 + 4]);
+      a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
+      a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
+      const int k = k0 + kk;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        int d = n0 + tx + 16 * j - k;  // in (-nch, nch + 128)
+        d = d > nch ? nch : d;         // columns beyond nch read h=0 slot
+        b[j] = htab[d + nch];
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    long m = m0 + ty * 8 + i;
+    if (m >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      int n = n0 + tx + 16 * j;
+      if (n < nch) Y[m * nch + n] = acc[i][j];
+    }
+  }
+}
+
+cudaError_t launch_filter_f32(const float* x, float* y, const float* d_taps, long rows, int nch, cudaStream_t s) {
+  size_t smem = sizeof(float) * (TF_BK * (TF_BM + 4) + 2 * nch + 1);
+  if (smem > 64 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_toeplitz_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((rows + TF_BM - 1) / TF_BM), (unsigned)((nch + TF_BN - 1) / TF_BN));
+  k_toeplitz_f32<<<grid, 256, smem, s>>>(x, y, d_taps, rows, nch);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// thickening
+// ---------------------------------------------------------------------------
+//
+// thicken_slices (cuda_kernels.cuh:289-320): output slice r is the
+// triangle-weighted mean of the native slices with nonzero weight
+// max(0, 1 - |z_n - z_r| / slice_thickness). The weights and their list per
+// output slice are computed on the host in the reference's float arithmetic;
+// the per-voxel sums run in the same slice order.
+__global__ void k_thicken(const float* __restrict__ vn, float* __restrict__ out, const int* __restrict__ off,
+                          const int* __restrict__ idx, const float* __restrict__ w, const float* __restrict__ ws,
+                          int nxy) {
+  const int r = blockIdx.y;
+  const int px = blockIdx.x * blockDim.x + threadIdx.x;
+  if (px >= nxy) return;
+  const int a = off[r], b = off[r + 1];
+  float val = 0.0f;
+  for (int t = a; t < b; t++) val = fmaf(w[t], __ldg(vn + (size_t)idx[t] * nxy + px), val);
+  out[(size_t)r * nxy + px] = val / ws[r];
+}
+
+cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
+                           const float* ws, int nxy, int nzr, cudaStream_t s) {
+  dim3 grid((unsigned)((nxy + 255) / 256), (unsigned)nzr);
+  k_thicken<<<grid, 256, 0, s>>>(vn, out, off, idx, w, ws, nxy);
+  return cudaGetLastError();
+}

@@ -1,0 +1,548 @@
+// Host side of the B200 WFBP library: the C ABI of include/freect_wfbp.h.
+//
+// What the reference does in ReconstructionMachine (applications/fct_wfbp/src/
+// ReconstructionMachine.cu) is split here into a context (geometry, slice
+// lists, filter taps, per-view tables, thickening weights) and four
+// asynchronous stages on a caller-chosen stream. Errors come back as status
+// codes with a message in the context instead of exit().
+#include "wfbp_internal.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+
+#define WFBP_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+int fail(wfbp_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      return fail((ctx), e_ == cudaErrorMemoryAllocation ? WFBP_ERR_OOM : WFBP_ERR_CUDA,      \
+                  std::string(#call) + ": " + cudaGetErrorName(e_) + " " + cudaGetErrorString(e_)); \
+    }                                                                                        \
+  } while (0)
+
+size_t next_pow2_at_least(size_t n) {
+  size_t p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// r(t) of generate_filter (ReconstructionMachine.cu:493-498): sin and cos of
+// the float argument in double precision, result stored as float.
+float ramp_r(float t) {
+  float v = (float)(sin((double)t) / (double)t + (cos((double)t) - 1.0f) / (double)(t * t));
+  if (t == 0) v = 0.5f;
+  return v;
+}
+
+int slice_lists(const CTGeometry* cg, const ReconConfig* rp, std::vector<float>& native, std::vector<float>& req) {
+  native.clear();
+  req.clear();
+  const size_t cap = 1u << 22;
+  if (rp->start_pos != rp->end_pos) {
+    float span = rp->end_pos - rp->start_pos;
+    float d_native = cg->collimated_slice_width * fabsf(span) / span;
+    float d_req = rp->slice_pitch * fabsf(span) / span;
+    if (!(fabsf(d_native) > 0) || !(fabsf(d_req) > 0)) return WFBP_ERR_INVALID_ARG;
+    if (d_req > 0) {
+      for (float loc = rp->start_pos; loc < rp->end_pos; loc += d_native) {
+        native.push_back(loc);
+        if (native.size() > cap) return WFBP_ERR_INVALID_ARG;
+      }
+      for (float loc = rp->start_pos; loc < rp->end_pos; loc += d_req) {
+        req.push_back(loc);
+        if (req.size() > cap) return WFBP_ERR_INVALID_ARG;
+      }
+    } else {
+      for (float loc = rp->start_pos; loc > rp->end_pos; loc += d_native) {
+        native.push_back(loc);
+        if (native.size() > cap) return WFBP_ERR_INVALID_ARG;
+      }
+      for (float loc = rp->start_pos; loc > rp->end_pos; loc += d_req) {
+        req.push_back(loc);
+        if (req.size() > cap) return WFBP_ERR_INVALID_ARG;
+      }
+    }
+  } else {
+    native.push_back(rp->start_pos);
+    req.push_back(rp->start_pos);
+  }
+  return WFBP_OK;
+}
+
+int make_taps(const CTGeometry* cg, int window, float c, float a, const float* user, int n_user, float* taps, int n) {
+  const float ds = cg->detector_pixel_size_col * cg->distance_source_to_isocenter / cg->distance_source_to_detector;
+  if (!(ds > 0)) return WFBP_ERR_INVALID_ARG;
+  if (window == WFBP_FILTER_REFERENCE) {
+    const float pi_f = 3.141592653589f;  // ReconstructionMachine.cu:490
+    for (int i = 0; i < n; i++)
+      taps[i] = (c * c / (2.0f * ds)) * (a * ramp_r(c * pi_f * i) + (((1.0f - a) / 2.0f) * ramp_r(pi_f * c * i + pi_f)) +
+                                         (((1.0f - a) / 2.0f) * ramp_r(pi_f * c * i - pi_f)));
+  } else if (window == WFBP_FILTER_SHEPP_LOGAN) {
+    for (int i = 0; i < n; i++) taps[i] = (float)(-2.0 / (M_PI * M_PI * (double)ds * (4.0 * i * (double)i - 1.0)));
+  } else if (window == WFBP_FILTER_USER) {
+    if (!user || n_user < 1) return WFBP_ERR_INVALID_ARG;
+    for (int i = 0; i < n; i++) taps[i] = i < n_user ? user[i] : 0.0f;
+  } else {
+    return WFBP_ERR_INVALID_ARG;
+  }
+  return WFBP_OK;
+}
+
+void free_dev(void*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+template <class T>
+void free_dev(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void release(wfbp_ctx* ctx) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->device);
+  free_dev(ctx->d_taps);
+  free_dev(ctx->d_chan_beta);
+  free_dev(ctx->d_chan_bidx);
+  free_dev(ctx->d_view_sc);
+  free_dev(ctx->d_view_z);
+  free_dev(ctx->d_z_native);
+  free_dev(ctx->d_thick_off);
+  free_dev(ctx->d_thick_idx);
+  free_dev(ctx->d_thick_w);
+  free_dev(ctx->d_thick_ws);
+  free_dev(ctx->s_rebinned);
+  free_dev(ctx->s_filtered);
+  free_dev(ctx->s_scales);
+  free_dev(ctx->s_vol_native);
+  free_dev(ctx->s_raw);
+  free_dev(ctx->s_vol);
+  cudaSetDevice(prev);
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+BPParams bp_params(const wfbp_ctx* ctx) {
+  BPParams p;
+  p.nx = ctx->nx; p.ny = ctx->ny; p.nz = ctx->nz;
+  p.nch = ctx->nch; p.nr = ctx->nr; p.V = ctx->V;
+  p.P2 = ctx->gp.projections_per_half_turn;
+  p.K = ctx->gp.n_half_turns;
+  p.fov = ctx->rp.recon_fov; p.x0 = ctx->rp.x_origin; p.y0 = ctx->rp.y_origin;
+  p.fov_half2 = ctx->gp.half_acquisition_fov_squared;
+  p.z_rot = ctx->cg.z_rot;
+  p.R2 = ctx->gp.distance_source_to_isocenter_squared;
+  p.rR = ctx->gp.recip_distance_source_to_isocenter;
+  p.zr2pi = ctx->gp.z_rot_over_2_pi;
+  p.tanc = ctx->gp.tanf_theta_cone;
+  p.ps = ctx->gp.pixel_scale;
+  p.c0 = ctx->cg.detector_central_col;
+  p.kp = (float)((double)ctx->nch + 1.75);
+  p.hn = 0.5f * ((float)ctx->nr - 1.0f);
+  p.nrm2 = (float)(ctx->nr - 2);
+  p.ncm2 = (float)(ctx->nch - 2);
+  p.dtheta = ctx->gp.two_pi_over_projections_per_rotation;
+  return p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// geometry
+// ---------------------------------------------------------------------------
+
+WFBP_API int wfbp_configure_geometry(const wfbp_scan_meta* m, const float* table, CTGeometry* cg, GPUPrecompute* gp) {
+  if (!m || !table || !cg || !gp) return WFBP_ERR_INVALID_ARG;
+  if (m->projections_per_rotation < 2 || m->total_num_projections <= m->projections_per_rotation ||
+      m->detector_channels < 4 || m->detector_rows < 2 || !(m->dist_source_to_detector > 0) ||
+      !(m->dist_source_to_isocenter > 0) || !(m->detector_transverse_spacing > 0) ||
+      !(m->detector_axial_spacing > 0))
+    return WFBP_ERR_INVALID_ARG;
+  memset(cg, 0, sizeof(*cg));
+  memset(gp, 0, sizeof(*gp));
+  // ReconstructionMachine.cu:48-69
+  cg->total_number_of_projections = (size_t)m->total_num_projections;
+  cg->projections_per_rotation = (size_t)m->projections_per_rotation;
+  cg->detector_pixel_size_col = m->detector_transverse_spacing;
+  cg->detector_pixel_size_row = m->detector_axial_spacing;
+  cg->num_detector_cols = (size_t)m->detector_channels;
+  cg->num_detector_cols_padded = 2 * (size_t)m->detector_channels;
+  cg->num_detector_cols_padded_fft = next_pow2_at_least(2 * (size_t)m->detector_channels);
+  cg->num_detector_rows = (size_t)m->detector_rows;
+  cg->num_detector_rows_padded = 2 * (size_t)m->detector_rows;
+  cg->detector_central_col = m->detector_central_channel;
+  cg->detector_central_row = m->detector_central_row;
+  cg->distance_source_to_isocenter = m->dist_source_to_isocenter;
+  cg->distance_source_to_detector = m->dist_source_to_detector;
+  cg->collimated_slice_width = m->dist_source_to_isocenter * (m->detector_axial_spacing / m->dist_source_to_detector);
+  cg->z_rot = fabsf(table[m->projections_per_rotation] - table[0]);
+  float cone_offset = ((float)(cg->num_detector_rows - 1)) / 2.0f;
+  cg->theta_cone = 2.0f * (float)atan((double)(cone_offset * cg->collimated_slice_width / cg->distance_source_to_isocenter));
+  cg->acquisition_field_of_view =
+      2.0f * cg->distance_source_to_isocenter *
+      (float)sin((double)((((float)cg->num_detector_cols - 1.0f) / 2.0f) * m->detector_transverse_spacing *
+                          (1.0f / cg->distance_source_to_detector)));
+  cg->anode_angle = m->anode_angle;
+  cg->ffs_phi = (m->ffs_mode & WFBP_FFS_PHI) != 0;
+  cg->ffs_z = (m->ffs_mode & WFBP_FFS_Z) != 0;
+  cg->ffs_diag = false;
+  // recon_structs.h:69-83
+  const float pi_f = 3.1415926535897f;
+  gp->half_acquisition_fov = 0.5f * cg->acquisition_field_of_view;
+  gp->half_acquisition_fov_squared = gp->half_acquisition_fov * gp->half_acquisition_fov;
+  gp->projections_per_half_turn = (int)(cg->projections_per_rotation / 2);
+  gp->n_half_turns = (int)(cg->total_number_of_projections / (size_t)gp->projections_per_half_turn);
+  gp->distance_source_to_isocenter_squared = cg->distance_source_to_isocenter * cg->distance_source_to_isocenter;
+  gp->z_rot_over_2_pi = cg->z_rot / (2.0f * pi_f);
+  gp->recip_distance_source_to_detector = 1.0f / cg->distance_source_to_detector;
+  gp->recip_distance_source_to_isocenter = 1.0f / cg->distance_source_to_isocenter;
+  gp->tanf_theta_cone = (float)tan((double)(cg->theta_cone / 2.0f));
+  gp->pixel_scale = cg->distance_source_to_detector / (cg->distance_source_to_isocenter * cg->detector_pixel_size_col);
+  gp->two_pi_over_projections_per_rotation = 2.0f * pi_f / (float)cg->projections_per_rotation;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_slice_locations(const CTGeometry* cg, const ReconConfig* rp, float* native_z, int native_cap,
+                                  int* n_native, float* requested_z, int requested_cap, int* n_requested) {
+  if (!cg || !rp) return WFBP_ERR_INVALID_ARG;
+  std::vector<float> nat, req;
+  int st = slice_lists(cg, rp, nat, req);
+  if (st) return st;
+  if (n_native) *n_native = (int)nat.size();
+  if (n_requested) *n_requested = (int)req.size();
+  if (native_z) std::copy(nat.begin(), nat.begin() + std::min<size_t>(nat.size(), (size_t)std::max(native_cap, 0)), native_z);
+  if (requested_z)
+    std::copy(req.begin(), req.begin() + std::min<size_t>(req.size(), (size_t)std::max(requested_cap, 0)), requested_z);
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_filter_taps(const CTGeometry* cg, int window, float c, float a, float* taps, int n) {
+  if (!cg || !taps || n < 1) return WFBP_ERR_INVALID_ARG;
+  return make_taps(cg, window, c, a, nullptr, 0, taps, n);
+}
+
+WFBP_API const char* wfbp_status_string(int status) {
+  switch (status) {
+    case WFBP_OK: return "WFBP_OK";
+    case WFBP_ERR_INVALID_ARG: return "WFBP_ERR_INVALID_ARG";
+    case WFBP_ERR_OOM: return "WFBP_ERR_OOM";
+    case WFBP_ERR_CUDA: return "WFBP_ERR_CUDA";
+    case WFBP_ERR_TIMEOUT: return "WFBP_ERR_TIMEOUT";
+    case WFBP_ERR_UNSUPPORTED: return "WFBP_ERR_UNSUPPORTED";
+    case WFBP_ERR_STATE: return "WFBP_ERR_STATE";
+  }
+  return "WFBP_ERR_UNKNOWN";
+}
+
+WFBP_API const char* wfbp_last_error(const wfbp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const wfbp_ext* ext, int device,
+                             wfbp_ctx** out) {
+  if (!cg || !rp || !out) return WFBP_ERR_INVALID_ARG;
+  *out = nullptr;
+  wfbp_ext e;
+  memset(&e, 0, sizeof(e));
+  e.version = WFBP_EXT_VERSION;
+  e.precision = WFBP_PRECISION_FP32;
+  e.filter_window = WFBP_FILTER_REFERENCE;
+  e.filter_c = 1.0f;
+  e.filter_a = 1.0f;
+  if (ext) {
+    if (ext->version != WFBP_EXT_VERSION) return WFBP_ERR_INVALID_ARG;
+    e = *ext;
+  }
+  if (e.precision != WFBP_PRECISION_FP32) return WFBP_ERR_UNSUPPORTED;
+  if (cg->ffs_phi || cg->ffs_z || cg->ffs_diag) return WFBP_ERR_UNSUPPORTED;
+  if (cg->projections_per_rotation < 2 || cg->total_number_of_projections <= cg->projections_per_rotation / 2 ||
+      cg->num_detector_cols < 4 || cg->num_detector_rows < 2 || rp->nx < 1 || rp->ny < 1 ||
+      !(rp->recon_fov > 0) || !(rp->slice_thickness > 0) || !(cg->distance_source_to_isocenter > 0) ||
+      !(cg->distance_source_to_detector > 0) || !(cg->detector_pixel_size_col > 0) ||
+      !(cg->collimated_slice_width > 0) || cg->num_detector_cols > 8192 || cg->num_detector_rows > 1024 ||
+      cg->total_number_of_projections > (1u << 24) || rp->nx > 8192 || rp->ny > 8192)
+    return WFBP_ERR_INVALID_ARG;
+
+  wfbp_ctx* ctx = new (std::nothrow) wfbp_ctx();
+  if (!ctx) return WFBP_ERR_OOM;
+  ctx->cg = *cg;
+  ctx->rp = *rp;
+  ctx->ext = e;
+  ctx->device = device;
+  ctx->V = (int)cg->total_number_of_projections;
+  ctx->nr = (int)cg->num_detector_rows;
+  ctx->nch = (int)cg->num_detector_cols;
+  ctx->P = (int)cg->projections_per_rotation;
+  ctx->n_readings = ctx->V;
+  ctx->raw_rows = ctx->nr;
+  ctx->raw_ch = ctx->nch;
+  ctx->nx = (int)rp->nx;
+  ctx->ny = (int)rp->ny;
+
+  // derived constants (recon_structs.h:69-83) from the given geometry
+  const float pi_f = 3.1415926535897f;
+  GPUPrecompute& gp = ctx->gp;
+  memset(&gp, 0, sizeof(gp));
+  gp.half_acquisition_fov = 0.5f * cg->acquisition_field_of_view;
+  gp.half_acquisition_fov_squared = gp.half_acquisition_fov * gp.half_acquisition_fov;
+  gp.projections_per_half_turn = (int)(cg->projections_per_rotation / 2);
+  gp.n_half_turns = (int)(cg->total_number_of_projections / (size_t)gp.projections_per_half_turn);
+  gp.distance_source_to_isocenter_squared = cg->distance_source_to_isocenter * cg->distance_source_to_isocenter;
+  gp.z_rot_over_2_pi = cg->z_rot / (2.0f * pi_f);
+  gp.recip_distance_source_to_detector = 1.0f / cg->distance_source_to_detector;
+  gp.recip_distance_source_to_isocenter = 1.0f / cg->distance_source_to_isocenter;
+  gp.tanf_theta_cone = (float)tan((double)(cg->theta_cone / 2.0f));
+  gp.pixel_scale = cg->distance_source_to_detector / (cg->distance_source_to_isocenter * cg->detector_pixel_size_col);
+  gp.two_pi_over_projections_per_rotation = 2.0f * pi_f / (float)cg->projections_per_rotation;
+  ctx->P2 = gp.projections_per_half_turn;
+  ctx->K = gp.n_half_turns;
+
+  int st = slice_lists(cg, rp, ctx->z_native, ctx->z_req);
+  if (st) { delete ctx; return st; }
+  ctx->nz = (int)ctx->z_native.size();
+  ctx->nzr = (int)ctx->z_req.size();
+  gp.n_slices_native = ctx->nz;
+  gp.n_slices_requested = ctx->nzr;
+
+  ctx->taps.resize(ctx->nch);
+  st = make_taps(cg, e.filter_window, e.filter_c, e.filter_a, e.user_taps, e.n_user_taps, ctx->taps.data(), ctx->nch);
+  if (st) { delete ctx; return st; }
+
+  // thickening weights (cuda_kernels.cuh:303-317), float arithmetic
+  ctx->thick_off.assign(ctx->nzr + 1, 0);
+  std::vector<float> ws(ctx->nzr, 0.0f);
+  for (int r = 0; r < ctx->nzr; r++) {
+    ctx->thick_off[r] = (int)ctx->thick_idx.size();
+    float wsum = 0.0f;
+    for (int i = 0; i < ctx->nz; i++) {
+      float w = fmaxf(0.0f, 1.0f - fabsf(ctx->z_native[i] - ctx->z_req[r]) / rp->slice_thickness);
+      if (w == 0.0f) continue;
+      wsum += w;
+      ctx->thick_idx.push_back(i);
+      ctx->thick_w.push_back(w);
+    }
+    ws[r] = wsum;
+  }
+  ctx->thick_off[ctx->nzr] = (int)ctx->thick_idx.size();
+
+  DeviceGuard g(device);
+  auto alloc_copy = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
+    cudaError_t e1 = cudaMalloc(dst, bytes > 0 ? bytes : 4);
+    if (e1 != cudaSuccess) return e1;
+    if (src && bytes) return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    return cudaSuccess;
+  };
+  cudaError_t ce = cudaSuccess;
+  if (!ce) ce = alloc_copy((void**)&ctx->d_taps, ctx->taps.data(), sizeof(float) * ctx->nch);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_chan_beta, nullptr, sizeof(float) * ctx->nch);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_chan_bidx, nullptr, sizeof(float) * ctx->nch);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_view_sc, nullptr, sizeof(float2) * ctx->V);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_view_z, nullptr, sizeof(float) * ctx->V);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_z_native, ctx->z_native.data(), sizeof(float) * ctx->nz);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_off, ctx->thick_off.data(), sizeof(int) * ctx->thick_off.size());
+  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_idx, ctx->thick_idx.data(), sizeof(int) * ctx->thick_idx.size());
+  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_w, ctx->thick_w.data(), sizeof(float) * ctx->thick_w.size());
+  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_ws, ws.data(), sizeof(float) * ws.size());
+  if (!ce) ce = launch_rebin_tables(ctx->d_chan_beta, ctx->d_chan_bidx, ctx->nch, cg->detector_central_col,
+                                    cg->detector_pixel_size_col, cg->distance_source_to_detector, 0);
+  if (!ce) ce = cudaDeviceSynchronize();
+  if (ce) {
+    int code = ce == cudaErrorMemoryAllocation ? WFBP_ERR_OOM : WFBP_ERR_CUDA;
+    release(ctx);
+    delete ctx;
+    return code;
+  }
+  *out = ctx;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_ctx_destroy(wfbp_ctx* ctx) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  release(ctx);
+  delete ctx;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_query(const wfbp_ctx* ctx, wfbp_dims* d) {
+  if (!ctx || !d) return WFBP_ERR_INVALID_ARG;
+  memset(d, 0, sizeof(*d));
+  d->n_views = ctx->V;
+  d->n_rows = ctx->nr;
+  d->n_channels = ctx->nch;
+  d->n_readings = ctx->n_readings;
+  d->raw_rows = ctx->raw_rows;
+  d->raw_channels = ctx->raw_ch;
+  d->nx = ctx->nx;
+  d->ny = ctx->ny;
+  d->n_slices_native = ctx->nz;
+  d->n_slices_requested = ctx->nzr;
+  d->precision = ctx->ext.precision;
+  const size_t samples = (size_t)ctx->V * ctx->nr * ctx->nch;
+  d->raw_bytes = sizeof(float) * (size_t)ctx->n_readings * ctx->raw_rows * ctx->raw_ch;
+  d->rebinned_bytes = sizeof(float) * samples;
+  d->filtered_bytes = sizeof(float) * samples;
+  d->row_scale_bytes = 0;
+  d->native_volume_bytes = sizeof(float) * (size_t)ctx->nz * ctx->nx * ctx->ny;
+  d->volume_bytes = sizeof(float) * (size_t)ctx->nzr * ctx->nx * ctx->ny;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!tube || !table) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_views: null array");
+  for (int j = 0; j < ctx->n_readings; j++)
+    if (!isfinite(tube[j]) || !isfinite(table[j]))
+      return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_views: non-finite angle or table position at reading " +
+                                                 std::to_string(j));
+  DeviceGuard g(ctx->device);
+  float *d_t = nullptr, *d_z = nullptr;
+  CUDA_TRY(ctx, cudaMalloc(&d_t, sizeof(float) * ctx->V));
+  cudaError_t e = cudaMalloc(&d_z, sizeof(float) * ctx->V);
+  if (!e) e = cudaMemcpy(d_t, tube, sizeof(float) * ctx->V, cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy(d_z, table, sizeof(float) * ctx->V, cudaMemcpyHostToDevice);
+  if (!e) e = launch_view_tables(d_t, d_z, ctx->d_view_sc, ctx->d_view_z, ctx->V, 0);
+  if (!e) e = cudaDeviceSynchronize();
+  cudaFree(d_t);
+  cudaFree(d_z);
+  CUDA_TRY(ctx, e);
+  ctx->views_set = true;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* requested_z) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (native_z) std::copy(ctx->z_native.begin(), ctx->z_native.end(), native_z);
+  if (requested_z) std::copy(ctx->z_req.begin(), ctx->z_req.end(), requested_z);
+  return WFBP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stages
+// ---------------------------------------------------------------------------
+
+WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw || !rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin: null buffer");
+  DeviceGuard g(ctx->device);
+  RebinParams p;
+  p.V = ctx->V;
+  p.nr = ctx->nr;
+  p.nch = ctx->nch;
+  p.dth = 2.0f * 3.14159265f / (float)ctx->P;  // cuda_kernels.cuh:15
+  p.q8 = ctx->ext.tex_weights ? 1 : 0;
+  CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* row_scales, void* stream) {
+  (void)row_scales;
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!rebinned || !filtered) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: null buffer");
+  DeviceGuard g(ctx->device);
+  CUDA_TRY(ctx, launch_filter_f32((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
+                                  ctx->nch, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_backproject(wfbp_ctx* ctx, const void* filtered, const float* row_scales, float* vol,
+                              unsigned long long* update_count, void* stream) {
+  (void)row_scales;
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!filtered || !vol) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject: null buffer");
+  if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_backproject: wfbp_set_views not called");
+  DeviceGuard g(ctx->device);
+  BPParams p = bp_params(ctx);
+  CUDA_TRY(ctx, launch_backproject_f32((const float*)filtered, vol, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p,
+                                       update_count, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_thicken(wfbp_ctx* ctx, const float* vn, float* vol, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!vn || !vol) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_thicken: null buffer");
+  DeviceGuard g(ctx->device);
+  CUDA_TRY(ctx, launch_thicken(vn, vol, ctx->d_thick_off, ctx->d_thick_idx, ctx->d_thick_w, ctx->d_thick_ws,
+                               ctx->nx * ctx->ny, ctx->nzr, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+namespace {
+int ensure_scratch(wfbp_ctx* ctx) {
+  wfbp_dims d;
+  wfbp_query(ctx, &d);
+  if (!ctx->s_rebinned) CUDA_TRY(ctx, cudaMalloc(&ctx->s_rebinned, d.rebinned_bytes));
+  if (!ctx->s_filtered) CUDA_TRY(ctx, cudaMalloc(&ctx->s_filtered, d.filtered_bytes));
+  if (!ctx->s_vol_native) CUDA_TRY(ctx, cudaMalloc(&ctx->s_vol_native, d.native_volume_bytes));
+  return WFBP_OK;
+}
+}  // namespace
+
+WFBP_API int wfbp_run(wfbp_ctx* ctx, const float* raw, float* vol, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw || !vol) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_run: null buffer");
+  if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_run: wfbp_set_views not called");
+  DeviceGuard g(ctx->device);
+  int st = ensure_scratch(ctx);
+  if (st) return st;
+  if ((st = wfbp_rebin(ctx, raw, ctx->s_rebinned, stream))) return st;
+  if ((st = wfbp_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, stream))) return st;
+  if ((st = wfbp_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, stream))) return st;
+  return wfbp_thicken(ctx, ctx->s_vol_native, vol, stream);
+}
+
+WFBP_API int wfbp_run_host(wfbp_ctx* ctx, const float* raw_host, float* vol_host, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw_host || !vol_host) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_run_host: null buffer");
+  DeviceGuard g(ctx->device);
+  wfbp_dims d;
+  wfbp_query(ctx, &d);
+  if (!ctx->s_raw) CUDA_TRY(ctx, cudaMalloc(&ctx->s_raw, d.raw_bytes));
+  if (!ctx->s_vol) CUDA_TRY(ctx, cudaMalloc(&ctx->s_vol, d.volume_bytes));
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->s_raw, raw_host, d.raw_bytes, cudaMemcpyHostToDevice, s));
+  int st = wfbp_run(ctx, ctx->s_raw, ctx->s_vol, stream);
+  if (st) return st;
+  CUDA_TRY(ctx, cudaMemcpyAsync(vol_host, ctx->s_vol, d.volume_bytes, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  return WFBP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// synthetic scans
+// ---------------------------------------------------------------------------
+
+WFBP_API int wfbp_synth_project(const wfbp_synth_scan* scan, const wfbp_ellipsoid* ellipsoids, int n, float* out,
+                                void* stream) {
+  if (!scan || !out || n < 0 || (n > 0 && !ellipsoids) || scan->n_readings < 1 || scan->rows < 1 ||
+      scan->channels < 1)
+    return WFBP_ERR_INVALID_ARG;
+  cudaError_t e = launch_synth(*scan, ellipsoids, n, out, (cudaStream_t)stream);
+  if (e != cudaSuccess) return e == cudaErrorInvalidValue ? WFBP_ERR_INVALID_ARG : WFBP_ERR_CUDA;
+  return WFBP_OK;
+}

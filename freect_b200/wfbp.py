@@ -1,0 +1,264 @@
+"""ctypes binding of the C ABI in include/freect_wfbp.h.
+
+The library is the compiled sm_100a code in freect_b200/lib/libfreect_wfbp.so;
+there is no fallback: if the library is missing or a call fails, an exception
+is raised. Device buffers are torch tensors (their data pointers are passed
+through the ABI) and every stage runs on torch's current CUDA stream unless a
+stream is given.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi_types as T
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libfreect_wfbp.so")
+_lib = None
+
+# name -> (restype, argtypes); the exported symbols of include/freect_wfbp.h
+_VP = C.c_void_p
+_PROTOS = {
+    "wfbp_configure_geometry": (C.c_int, [C.POINTER(T.ScanMeta), C.POINTER(C.c_float), C.POINTER(T.CTGeometry),
+                                          C.POINTER(T.GPUPrecompute)]),
+    "wfbp_slice_locations": (C.c_int, [C.POINTER(T.CTGeometry), C.POINTER(T.ReconConfig), C.POINTER(C.c_float),
+                                       C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int,
+                                       C.POINTER(C.c_int)]),
+    "wfbp_filter_taps": (C.c_int, [C.POINTER(T.CTGeometry), C.c_int, C.c_float, C.c_float, C.POINTER(C.c_float),
+                                   C.c_int]),
+    "wfbp_ctx_create": (C.c_int, [C.POINTER(T.CTGeometry), C.POINTER(T.ReconConfig), C.POINTER(T.Ext), C.c_int,
+                                  C.POINTER(_VP)]),
+    "wfbp_ctx_destroy": (C.c_int, [_VP]),
+    "wfbp_query": (C.c_int, [_VP, C.POINTER(T.Dims)]),
+    "wfbp_set_views": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "wfbp_get_slices": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "wfbp_last_error": (C.c_char_p, [_VP]),
+    "wfbp_status_string": (C.c_char_p, [C.c_int]),
+    "wfbp_rebin": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_filter": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "wfbp_backproject": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "wfbp_thicken": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_run": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_run_host": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_synth_project": (C.c_int, [C.POINTER(T.SynthScan), C.POINTER(T.Ellipsoid), C.c_int, _VP, _VP]),
+}
+
+
+class WfbpError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (T.STATUS_NAMES.get(status, status), msg))
+        self.status = status
+
+
+def lib_path():
+    return _LIB_PATH
+
+
+def load():
+    """Loads the compiled library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError("freect_b200: %s is missing; build it with `python -m freect_b200.build_lib`"
+                              % _LIB_PATH)
+        lib = C.CDLL(_LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return sorted(_PROTOS)
+
+
+def _check(status, what, ctx=None):
+    if status != 0:
+        msg = what
+        if ctx is not None:
+            m = load().wfbp_last_error(ctx)
+            if m:
+                msg += ": " + m.decode()
+        raise WfbpError(status, msg)
+
+
+def _fptr(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dptr(t):
+    """device pointer of a torch tensor (or None)"""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+def configure_geometry(meta, table_positions):
+    """ReconstructionMachine::ConfigureCTGeometry + GPUPrecompute::InitFromCTGeometry."""
+    cg, gp = T.CTGeometry(), T.GPUPrecompute()
+    tbl, ptr = _fptr(table_positions)
+    if tbl.size < meta.total_num_projections:
+        raise ValueError("table_positions shorter than total_num_projections")
+    _check(load().wfbp_configure_geometry(C.byref(meta), ptr, C.byref(cg), C.byref(gp)), "wfbp_configure_geometry")
+    return cg, gp
+
+
+def slice_locations(cg, rp):
+    """Native and requested slice z lists (float32), ReconstructionMachine.cu:107-137."""
+    lib = load()
+    nn, nr = C.c_int(), C.c_int()
+    _check(lib.wfbp_slice_locations(C.byref(cg), C.byref(rp), None, 0, C.byref(nn), None, 0, C.byref(nr)),
+           "wfbp_slice_locations")
+    nat = np.zeros(nn.value, np.float32)
+    req = np.zeros(nr.value, np.float32)
+    _check(lib.wfbp_slice_locations(C.byref(cg), C.byref(rp), nat.ctypes.data_as(C.POINTER(C.c_float)), nn.value,
+                                    C.byref(nn), req.ctypes.data_as(C.POINTER(C.c_float)), nr.value, C.byref(nr)),
+           "wfbp_slice_locations")
+    return nat, req
+
+
+def filter_taps(cg, window=T.FILTER_REFERENCE, c=1.0, a=1.0, n=None):
+    n = int(cg.num_detector_cols) if n is None else n
+    out = np.zeros(n, np.float32)
+    _check(load().wfbp_filter_taps(C.byref(cg), window, c, a, out.ctypes.data_as(C.POINTER(C.c_float)), n),
+           "wfbp_filter_taps")
+    return out
+
+
+def make_ext(precision=T.PRECISION_FP32, filter_window=T.FILTER_REFERENCE, filter_c=1.0, filter_a=1.0,
+             user_taps=None, tex_weights=0, bp_slab=0):
+    e = T.Ext()
+    e.version = T.EXT_VERSION
+    e.precision = precision
+    e.filter_window = filter_window
+    e.filter_c = filter_c
+    e.filter_a = filter_a
+    e.tex_weights = tex_weights
+    e.bp_slab = bp_slab
+    if user_taps is not None:
+        arr = np.ascontiguousarray(user_taps, dtype=np.float32)
+        e._taps_keepalive = arr
+        e.user_taps = arr.ctypes.data_as(C.POINTER(C.c_float))
+        e.n_user_taps = arr.size
+    return e
+
+
+class Context:
+    """One scan geometry + recon config on one device (wfbp_ctx)."""
+
+    def __init__(self, cg, rp, ext=None, device=0):
+        self._lib = load()
+        self._h = C.c_void_p()
+        self.cg, self.rp = cg, rp
+        self.ext = ext if ext is not None else make_ext()
+        _check(self._lib.wfbp_ctx_create(C.byref(cg), C.byref(rp), C.byref(self.ext), device, C.byref(self._h)),
+               "wfbp_ctx_create")
+        self.device = device
+        d = T.Dims()
+        _check(self._lib.wfbp_query(self._h, C.byref(d)), "wfbp_query", self._h)
+        self.dims = d
+
+    def close(self):
+        if self._h:
+            self._lib.wfbp_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def slices(self):
+        nat = np.zeros(self.dims.n_slices_native, np.float32)
+        req = np.zeros(self.dims.n_slices_requested, np.float32)
+        _check(self._lib.wfbp_get_slices(self._h, nat.ctypes.data_as(C.POINTER(C.c_float)),
+                                         req.ctypes.data_as(C.POINTER(C.c_float))), "wfbp_get_slices", self._h)
+        return nat, req
+
+    def set_views(self, tube_angles, table_positions):
+        t, tp = _fptr(tube_angles)
+        z, zp = _fptr(table_positions)
+        if t.size < self.dims.n_readings or z.size < self.dims.n_readings:
+            raise ValueError("need %d tube angles and table positions" % self.dims.n_readings)
+        _check(self._lib.wfbp_set_views(self._h, tp, zp), "wfbp_set_views", self._h)
+
+    # ---- stages (torch CUDA tensors) ----
+    def rebin(self, raw, rebinned, stream=None):
+        _check(self._lib.wfbp_rebin(self._h, _dptr(raw), _dptr(rebinned), _stream(stream)), "wfbp_rebin", self._h)
+
+    def filter(self, rebinned, filtered, row_scales=None, stream=None):
+        _check(self._lib.wfbp_filter(self._h, _dptr(rebinned), _dptr(filtered), _dptr(row_scales), _stream(stream)),
+               "wfbp_filter", self._h)
+
+    def backproject(self, filtered, volume_native, row_scales=None, update_count=None, stream=None):
+        _check(self._lib.wfbp_backproject(self._h, _dptr(filtered), _dptr(row_scales), _dptr(volume_native),
+                                          _dptr(update_count), _stream(stream)), "wfbp_backproject", self._h)
+
+    def thicken(self, volume_native, volume, stream=None):
+        _check(self._lib.wfbp_thicken(self._h, _dptr(volume_native), _dptr(volume), _stream(stream)),
+               "wfbp_thicken", self._h)
+
+    def run(self, raw, volume, stream=None):
+        _check(self._lib.wfbp_run(self._h, _dptr(raw), _dptr(volume), _stream(stream)), "wfbp_run", self._h)
+
+    def run_host(self, raw_host, volume_host=None, stream=None):
+        """raw_host: float32 array (numpy or pinned torch CPU tensor); returns the volume."""
+        import torch
+        d = self.dims
+        shape = (d.n_slices_requested, d.ny, d.nx)
+        if volume_host is None:
+            volume_host = np.zeros(shape, np.float32)
+        rp = raw_host.data_ptr() if isinstance(raw_host, torch.Tensor) else raw_host.ctypes.data
+        vp = volume_host.data_ptr() if isinstance(volume_host, torch.Tensor) else volume_host.ctypes.data
+        _check(self._lib.wfbp_run_host(self._h, C.c_void_p(rp), C.c_void_p(vp), _stream(stream)), "wfbp_run_host",
+               self._h)
+        return volume_host
+
+    # ---- allocation helpers ----
+    def alloc(self, what, device=None):
+        import torch
+        dev = torch.device("cuda", self.device if device is None else device)
+        d = self.dims
+        if what == "raw":
+            return torch.empty((d.n_readings, d.raw_rows, d.raw_channels), dtype=torch.float32, device=dev)
+        if what == "rebinned":
+            return torch.empty(d.rebinned_bytes // 4, dtype=torch.float32, device=dev)
+        if what == "filtered":
+            return torch.empty(d.filtered_bytes // 4, dtype=torch.float32, device=dev)
+        if what == "row_scales":
+            return torch.empty(max(d.row_scale_bytes // 4, 1), dtype=torch.float32, device=dev)
+        if what == "native":
+            return torch.empty((d.n_slices_native, d.ny, d.nx), dtype=torch.float32, device=dev)
+        if what == "volume":
+            return torch.empty((d.n_slices_requested, d.ny, d.nx), dtype=torch.float32, device=dev)
+        raise ValueError(what)
+
+
+def synth_project(scan, ellipsoids, out, stream=None):
+    """Line integrals (+ noise) of an ellipsoid phantom into out (CUDA float32)."""
+    arr = (T.Ellipsoid * max(len(ellipsoids), 1))()
+    for i, e in enumerate(ellipsoids):
+        arr[i] = e
+    _check(load().wfbp_synth_project(C.byref(scan), arr, len(ellipsoids), _dptr(out), _stream(stream)),
+           "wfbp_synth_project")

@@ -1,0 +1,313 @@
+/*
+ * freect_wfbp.h — C ABI of the B200 (sm_100a) helical WFBP path.
+ *
+ * This is the drop-in boundary for FreeCT fct_wfbp's reconstruction path:
+ *   rebin (fan -> parallel, optional flying focal spot merge)
+ *   -> ramp filter (Toeplitz contraction along the channel axis)
+ *   -> helical Q-weighted backprojection
+ *   -> final slice thickening.
+ *
+ * The reference has no plugin or FFI layer; its boundary is the C++ class
+ * fct::ReconstructionMachine (applications/fct_wfbp/include/ReconstructionMachine.h:8-50)
+ * whose stage methods RebinAndFilter / Backproject / ApplyFinalSliceThicknessing
+ * (ReconstructionMachine.h:25-28) exchange device buffers with fixed layouts.
+ * Every entry point below replaces one of those methods (cited per function)
+ * and keeps its buffer layout, but:
+ *   - buffers are caller-owned device pointers (scratch is context-owned),
+ *   - every call takes an explicit CUDA stream (passed as void*),
+ *   - errors are returned as status codes instead of exit() (the reference's
+ *     gpuErrChk/cufftErrChk call exit(), gpu_error_check.h:38-58),
+ *   - no call synchronises the device unless documented.
+ *
+ * All structs keep the reference's field order and types, so host code that
+ * fills the reference's structs can pass them unchanged.
+ */
+#ifndef FREECT_WFBP_H
+#define FREECT_WFBP_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Reference structs (byte-identical to applications/fct_wfbp/include/       */
+/* recon_structs.h:6-31, 33-50, 52-67)                                        */
+/* ------------------------------------------------------------------------ */
+
+/* recon_structs.h:6-31 */
+typedef struct CTGeometry {
+  size_t total_number_of_projections;
+  size_t projections_per_rotation;
+  float detector_pixel_size_col;     /* transverse spacing at the detector (mm) */
+  float detector_pixel_size_row;     /* axial spacing at the detector (mm) */
+  size_t num_detector_cols;
+  size_t num_detector_cols_padded;
+  size_t num_detector_cols_padded_fft;
+  size_t num_detector_rows;
+  size_t num_detector_rows_padded;
+  float detector_central_col;
+  float detector_central_row;
+  float distance_source_to_detector;
+  float distance_source_to_isocenter;
+  float collimated_slice_width;
+  float theta_cone;
+  float acquisition_field_of_view;
+  float z_rot;
+  float anode_angle;
+  bool ffs_phi;
+  bool ffs_z;
+  bool ffs_diag;
+} CTGeometry;
+
+/* recon_structs.h:33-50 */
+typedef struct ReconConfig {
+  char raw_data_dir[4096];
+  char output_dir[4096];
+  char output_file[255];
+  float start_pos;
+  float end_pos;
+  float recon_fov;
+  float slice_thickness;
+  float slice_pitch;
+  size_t nx;
+  size_t ny;
+  int recon_kernel;
+  float x_origin;
+  float y_origin;
+  float tube_angle_offset;
+  float adaptive_filtration_s;
+} ReconConfig;
+
+/* recon_structs.h:52-67 (the data members; InitFromCTGeometry is
+ * wfbp_configure_geometry below) */
+typedef struct GPUPrecompute {
+  float half_acquisition_fov;
+  float half_acquisition_fov_squared;
+  int projections_per_half_turn;
+  int n_half_turns;
+  float distance_source_to_isocenter_squared;
+  float z_rot_over_2_pi;
+  float recip_distance_source_to_detector;
+  float recip_distance_source_to_isocenter;
+  float tanf_theta_cone;
+  float pixel_scale;
+  float two_pi_over_projections_per_rotation;
+  int n_slices_native;
+  int n_slices_requested;
+} GPUPrecompute;
+
+/* ------------------------------------------------------------------------ */
+/* Scan metadata: the RawDataSet getters that ConfigureCTGeometry reads      */
+/* (modules/fct_read/include/fct/RawDataSet.h:90-106)                        */
+/* ------------------------------------------------------------------------ */
+typedef struct wfbp_scan_meta {
+  int total_num_projections;         /* readings in the file (after FFS: readings, not views) */
+  int projections_per_rotation;      /* readings per rotation */
+  int detector_channels;
+  int detector_rows;
+  float detector_transverse_spacing; /* mm at the detector */
+  float detector_axial_spacing;      /* mm at the detector */
+  float detector_central_channel;
+  float detector_central_row;
+  float dist_source_to_isocenter;
+  float dist_source_to_detector;
+  int ffs_mode;                      /* wfbp_ffs_mode */
+  float anode_angle;                 /* rad, used by z-FFS */
+} wfbp_scan_meta;
+
+/* ------------------------------------------------------------------------ */
+/* Status codes and options                                                 */
+/* ------------------------------------------------------------------------ */
+enum wfbp_status {
+  WFBP_OK = 0,
+  WFBP_ERR_INVALID_ARG = 1,   /* bad pointer, size, or struct field */
+  WFBP_ERR_OOM = 2,           /* a context allocation failed */
+  WFBP_ERR_CUDA = 3,          /* a CUDA runtime call or kernel launch failed */
+  WFBP_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up */
+  WFBP_ERR_UNSUPPORTED = 5,   /* option not supported for this geometry */
+  WFBP_ERR_STATE = 6          /* call out of order (e.g. views not set) */
+};
+
+enum wfbp_precision {
+  WFBP_PRECISION_FP32 = 0,    /* FP32 rebin, FP32 SIMT Toeplitz filter, FP32 rows, FP32 backprojection */
+  WFBP_PRECISION_MIXED = 1    /* split hi+lo BF16 tcgen05 filter (FP32 accumulate in TMEM),
+                                 FP16 filtered rows with per-row scales, FP32 backprojection */
+};
+
+enum wfbp_filter_window {
+  WFBP_FILTER_REFERENCE = 0,  /* generate_filter(cg, c, a): ReconstructionMachine.cu:478-513 */
+  WFBP_FILTER_SHEPP_LOGAN = 1,/* discrete Shepp-Logan kernel h[n] = -2/(pi^2 ds (4n^2-1)) */
+  WFBP_FILTER_USER = 2        /* caller-provided symmetric taps h[0..n-1] */
+};
+
+enum wfbp_ffs_mode {
+  WFBP_FFS_NONE = 0,
+  WFBP_FFS_PHI = 1,
+  WFBP_FFS_Z = 2,
+  WFBP_FFS_PHIZ = 3
+};
+
+/* Extension options that the reference has no field for. */
+#define WFBP_EXT_VERSION 1
+typedef struct wfbp_ext {
+  int version;                /* must be WFBP_EXT_VERSION */
+  int precision;              /* wfbp_precision */
+  int filter_window;          /* wfbp_filter_window */
+  float filter_c;             /* generate_filter's c (reference default 1) */
+  float filter_a;             /* generate_filter's a (reference default 1) */
+  const float* user_taps;     /* WFBP_FILTER_USER: h[0..n_user_taps-1], h[-n]=h[n] */
+  int n_user_taps;
+  int tex_weights;            /* 1: rebin uses 8-bit fractional bilinear weights like the
+                                 texture unit the reference samples through (cuda_kernels.cuh:36) */
+  int bp_slab;                /* 0 = default; native slices per backprojection slab */
+  int reserved[7];
+} wfbp_ext;
+
+/* Sizes of every stage buffer a context expects (bytes unless noted). */
+typedef struct wfbp_dims {
+  int n_views;                /* V after FFS merge */
+  int n_rows;                 /* rows after FFS merge */
+  int n_channels;             /* channels after FFS merge */
+  int n_readings;             /* raw readings (V * readings_per_view) */
+  int raw_rows, raw_channels; /* raw frame shape */
+  int nx, ny;
+  int n_slices_native;
+  int n_slices_requested;
+  int precision;
+  size_t raw_bytes;           /* float [n_readings][raw_rows][raw_channels] */
+  size_t rebinned_bytes;      /* stage-1 output (FP32 [V][nr][nch], or the split BF16 operand planes) */
+  size_t filtered_bytes;      /* stage-2 output (FP32 or FP16 [V][nr][nch]) */
+  size_t row_scale_bytes;     /* FP32 [V][nr] (MIXED only, else 0) */
+  size_t native_volume_bytes; /* FP32 [nz_native][ny][nx] */
+  size_t volume_bytes;        /* FP32 [nz_requested][ny][nx] */
+} wfbp_dims;
+
+typedef struct wfbp_ctx wfbp_ctx;
+
+/* ------------------------------------------------------------------------ */
+/* Geometry (host-only, no device needed)                                   */
+/* ------------------------------------------------------------------------ */
+
+/* ReconstructionMachine::ConfigureCTGeometry (ReconstructionMachine.cu:44-74)
+ * followed by GPUPrecompute::InitFromCTGeometry (recon_structs.h:69-83).
+ * table_positions: n = meta->total_num_projections floats (needs n > P). */
+int wfbp_configure_geometry(const wfbp_scan_meta* meta, const float* table_positions,
+                            CTGeometry* cg, GPUPrecompute* gp);
+
+/* Slice lists of ReconstructionMachine::AllocateKeyArrays
+ * (ReconstructionMachine.cu:107-137), float accumulation included.
+ * Either output pointer may be NULL to query counts. */
+int wfbp_slice_locations(const CTGeometry* cg, const ReconConfig* rp,
+                         float* native_z, int native_cap, int* n_native,
+                         float* requested_z, int requested_cap, int* n_requested);
+
+/* Filter taps: the spatial-domain kernel of generate_filter
+ * (ReconstructionMachine.cu:478-513) before its FFT, as the symmetric half
+ * h[0..n-1] (h[-k] = h[k]) in FP32. */
+int wfbp_filter_taps(const CTGeometry* cg, int window, float c, float a, float* taps, int n);
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Creates a context on `device` for one scan geometry and recon config.
+ * Replaces the state the reference keeps in ReconstructionMachine
+ * (ReconstructionMachine.h:30-48) plus its __constant__ copies
+ * (cuda_kernels.cuh:5-7). `ext` may be NULL (FP32, reference filter). */
+int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const wfbp_ext* ext,
+                    int device, wfbp_ctx** out);
+int wfbp_ctx_destroy(wfbp_ctx* ctx);
+int wfbp_query(const wfbp_ctx* ctx, wfbp_dims* dims);
+
+/* Per-view tube angles and table positions, host arrays of n_readings floats
+ * (ReconstructionMachine.cu:96-102). Builds the FP64 per-view tables. */
+int wfbp_set_views(wfbp_ctx* ctx, const float* tube_angles, const float* table_positions);
+
+/* Copies the native / requested slice z lists (as wfbp_slice_locations). */
+int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* requested_z);
+
+/* Last error message of this context (never NULL). */
+const char* wfbp_last_error(const wfbp_ctx* ctx);
+const char* wfbp_status_string(int status);
+
+/* ------------------------------------------------------------------------ */
+/* Stages (device pointers, asynchronous on `stream`)                       */
+/* ------------------------------------------------------------------------ */
+
+/* Stage 1 of RebinAndFilter (ReconstructionMachine.cu:141-256 and
+ * rebin_kernel, cuda_kernels.cuh:11-39): host reshape/flip + rebin of every
+ * row in one launch. raw: FP32 [n_readings][raw_rows][raw_channels].
+ * rebinned: FP32 [V][nr][nch] (row index = flipped row sheet index), or for
+ * WFBP_PRECISION_MIXED the split BF16 operand planes of the filter. */
+int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream);
+
+/* Stage 2 of RebinAndFilter (ReconstructionMachine.cu:262-290: R2C,
+ * multiply_filter, C2R, reshape_rebin_into_final_array) as a Toeplitz
+ * contraction. filtered: FP32 [V][nr][nch] (FP32) or FP16 [V][nr][nch]
+ * plus row_scales FP32 [V][nr] (MIXED; row_scales may be NULL for FP32). */
+int wfbp_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* row_scales,
+                void* stream);
+
+/* ReconstructionMachine::Backproject (ReconstructionMachine.cu:308-385,
+ * backproject_kernel cuda_kernels.cuh:198-287). volume_native: FP32
+ * [nz_native][ny][nx], overwritten. update_count: optional device uint64
+ * that receives the number of contributing voxel-view updates (adds to it). */
+int wfbp_backproject(wfbp_ctx* ctx, const void* filtered, const float* row_scales,
+                     float* volume_native, unsigned long long* update_count, void* stream);
+
+/* ReconstructionMachine::ApplyFinalSliceThicknessing (ReconstructionMachine.cu:387-434,
+ * thicken_slices cuda_kernels.cuh:289-320), without the D2H copy. */
+int wfbp_thicken(wfbp_ctx* ctx, const float* volume_native, float* volume, void* stream);
+
+/* RunReconstruction (ReconstructionMachine.cu:76-82) on device buffers:
+ * raw (device) -> volume (device), with context-owned intermediates. */
+int wfbp_run(wfbp_ctx* ctx, const float* raw, float* volume, void* stream);
+
+/* RunReconstruction from host memory: H2D of the raw readings, the four
+ * stages, D2H of the final volume (ReconstructionMachine.cu:246,423),
+ * synchronous on return. Pinned host buffers overlap the copies with the
+ * stages. */
+int wfbp_run_host(wfbp_ctx* ctx, const float* raw_host, float* volume_host, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic scans (test-data generator; no counterpart in the reference)    */
+/* ------------------------------------------------------------------------ */
+
+typedef struct wfbp_ellipsoid {
+  double cx, cy, cz;          /* centre (mm) */
+  double ax, ay, az;          /* semi-axes (mm) */
+  double phi;                 /* rotation about z (rad) */
+  double mu;                  /* additive attenuation (1/mm) */
+} wfbp_ellipsoid;
+
+typedef struct wfbp_synth_scan {
+  int n_readings, rows, channels, readings_per_rotation;
+  double sid, sdd;            /* mm */
+  double dcol, drow;          /* detector spacing at the detector (mm) */
+  double central_channel;
+  double angle0, dangle;      /* tube angle of reading 0, signed step per reading (rad) */
+  double z0, dz;              /* table position of reading 0, signed step per reading (mm) */
+  double i0;                  /* incident photons (0 = noiseless line integrals) */
+  unsigned long long seed;
+  int ffs_mode;               /* wfbp_ffs_mode */
+  double ffs_dphi;            /* phi-FFS: +- source shift along the tangent (mm) */
+  double ffs_dz;              /* z-FFS: +- source shift along z (mm) */
+  double ffs_dr;              /* z-FFS: +- radial source shift (mm) */
+} wfbp_synth_scan;
+
+/* Line integrals (and Poisson noise, log transform) through the ellipsoid
+ * phantom in the geometry conventions that the reference's rebin and
+ * backprojection invert. out: device FP32 [n_readings][rows][channels]. */
+int wfbp_synth_project(const wfbp_synth_scan* scan, const wfbp_ellipsoid* ellipsoids,
+                       int n_ellipsoids, float* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FREECT_WFBP_H */

@@ -1,0 +1,106 @@
+"""Golden fixtures from the reference's own kernels.
+
+Runs applications/fct_wfbp/include/cuda_kernels.cuh -- compiled unmodified
+from the reference tree into oracle/_ref/libref_wfbp_shim.so by
+oracle/ref_shim/Makefile -- on a CUDA device, with the stage logic of
+ReconstructionMachine.cu restated in oracle/ref_shim/ref_kernels_shim.cu,
+and stores inputs and outputs as .npz files:
+
+  ref_<case>.npz   raw frames, tube angles, table positions, the reference's
+                   filtered projections, native volume and final volume
+  tex_probe.npz    hardware bilinear texture samples at random coordinates
+                   (pins the texture unit's fractional-weight rounding)
+
+Usage (needs a GPU): python tests/golden/make_reference_fixtures.py [outdir]
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from freect_b200 import abi_types as T  # noqa: E402
+from freect_b200 import scans  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+SHIM = os.path.join(ROOT, "oracle", "_ref", "libref_wfbp_shim.so")
+
+
+def cases():
+    """(name, spec) pairs small enough to commit."""
+    out = [("tiny", scans.tiny(seed=11))]
+    s = scans.tiny(seed=12, nch=160, nr=12, P=200, rotations=3, nx=64, n_slices=6)
+    out.append(("medium", s))
+    s = scans.tiny(seed=13, nch=64, nr=4, P=64, rotations=2.5, nx=32, n_slices=3)
+    s.rotations = (64 * 2 + 69) / 64.0  # V = 197: views past the rebin grid
+    out.append(("oddviews", s))
+    s = scans.tiny(seed=14, nch=96, nr=8, P=96, rotations=3, nx=32, n_slices=4, window=T.FILTER_SHEPP_LOGAN)
+    out.append(("shepplogan", s))
+    return out
+
+
+def load_shim():
+    lib = C.CDLL(SHIM)
+    F = C.POINTER(C.c_float)
+    lib.ref_shim_run.restype = C.c_int
+    lib.ref_shim_run.argtypes = [C.POINTER(T.CTGeometry), C.POINTER(T.ReconConfig), C.POINTER(T.GPUPrecompute),
+                                 F, F, F, F, F, C.c_int, F, C.c_int, F, F, F]
+    lib.ref_shim_tex_probe.restype = C.c_int
+    lib.ref_shim_tex_probe.argtypes = [F, C.c_int, C.c_int, F, C.c_int, F]
+    return lib
+
+
+def taps_for(spec, cg):
+    if spec.window == T.FILTER_REFERENCE:
+        return O.taps_ref_fft(cg)
+    return O.taps_fft_from_half(cg, O.taps_f64(cg, spec.window).astype(np.float32))
+
+
+def run_reference(lib, spec, raw):
+    tube, table = spec.views()
+    cg, gp = O.configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    zn, zr = O.slice_locations(cg, rp)
+    gp.n_slices_native, gp.n_slices_requested = zn.size, zr.size
+    taps = taps_for(spec, cg)
+    V, nr, nch = spec.V, spec.nr, spec.nch
+    filt = np.zeros((V, nr, nch), np.float32)
+    native = np.zeros((zn.size, spec.ny, spec.nx), np.float32)
+    vol = np.zeros((zr.size, spec.ny, spec.nx), np.float32)
+    raw = np.ascontiguousarray(raw, np.float32)
+    st = lib.ref_shim_run(C.byref(cg), C.byref(rp), C.byref(gp), O.fp(raw), O.fp(taps), O.fp(tube), O.fp(table),
+                          O.fp(zn), zn.size, O.fp(zr), zr.size, O.fp(filt), O.fp(native), O.fp(vol))
+    if st != 0:
+        raise RuntimeError("ref_shim_run failed with %d" % st)
+    return dict(raw=raw, tube=tube, table=table, taps_fft=taps, filtered=filt, native=native, volume=vol,
+                z_native=zn, z_req=zr)
+
+
+def tex_probe(lib, seed=5, w=37, h=23, n=20000):
+    rng = np.random.default_rng(seed)
+    img = rng.standard_normal((h, w)).astype(np.float32)
+    xy = np.stack([rng.uniform(-2, w + 2, n), rng.uniform(-2, h + 2, n)], 1).astype(np.float32)
+    out = np.zeros(n, np.float32)
+    st = lib.ref_shim_tex_probe(O.fp(img), w, h, O.fp(np.ascontiguousarray(xy)), n, O.fp(out))
+    if st != 0:
+        raise RuntimeError("ref_shim_tex_probe failed with %d" % st)
+    return dict(img=img, xy=xy, out=out)
+
+
+def main(outdir):
+    os.makedirs(outdir, exist_ok=True)
+    lib = load_shim()
+    for name, spec in cases():
+        raw = O.synth_project(spec.synth(), spec.ellipsoids())
+        res = run_reference(lib, spec, raw)
+        np.savez_compressed(os.path.join(outdir, "ref_%s.npz" % name), **res)
+        print(name, spec.V, spec.nr, spec.nch, res["volume"].shape, float(np.nanmean(res["volume"])))
+    np.savez_compressed(os.path.join(outdir, "tex_probe.npz"), **tex_probe(lib))
+    print("wrote", outdir)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))

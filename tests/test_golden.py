@@ -1,0 +1,82 @@
+"""The oracle against outputs of the reference's own kernels.
+
+tests/golden/ref_*.npz and tex_probe.npz were produced by
+tests/golden/make_reference_fixtures.py, which runs the reference's
+cuda_kernels.cuh (compiled unmodified from its source tree with a texture
+object standing in for the removed texture-reference API) on a B200.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from freect_b200 import abi_types as T
+from freect_b200 import scans
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REF_FILES = sorted(glob.glob(os.path.join(GOLD, "ref_*.npz")))
+
+
+def tex_emulate(img, xy, rounding):
+    """tex2D, linear filter, clamp addressing, unnormalised coordinates, with
+    the fractional weights reduced to 8 bits by `rounding`."""
+    h, w = img.shape
+    xb = xy[:, 0].astype(np.float32) - np.float32(0.5)
+    yb = xy[:, 1].astype(np.float32) - np.float32(0.5)
+    fx, fy = np.floor(xb), np.floor(yb)
+    ax, ay = (xb - fx).astype(np.float32), (yb - fy).astype(np.float32)
+    if rounding == "nearest":
+        ax = np.rint(ax * 256) / 256
+        ay = np.rint(ay * 256) / 256
+    elif rounding == "truncate":
+        ax = np.floor(ax * 256) / 256
+        ay = np.floor(ay * 256) / 256
+    x0 = np.clip(fx.astype(int), 0, w - 1)
+    x1 = np.clip(fx.astype(int) + 1, 0, w - 1)
+    y0 = np.clip(fy.astype(int), 0, h - 1)
+    y1 = np.clip(fy.astype(int) + 1, 0, h - 1)
+    return ((1 - ax) * (1 - ay) * img[y0, x0] + ax * (1 - ay) * img[y0, x1] + (1 - ax) * ay * img[y1, x0]
+            + ax * ay * img[y1, x1])
+
+
+def test_fixtures_present():
+    assert len(REF_FILES) >= 4, "run tests/golden/make_reference_fixtures.py on a GPU"
+    assert os.path.exists(os.path.join(GOLD, "tex_probe.npz"))
+
+
+def test_texture_unit_weights_are_8bit_round_to_nearest():
+    d = np.load(os.path.join(GOLD, "tex_probe.npz"))
+    img, xy, hw = d["img"], d["xy"], d["out"]
+    err = {r: np.abs(tex_emulate(img, xy, r) - hw).max() for r in ("nearest", "truncate", "exact")}
+    assert err["nearest"] < 2e-3, err
+    assert err["nearest"] <= err["truncate"] and err["nearest"] < err["exact"], err
+
+
+def _spec_for(name):
+    from tests.golden.make_reference_fixtures import cases
+    return dict(cases())[name]
+
+
+@pytest.mark.parametrize("path", REF_FILES, ids=[os.path.basename(p) for p in REF_FILES])
+def test_oracle_transcript_matches_reference_kernels(orc, path):
+    name = os.path.basename(path)[4:-4]
+    spec = _spec_for(name)
+    d = np.load(path)
+    raw = d["raw"]
+    cg, gp = orc.configure_geometry(spec.meta(), d["table"])
+    filt = orc.rebin_filter_ref32(cg, raw, d["taps_fft"], q8=True)
+    scale = np.abs(d["filtered"]).max()
+    diff = np.abs(filt - d["filtered"])
+    # cuFFT's FP32 rounding vs the oracle's double FFT, plus rare texel
+    # fraction flips from asinf/contraction ulps
+    assert np.mean(diff < 1e-5 * scale) > 0.999
+    assert diff.max() < 2e-3 * scale
+    ref = orc.reconstruct_ref32(spec, raw, taps_half=None, q8=True)
+    rms, mx, n = orc.hu_error(ref["volume"], d["volume"])
+    assert n == d["volume"].size
+    assert rms < 0.05 and mx < 0.5, (rms, mx)
+    # and the exact-weight FP64 oracle is within the parity budget of the reference
+    r64 = orc.reconstruct_f64(spec, raw)
+    rms64, mx64, _ = orc.hu_error(r64["volume"], d["volume"])
+    assert rms64 < 0.5, (rms64, mx64)

@@ -1,0 +1,228 @@
+"""GPU parity: every stage of the sm_100a path, called through the C ABI,
+against the oracle on the same seeded inputs.
+
+Tolerances: stages are compared elementwise relative to the data's scale
+(FP32 arithmetic in a different order); volumes in HU (1 HU = 1.9e-5 /mm):
+the FP32 form must stay within 0.5 HU RMS / 2 HU max of the reference
+transcript (the north-star parity gate).
+"""
+import numpy as np
+import pytest
+
+from freect_b200 import abi_types as T
+from freect_b200 import scans, wfbp
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+DEV = torch.device("cuda", 0)
+
+
+def make_ctx(spec, **ext):
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    ctx = wfbp.Context(cg, spec.recon_config(), wfbp.make_ext(filter_window=spec.window, **ext), device=0)
+    ctx.set_views(tube, table)
+    return ctx, cg, gp
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(DEV)
+
+
+@pytest.fixture(scope="module")
+def tiny(orc):
+    spec = scans.tiny()
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    return spec, raw
+
+
+@pytest.mark.parametrize("q8", [0, 1])
+def test_rebin_matches_oracle(orc, tiny, q8):
+    spec, raw = tiny
+    ctx, cg, _ = make_ctx(spec, tex_weights=q8)
+    out = ctx.alloc("rebinned")
+    ctx.rebin(dev(raw), out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(spec.V, spec.nr, spec.nch)
+    ref = orc.rebin_ref32(cg, raw, q8=bool(q8))
+    scale = np.abs(ref).max()
+    d = np.abs(got - ref)
+    # identical formula; contraction / asinf ulps can move a texel fraction
+    assert np.mean(d < 1e-5 * scale) > 0.999
+    assert d.max() < (1.0 / 128 if q8 else 1e-3) * scale
+    ref64 = orc.rebin_f64(cg, raw)
+    if not q8:
+        assert np.abs(got - ref64).max() < 1e-3 * scale
+
+
+def test_filter_matches_oracle(orc, tiny):
+    spec, raw = tiny
+    ctx, cg, _ = make_ctx(spec)
+    reb = orc.rebin_ref32(cg, raw)
+    out = ctx.alloc("filtered")
+    ctx.filter(dev(reb), out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(reb.shape)
+    half = wfbp.filter_taps(cg).astype(np.float64)
+    ref = orc.filter_f64(reb, half)
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() < 2e-5 * scale
+
+
+def test_backproject_matches_oracle(orc, tiny):
+    spec, raw = tiny
+    ctx, cg, gp = make_ctx(spec)
+    tube, table = spec.views()
+    filt = orc.rebin_filter_ref32(cg, raw, orc.taps_ref_fft(cg))
+    nat, _ = ctx.slices()
+    vn = ctx.alloc("native")
+    cnt = torch.zeros(1, dtype=torch.int64, device=DEV)
+    ctx.backproject(dev(filt), vn, update_count=cnt)
+    torch.cuda.synchronize()
+    got = vn.cpu().numpy()
+    ref = orc.backproject_ref32(cg, ctx.rp, gp, filt, tube, table, nat)
+    rms, mx, n = orc.hu_error(got, ref)
+    assert n == got.size
+    assert rms < 0.05 and mx < 0.5
+    v64, n64 = orc.backproject_f64(cg, ctx.rp, filt.astype(np.float64), tube.astype(np.float64),
+                                   table.astype(np.float64), nat)
+    assert abs(int(cnt.item()) - n64) <= 1e-4 * n64
+
+
+def test_thicken_matches_oracle(orc, tiny):
+    spec, _ = tiny
+    ctx, cg, gp = make_ctx(spec)
+    nat, req = ctx.slices()
+    rng = np.random.default_rng(3)
+    vn = rng.standard_normal((nat.size, spec.ny, spec.nx)).astype(np.float32)
+    out = ctx.alloc("volume")
+    ctx.thicken(dev(vn), out)
+    torch.cuda.synchronize()
+    ref = orc.thicken_ref32(ctx.rp, vn, nat, req)
+    assert np.allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("q8", [1, 0])
+def test_full_path_vs_reference_transcript(orc, tiny, q8):
+    spec, raw = tiny
+    ctx, cg, gp = make_ctx(spec, tex_weights=q8)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    got = vol.cpu().numpy()
+    ref = orc.reconstruct_ref32(spec, raw, q8=bool(q8))
+    rms, mx, n = orc.hu_error(got, ref["volume"])
+    assert n == got.size
+    assert rms <= 0.5 and mx <= 2.0
+    r64 = orc.reconstruct_f64(spec, raw)
+    rms64, mx64, _ = orc.hu_error(got, r64["volume"])
+    assert rms64 <= (0.5 if q8 else 0.1)
+
+
+def test_small_config_vs_reference_transcript(orc):
+    # the small scanner (672 x 16, 1160 views/rot, 3 rotations) on a 128^2 grid
+    spec = scans.small(seed=1)
+    spec.nx = spec.ny = 128
+    spec.n_slices = 6
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    ctx, cg, gp = make_ctx(spec, tex_weights=1)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    got = vol.cpu().numpy()
+    ref = orc.reconstruct_ref32(spec, raw, q8=True)
+    rms, mx, n = orc.hu_error(got, ref["volume"])
+    assert n == got.size, "NaN voxels"
+    assert rms <= 0.5 and mx <= 2.0, (rms, mx)
+
+
+def test_odd_sizes(orc):
+    # sizes no launch divides evenly: nx=33, ny=17, V % 8 != 0, nch % 4 != 0
+    spec = scans.tiny(nch=90, nr=5, P=100, rotations=2.57, nx=33, n_slices=3)
+    spec.ny = 17
+    assert spec.V % 8 != 0
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    ctx, cg, gp = make_ctx(spec)
+    tube, table = spec.views()
+    reb = ctx.alloc("rebinned")
+    ctx.rebin(dev(raw), reb)
+    filt = ctx.alloc("filtered")
+    ctx.filter(reb, filt)
+    vn = ctx.alloc("native")
+    ctx.backproject(filt, vn)
+    torch.cuda.synchronize()
+    ref_reb = orc.rebin_ref32(cg, raw)
+    scale = np.abs(ref_reb).max()
+    assert np.abs(reb.cpu().numpy().reshape(ref_reb.shape) - ref_reb).max() < 1e-3 * scale
+    ref_f = orc.filter_f64(ref_reb, wfbp.filter_taps(cg).astype(np.float64))
+    got_f = filt.cpu().numpy().reshape(ref_f.shape)
+    assert np.abs(got_f - ref_f).max() < 1e-4 * np.abs(ref_f).max()
+    nat, _ = ctx.slices()
+    ref_v = orc.backproject_ref32(cg, ctx.rp, gp, got_f, tube, table, nat)
+    rms, mx, n = orc.hu_error(vn.cpu().numpy(), ref_v)
+    assert rms < 0.05 and mx < 0.5
+
+
+def test_synth_gpu_matches_cpu(orc):
+    spec = scans.tiny()
+    scan = spec.synth(i0=0)
+    ref = orc.synth_project(scan, spec.ellipsoids())
+    out = torch.empty(ref.shape, dtype=torch.float32, device=DEV)
+    wfbp.synth_project(scan, spec.ellipsoids(), out)
+    torch.cuda.synchronize()
+    assert np.allclose(out.cpu().numpy(), ref, rtol=1e-6, atol=1e-6)
+
+
+def test_run_host_matches_run(orc, tiny):
+    spec, raw = tiny
+    ctx, cg, gp = make_ctx(spec, tex_weights=1)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    host = ctx.run_host(np.ascontiguousarray(raw))
+    assert np.array_equal(host, vol.cpu().numpy())
+
+
+def test_state_and_argument_errors(tiny):
+    spec, raw = tiny
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    ctx = wfbp.Context(cg, spec.recon_config())
+    f = ctx.alloc("filtered")
+    vn = ctx.alloc("native")
+    with pytest.raises(wfbp.WfbpError) as e:
+        ctx.backproject(f, vn)  # views not set
+    assert e.value.status == T.WFBP_OK + 6
+    bad = tube.copy()
+    bad[5] = np.nan
+    with pytest.raises(wfbp.WfbpError) as e:
+        ctx.set_views(bad, table)
+    assert e.value.status == 1
+    assert "reading 5" in str(e.value)
+
+
+def _golden_files():
+    import glob
+    import os
+    return sorted(glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_*.npz")))
+
+
+@pytest.mark.parametrize("path", _golden_files(), ids=lambda p: p.rsplit("/", 1)[-1])
+def test_fp32_form_vs_reference_kernels(orc, path):
+    # The parity gate against the reference's own fct_wfbp kernels (run on a
+    # B200 via the shim): the FP32 form within 0.5 HU RMS / 2 HU max.
+    from tests.golden.make_reference_fixtures import cases
+    name = path.rsplit("/", 1)[-1][4:-4]
+    spec = dict(cases())[name]
+    d = np.load(path)
+    ctx, cg, gp = make_ctx(spec, tex_weights=1)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(d["raw"]), vol)
+    torch.cuda.synchronize()
+    rms, mx, n = orc.hu_error(vol.cpu().numpy(), d["volume"])
+    assert n == d["volume"].size
+    assert rms <= 0.5 and mx <= 2.0, (rms, mx)
