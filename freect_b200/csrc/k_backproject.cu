@@ -16,6 +16,8 @@
 // fails the reference's z cull (|z_j - z| > z_rot) for every slice of its slab.
 #include "wfbp_internal.h"
 
+#include <type_traits>
+
 namespace {
 
 constexpr int BP_TX = 16, BP_TY = 8, BP_THREADS = BP_TX * BP_TY;
@@ -27,11 +29,17 @@ __device__ __forceinline__ float q_weight(float qh) {
   return fmaf(0.5f, __cosf(3.14159265f * t), 0.5f);
 }
 
-template <int ZS, bool COUNT>
+__device__ __forceinline__ float ld_tap(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_tap(const __half* p) { return __half2float(__ldg(p)); }
+
+// T = float: FP32 filtered rows. T = __half: FP16 rows, row r of view j
+// stored as y / scale[j][r] (scales != nullptr).
+template <int ZS, bool COUNT, typename T>
 __global__ void __launch_bounds__(BP_THREADS)
-k_bp_f32(const float* __restrict__ D, float* __restrict__ vol, const float2* __restrict__ view_sc,
-         const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p,
-         unsigned long long* __restrict__ count) {
+k_bp(const T* __restrict__ D, const float* __restrict__ scales, float* __restrict__ vol,
+     const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
+     BPParams p, unsigned long long* __restrict__ count) {
+  constexpr bool SCALED = !std::is_same<T, float>::value;
   const int ix = blockIdx.x * BP_TX + (threadIdx.x % BP_TX);
   const int iy = blockIdx.y * BP_TY + (threadIdx.x / BP_TX);
   const int s0 = blockIdx.z * ZS;
@@ -79,7 +87,8 @@ k_bp_f32(const float* __restrict__ D, float* __restrict__ vol, const float2* __r
         const float pf = floorf(p_idx);
         if (!(pf >= 0.0f && ceilf(p_idx) <= p.ncm2)) continue;  // cuda_kernels.cuh:259-263
         const float wp = p_idx - pf;
-        const float* Dv = D + (size_t)j * view_elems + (int)pf;
+        const T* Dv = D + (size_t)j * view_elems + (int)pf;
+        const float* Sv = SCALED ? scales + (size_t)j * p.nr : nullptr;
 #pragma unroll
         for (int i = 0; i < ZS; i++) {
           const float dz = z[i] - zt;
@@ -90,10 +99,14 @@ k_bp_f32(const float* __restrict__ D, float* __restrict__ vol, const float2* __r
           const float wq = q_idx - qf;
           int r = (int)qf;
           r = min(max(r, 0), p.nr - 2);
-          const float* d0 = Dv + r * p.nch;
-          const float d00 = __ldg(d0), d01 = __ldg(d0 + 1), d10 = __ldg(d0 + p.nch), d11 = __ldg(d0 + p.nch + 1);
-          const float top = fmaf(wp, d01 - d00, d00);
-          const float bot = fmaf(wp, d11 - d10, d10);
+          const T* d0 = Dv + r * p.nch;
+          const float d00 = ld_tap(d0), d01 = ld_tap(d0 + 1), d10 = ld_tap(d0 + p.nch), d11 = ld_tap(d0 + p.nch + 1);
+          float top = fmaf(wp, d01 - d00, d00);
+          float bot = fmaf(wp, d11 - d10, d10);
+          if (SCALED) {
+            top *= __ldg(Sv + r);
+            bot *= __ldg(Sv + r + 1);
+          }
           const float g = fmaf(wq, bot - top, top);
           const float W = ok ? q_weight(qh) : 0.0f;
           ag[i] = fmaf(W, g, ag[i]);
@@ -120,14 +133,28 @@ k_bp_f32(const float* __restrict__ D, float* __restrict__ vol, const float2* __r
 
 }  // namespace
 
-cudaError_t launch_backproject_f32(const float* D, float* vol, const float2* sc, const float* vz, const float* zs,
-                                   const BPParams& p, unsigned long long* count, cudaStream_t s) {
+namespace {
+template <typename T>
+cudaError_t launch_bp(const T* D, const float* scales, float* vol, const float2* sc, const float* vz,
+                      const float* zs, const BPParams& p, unsigned long long* count, cudaStream_t s) {
   constexpr int ZS = 8;
   dim3 grid((unsigned)((p.nx + BP_TX - 1) / BP_TX), (unsigned)((p.ny + BP_TY - 1) / BP_TY),
             (unsigned)((p.nz + ZS - 1) / ZS));
   if (count)
-    k_bp_f32<ZS, true><<<grid, BP_THREADS, 0, s>>>(D, vol, sc, vz, zs, p, count);
+    k_bp<ZS, true, T><<<grid, BP_THREADS, 0, s>>>(D, scales, vol, sc, vz, zs, p, count);
   else
-    k_bp_f32<ZS, false><<<grid, BP_THREADS, 0, s>>>(D, vol, sc, vz, zs, p, count);
+    k_bp<ZS, false, T><<<grid, BP_THREADS, 0, s>>>(D, scales, vol, sc, vz, zs, p, count);
   return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_backproject_f32(const float* D, float* vol, const float2* sc, const float* vz, const float* zs,
+                                   const BPParams& p, unsigned long long* count, cudaStream_t s) {
+  return launch_bp<float>(D, nullptr, vol, sc, vz, zs, p, count, s);
+}
+
+cudaError_t launch_backproject_f16(const __half* D, const float* scales, float* vol, const float2* sc,
+                                   const float* vz, const float* zs, const BPParams& p, unsigned long long* count,
+                                   cudaStream_t s) {
+  return launch_bp<__half>(D, scales, vol, sc, vz, zs, p, count, s);
 }

@@ -1,0 +1,316 @@
+// Ramp filter as a split-precision Toeplitz contraction on the 5th-generation
+// tensor cores (tcgen05 / UMMA, sm_100a).
+//
+// The reference filters each zero-padded detector row with cuFFT
+// (ReconstructionMachine.cu:206-290, cuda_kernels.cuh:41-58). With >= nch-1
+// zeros of padding that circular convolution equals, on the data window, the
+// linear convolution y[n] = sum_k h[|n-k|] x[k]: Y = X T with X the rebinned
+// rows [M = V*nr][K = nch] and T the symmetric Toeplitz matrix of the taps.
+//
+// Precision: X = Xhi + Xlo and T = Thi + Tlo in BF16 (hi = bf16(v),
+// lo = bf16(v - hi)); Y = Xhi Thi + Xhi Tlo + Xlo Thi accumulated in FP32 in
+// tensor memory (the dropped Xlo Tlo term is ~2^-16 relative).
+//
+// Tiling: one CTA computes a 128 x BN tile of Y (BN <= 256, a multiple of 16).
+// Warp 0 lane 0 issues TMA loads (128B-swizzled, K-major) of the four operand
+// tiles of each 64-wide K block into a 2-stage ring; warp 1 lane 0 issues the
+// 3 x 4 UMMAs (M128 x N BN x K16) per K block and commits each stage back to
+// the producer; all four warps then read the FP32 accumulator out of tensor
+// memory (tcgen05.ld 32x32b, one row per thread) and store FP32 rows or FP16
+// rows scaled by a per-row power of two. Every mbarrier wait is bounded: on
+// timeout the CTA records an error code, stops issuing work, waits (bounded)
+// for its TMA copies and frees its tensor memory before returning.
+#include "wfbp_internal.h"
+
+#include <cuda.h>
+
+namespace {
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 64;  // 64 bf16 = 128 bytes, one swizzle row
+constexpr int TC_STAGES = 2;
+constexpr int TC_THREADS = 128;
+constexpr uint32_t TC_TMEM_COLS = 256;
+constexpr long long SPIN_LIMIT = 1ll << 26;
+
+struct TcParams {
+  int M;          // rows of X (V * nr)
+  int nch;        // valid output channels
+  int BN;         // N tile
+  int kblocks;    // Kp / 64
+  int np;         // padded N (rows of one B plane)
+  int out_fp16;   // 1: FP16 + row scales, 0: FP32
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait on phase parity; returns false after SPIN_LIMIT polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < SPIN_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), LBO 16 bytes, descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// kind::f16 instruction descriptor: D F32, A/B BF16, both K-major, M=128, N=bn.
+__host__ __device__ constexpr uint32_t idesc_bf16(int bn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcParams p,
+              float* __restrict__ y32, __half* __restrict__ y16, const float* __restrict__ row_scale,
+              float* __restrict__ row_scale_out, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t a_bytes = TC_BM * TC_BK * 2;          // 16 KB per plane
+  const uint32_t b_bytes = (uint32_t)p.BN * TC_BK * 2; // BN x 128 B per plane
+  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * stage_bytes);
+  uint64_t* empty = full + TC_STAGES;
+  uint64_t* done = empty + TC_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  __shared__ int s_fail;
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * p.BN;
+
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    for (int s = 0; s < TC_STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  int issued = 0;  // K blocks whose loads the producer issued
+  if (warp == 0 && lane == 0) {
+    for (int kb = 0; kb < p.kblocks; kb++) {
+      const int s = kb % TC_STAGES;
+      if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1)) {
+        atomicExch(&s_fail, 1);
+        break;
+      }
+      if (*((volatile int*)&s_fail)) break;
+      uint8_t* st = smem + s * stage_bytes;
+      mbar_expect_tx(&full[s], stage_bytes);
+      const int kx = kb * TC_BK;
+      tma_load_2d(st, &mapA, &full[s], kx, m0);
+      tma_load_2d(st + a_bytes, &mapA, &full[s], kx, p.M + m0);
+      tma_load_2d(st + 2 * a_bytes, &mapB, &full[s], kx, n0);
+      tma_load_2d(st + 2 * a_bytes + b_bytes, &mapB, &full[s], kx, p.np + n0);
+      issued = kb + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    const uint32_t idesc = idesc_bf16(p.BN);
+    bool ok = true;
+    for (int kb = 0; kb < p.kblocks && ok; kb++) {
+      const int s = kb % TC_STAGES;
+      if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1)) {
+        atomicExch(&s_fail, 1);
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t st = smem_u32(smem + s * stage_bytes);
+      const uint32_t ahi = st, alo = st + a_bytes, bhi = st + 2 * a_bytes, blo = bhi + b_bytes;
+#pragma unroll
+      for (int kk = 0; kk < TC_BK / 16; kk++) {
+        const uint32_t off = kk * 32;  // 16 bf16 along K inside the swizzle row
+        umma_bf16(tmem, sw128_desc(ahi + off), sw128_desc(bhi + off), idesc, (kb | kk) ? 1u : 0u);
+        umma_bf16(tmem, sw128_desc(ahi + off), sw128_desc(blo + off), idesc, 1u);
+        umma_bf16(tmem, sw128_desc(alo + off), sw128_desc(bhi + off), idesc, 1u);
+      }
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);  // arrives when every issued MMA has completed
+  }
+  __syncwarp();
+
+  // epilogue: warp w owns TMEM lanes / tile rows 32w .. 32w+31
+  const bool have = mbar_wait(done, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!have) atomicExch(&s_fail, 1);
+  __syncthreads();
+  const bool failed = *((volatile int*)&s_fail) != 0;
+  if (!failed) {
+    const int m = m0 + warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const float inv = (p.out_fp16 && m < p.M) ? 1.0f / row_scale[m] : 1.0f;
+    if (p.out_fp16 && blockIdx.y == 0 && m < p.M && row_scale_out) row_scale_out[m] = row_scale[m];
+    for (int c = 0; c < p.BN; c += 16) {
+      float v[16];
+      tmem_ld16(trow + (uint32_t)c, v);
+      const int n = n0 + c;
+      if (m >= p.M || n >= p.nch) continue;
+      if (p.out_fp16) {
+        __half* dst = y16 + (size_t)m * p.nch + n;
+        if (n + 16 <= p.nch && ((p.nch & 7) == 0)) {
+          __align__(16) __half h[16];
+#pragma unroll
+          for (int i = 0; i < 16; i++) h[i] = __float2half_rn(v[i] * inv);
+          reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<uint4*>(h)[0];
+          reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<uint4*>(h)[1];
+        } else {
+          for (int i = 0; i < 16 && n + i < p.nch; i++) dst[i] = __float2half_rn(v[i] * inv);
+        }
+      } else {
+        float* dst = y32 + (size_t)m * p.nch + n;
+        if (n + 16 <= p.nch && ((p.nch & 3) == 0)) {
+#pragma unroll
+          for (int i = 0; i < 16; i += 4) reinterpret_cast<float4*>(dst)[i / 4] = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        } else {
+          for (int i = 0; i < 16 && n + i < p.nch; i++) dst[i] = v[i];
+        }
+      }
+    }
+  } else if (warp == 0 && lane == 0) {
+    atomicExch(err, WFBP_ERR_TIMEOUT);
+    // let issued copies land before the shared memory is released (bounded)
+    for (int kb = (issued > TC_STAGES ? issued - TC_STAGES : 0); kb < issued; kb++)
+      mbar_wait(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D bf16 map over `rows` rows of `kp` elements, box 64 x box_rows, 128B swizzle.
+bool make_map(CUtensorMap* map, const void* base, uint64_t kp, uint64_t rows, uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {kp, rows};
+  cuuint64_t strides[1] = {kp * 2};
+  cuuint32_t box[2] = {TC_BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+size_t tc_smem_bytes(int bn) { return (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 2 + 2 * bn * TC_BK * 2) + 1024 + 256; }
+
+// Chooses the N tile (multiple of 16, <= 256) that minimises padding of nch.
+int tc_choose_bn(int nch) {
+  int best = 256;
+  long best_pad = -1;
+  for (int bn = 256; bn >= 64; bn -= 16) {
+    long np = ((long)(nch + bn - 1) / bn) * bn;
+    if (best_pad < 0 || np < best_pad) { best_pad = np; best = bn; }
+  }
+  return best;
+}
+
+// a_planes: bf16 [2][M][kp] (hi then lo); b_planes: bf16 [2][np][kp].
+cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
+                             float* y32, __half* y16, const float* row_scale, float* row_scale_out, int* err,
+                             cudaStream_t s) {
+  if (bn < 16 || bn > 256 || bn % 16 || kp % TC_BK || np % bn) return cudaErrorInvalidValue;
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, a_planes, (uint64_t)kp, 2ull * M, TC_BM)) return cudaErrorInvalidValue;
+  if (!make_map(&mb, b_planes, (uint64_t)kp, 2ull * np, (uint32_t)bn)) return cudaErrorInvalidValue;
+  TcParams p;
+  p.M = M;
+  p.nch = nch;
+  p.BN = bn;
+  p.kblocks = kp / TC_BK;
+  p.np = np;
+  p.out_fp16 = y16 != nullptr;
+  size_t smem = tc_smem_bytes(bn);
+  cudaError_t e = cudaFuncSetAttribute(k_toeplitz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((M + TC_BM - 1) / TC_BM), (unsigned)(np / bn));
+  k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(ma, mb, p, y32, y16, row_scale, row_scale_out, err);
+  return cudaGetLastError();
+}

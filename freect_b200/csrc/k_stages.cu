@@ -242,3 +242,64 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
   k_thicken<<<grid, 256, 0, s>>>(vn, out, off, idx, w, ws, nxy);
   return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// rebin for the mixed-precision filter
+// ---------------------------------------------------------------------------
+//
+// Same samples as k_rebin_f32, written as the two BF16 operand planes of the
+// tensor-core Toeplitz filter: hi = bf16(x), lo = bf16(x - hi), rows padded
+// with zeros to kp (a multiple of 64). One CTA per detector row also writes
+// the row's FP16 storage scale: the smallest power of two s with
+// max|x| * sum|h| / s <= 16384, which bounds every filtered value of the row
+// (|y| <= sum|h| max|x|) well inside the FP16 range.
+constexpr int RS_THREADS = 256;
+
+__global__ void __launch_bounds__(RS_THREADS)
+k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
+              float* __restrict__ row_scale, const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
+              RebinParams p, int kp, float taps_l1) {
+  __shared__ float s_red[RS_THREADS / 32];
+  const long row = blockIdx.x;
+  const int v = (int)(row / p.nr), i = (int)(row % p.nr);
+  const float* rawrow = raw + (size_t)(p.nr - 1 - i) * p.nch;
+  const size_t vs = (size_t)p.nr * p.nch;
+  float amax = 0.0f;
+  for (int q = threadIdx.x; q < kp / 4; q += RS_THREADS) {
+    const int c = q * 4;
+    float x[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      x[u] = (c + u < p.nch) ? rebin_sample(rawrow, vs, p.V, p.nch, __ldg(bidx_t + c + u), __ldg(beta_t + c + u), v,
+                                            p.dth, p.q8)
+                             : 0.0f;
+    __align__(8) __nv_bfloat16 hi[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      hi[u] = __float2bfloat16_rn(x[u]);
+      lo[u] = __float2bfloat16_rn(x[u] - __bfloat162float(hi[u]));
+      amax = fmaxf(amax, fabsf(x[u]));
+    }
+    *reinterpret_cast<uint2*>(a_hi + (size_t)row * kp + c) = *reinterpret_cast<uint2*>(hi);
+    *reinterpret_cast<uint2*>(a_lo + (size_t)row * kp + c) = *reinterpret_cast<uint2*>(lo);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x / 32] = amax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.0f;
+    for (int w = 0; w < RS_THREADS / 32; w++) m = fmaxf(m, s_red[w]);
+    float bound = fmaxf(m * taps_l1, 1e-30f) * (1.0f / 16384.0f);
+    row_scale[row] = exp2f(ceilf(log2f(bound)));
+  }
+}
+
+cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, const float* d_beta,
+                               const float* d_bidx, const RebinParams& p, int kp, float taps_l1, cudaStream_t s) {
+  const long rows = (long)p.V * p.nr;
+  __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
+  __nv_bfloat16* lo = hi + (size_t)rows * kp;
+  k_rebin_split<<<(unsigned)rows, RS_THREADS, 0, s>>>(raw, hi, lo, row_scale, d_beta, d_bidx, p, kp, taps_l1);
+  return cudaGetLastError();
+}

@@ -100,6 +100,20 @@ int make_taps(const CTGeometry* cg, int window, float c, float a, const float* u
   return WFBP_OK;
 }
 
+uint16_t bf16_rn(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+float bf16_to_f(uint16_t b) {
+  uint32_t u = (uint32_t)b << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
 void free_dev(void*& p) {
   if (p) cudaFree(p);
   p = nullptr;
@@ -124,6 +138,8 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_thick_idx);
   free_dev(ctx->d_thick_w);
   free_dev(ctx->d_thick_ws);
+  free_dev(ctx->d_bplanes);
+  free_dev(ctx->d_err);
   free_dev(ctx->s_rebinned);
   free_dev(ctx->s_filtered);
   free_dev(ctx->s_scales);
@@ -279,7 +295,7 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     if (ext->version != WFBP_EXT_VERSION) return WFBP_ERR_INVALID_ARG;
     e = *ext;
   }
-  if (e.precision != WFBP_PRECISION_FP32) return WFBP_ERR_UNSUPPORTED;
+  if (e.precision != WFBP_PRECISION_FP32 && e.precision != WFBP_PRECISION_MIXED) return WFBP_ERR_INVALID_ARG;
   if (cg->ffs_phi || cg->ffs_z || cg->ffs_diag) return WFBP_ERR_UNSUPPORTED;
   if (cg->projections_per_rotation < 2 || cg->total_number_of_projections <= cg->projections_per_rotation / 2 ||
       cg->num_detector_cols < 4 || cg->num_detector_rows < 2 || rp->nx < 1 || rp->ny < 1 ||
@@ -369,6 +385,29 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
   if (!ce) ce = alloc_copy((void**)&ctx->d_thick_idx, ctx->thick_idx.data(), sizeof(int) * ctx->thick_idx.size());
   if (!ce) ce = alloc_copy((void**)&ctx->d_thick_w, ctx->thick_w.data(), sizeof(float) * ctx->thick_w.size());
   if (!ce) ce = alloc_copy((void**)&ctx->d_thick_ws, ws.data(), sizeof(float) * ws.size());
+  if (!ce) ce = alloc_copy((void**)&ctx->d_err, nullptr, sizeof(int));
+  if (!ce) ce = cudaMemset(ctx->d_err, 0, sizeof(int));
+  if (!ce && e.precision == WFBP_PRECISION_MIXED) {
+    // Toeplitz operand T[n][k] = h[|n - k|], split into BF16 hi/lo planes,
+    // zero-padded to [np][kp]
+    const int nch = ctx->nch;
+    ctx->tc_kp = (nch + 63) / 64 * 64;
+    ctx->tc_bn = tc_choose_bn(nch);
+    ctx->tc_np = (nch + ctx->tc_bn - 1) / ctx->tc_bn * ctx->tc_bn;
+    const size_t plane = (size_t)ctx->tc_np * ctx->tc_kp;
+    std::vector<uint16_t> b(2 * plane, 0);
+    double l1 = 0.0;
+    for (int d = 0; d < nch; d++) l1 += (d ? 2.0 : 1.0) * fabs((double)ctx->taps[d]);
+    ctx->taps_l1 = (float)l1;
+    for (int n = 0; n < nch; n++)
+      for (int k = 0; k < nch; k++) {
+        float h = ctx->taps[n > k ? n - k : k - n];
+        uint16_t hi = bf16_rn(h);
+        b[(size_t)n * ctx->tc_kp + k] = hi;
+        b[plane + (size_t)n * ctx->tc_kp + k] = bf16_rn(h - bf16_to_f(hi));
+      }
+    ce = alloc_copy(&ctx->d_bplanes, b.data(), sizeof(uint16_t) * b.size());
+  }
   if (!ce) ce = launch_rebin_tables(ctx->d_chan_beta, ctx->d_chan_bidx, ctx->nch, cg->detector_central_col,
                                     cg->detector_pixel_size_col, cg->distance_source_to_detector, 0);
   if (!ce) ce = cudaDeviceSynchronize();
@@ -405,9 +444,17 @@ WFBP_API int wfbp_query(const wfbp_ctx* ctx, wfbp_dims* d) {
   d->precision = ctx->ext.precision;
   const size_t samples = (size_t)ctx->V * ctx->nr * ctx->nch;
   d->raw_bytes = sizeof(float) * (size_t)ctx->n_readings * ctx->raw_rows * ctx->raw_ch;
-  d->rebinned_bytes = sizeof(float) * samples;
-  d->filtered_bytes = sizeof(float) * samples;
-  d->row_scale_bytes = 0;
+  const size_t M = (size_t)ctx->V * ctx->nr;
+  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
+    // split BF16 planes [2][M][kp] followed by the FP32 row scales [M]
+    d->rebinned_bytes = 2 * M * (size_t)ctx->tc_kp * sizeof(uint16_t) + M * sizeof(float);
+    d->filtered_bytes = sizeof(uint16_t) * samples;
+    d->row_scale_bytes = M * sizeof(float);
+  } else {
+    d->rebinned_bytes = sizeof(float) * samples;
+    d->filtered_bytes = sizeof(float) * samples;
+    d->row_scale_bytes = 0;
+  }
   d->native_volume_bytes = sizeof(float) * (size_t)ctx->nz * ctx->nx * ctx->ny;
   d->volume_bytes = sizeof(float) * (size_t)ctx->nzr * ctx->nx * ctx->ny;
   return WFBP_OK;
@@ -435,6 +482,18 @@ WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table
   return WFBP_OK;
 }
 
+WFBP_API int wfbp_check_device_status(wfbp_ctx* ctx) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  DeviceGuard g(ctx->device);
+  int h = 0;
+  CUDA_TRY(ctx, cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h != 0) {
+    cudaMemset(ctx->d_err, 0, sizeof(int));
+    return fail(ctx, h, "a bounded device-side wait gave up (tensor-core filter pipeline)");
+  }
+  return WFBP_OK;
+}
+
 WFBP_API int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* requested_z) {
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (native_z) std::copy(ctx->z_native.begin(), ctx->z_native.end(), native_z);
@@ -456,15 +515,30 @@ WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* s
   p.nch = ctx->nch;
   p.dth = 2.0f * 3.14159265f / (float)ctx->P;  // cuda_kernels.cuh:15
   p.q8 = ctx->ext.tex_weights ? 1 : 0;
-  CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream));
+  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
+    const size_t M = (size_t)ctx->V * ctx->nr;
+    float* scales = reinterpret_cast<float*>(static_cast<uint8_t*>(rebinned) + 2 * M * (size_t)ctx->tc_kp * 2);
+    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, scales, ctx->d_chan_beta, ctx->d_chan_bidx, p, ctx->tc_kp,
+                                     ctx->taps_l1, (cudaStream_t)stream));
+  } else {
+    CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream));
+  }
   return WFBP_OK;
 }
 
 WFBP_API int wfbp_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* row_scales, void* stream) {
-  (void)row_scales;
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (!rebinned || !filtered) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: null buffer");
   DeviceGuard g(ctx->device);
+  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
+    if (!row_scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: mixed precision needs row_scales");
+    const int M = ctx->V * ctx->nr;
+    const float* sc_in = reinterpret_cast<const float*>(static_cast<const uint8_t*>(rebinned) +
+                                                        2 * (size_t)M * (size_t)ctx->tc_kp * 2);
+    CUDA_TRY(ctx, launch_filter_tc(rebinned, ctx->d_bplanes, M, ctx->nch, ctx->tc_kp, ctx->tc_np, ctx->tc_bn, nullptr,
+                                   (__half*)filtered, sc_in, row_scales, ctx->d_err, (cudaStream_t)stream));
+    return WFBP_OK;
+  }
   CUDA_TRY(ctx, launch_filter_f32((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
                                   ctx->nch, (cudaStream_t)stream));
   return WFBP_OK;
@@ -472,12 +546,17 @@ WFBP_API int wfbp_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, fl
 
 WFBP_API int wfbp_backproject(wfbp_ctx* ctx, const void* filtered, const float* row_scales, float* vol,
                               unsigned long long* update_count, void* stream) {
-  (void)row_scales;
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (!filtered || !vol) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject: null buffer");
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_backproject: wfbp_set_views not called");
   DeviceGuard g(ctx->device);
   BPParams p = bp_params(ctx);
+  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
+    if (!row_scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject: mixed precision needs row_scales");
+    CUDA_TRY(ctx, launch_backproject_f16((const __half*)filtered, row_scales, vol, ctx->d_view_sc, ctx->d_view_z,
+                                         ctx->d_z_native, p, update_count, (cudaStream_t)stream));
+    return WFBP_OK;
+  }
   CUDA_TRY(ctx, launch_backproject_f32((const float*)filtered, vol, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p,
                                        update_count, (cudaStream_t)stream));
   return WFBP_OK;
@@ -499,6 +578,7 @@ int ensure_scratch(wfbp_ctx* ctx) {
   if (!ctx->s_rebinned) CUDA_TRY(ctx, cudaMalloc(&ctx->s_rebinned, d.rebinned_bytes));
   if (!ctx->s_filtered) CUDA_TRY(ctx, cudaMalloc(&ctx->s_filtered, d.filtered_bytes));
   if (!ctx->s_vol_native) CUDA_TRY(ctx, cudaMalloc(&ctx->s_vol_native, d.native_volume_bytes));
+  if (!ctx->s_scales && d.row_scale_bytes) CUDA_TRY(ctx, cudaMalloc(&ctx->s_scales, d.row_scale_bytes));
   return WFBP_OK;
 }
 }  // namespace
@@ -530,7 +610,7 @@ WFBP_API int wfbp_run_host(wfbp_ctx* ctx, const float* raw_host, float* vol_host
   if (st) return st;
   CUDA_TRY(ctx, cudaMemcpyAsync(vol_host, ctx->s_vol, d.volume_bytes, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(ctx, cudaStreamSynchronize(s));
-  return WFBP_OK;
+  return wfbp_check_device_status(ctx);
 }
 
 // ---------------------------------------------------------------------------

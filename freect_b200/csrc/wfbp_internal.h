@@ -66,6 +66,12 @@ struct wfbp_ctx {
   float* d_thick_w = nullptr;
   float* d_thick_ws = nullptr;      // [nzr] sum of weights
 
+  // mixed precision: Toeplitz operand planes for the tensor-core filter
+  int tc_kp = 0, tc_np = 0, tc_bn = 0;
+  float taps_l1 = 0.0f;             // sum over |d| < nch of |h[d]|
+  void* d_bplanes = nullptr;        // bf16 [2][tc_np][tc_kp]
+  int* d_err = nullptr;             // device-side error word (bounded waits)
+
   // context-owned scratch for wfbp_run / wfbp_run_host
   void* s_rebinned = nullptr;
   void* s_filtered = nullptr;
@@ -89,6 +95,15 @@ cudaError_t launch_filter_f32(const float* x, float* y, const float* d_taps, lon
 cudaError_t launch_backproject_f32(const float* D, float* vol, const float2* sc, const float* vz,
                                    const float* zs, const BPParams& p, unsigned long long* count,
                                    cudaStream_t s);
+cudaError_t launch_backproject_f16(const __half* D, const float* scales, float* vol, const float2* sc,
+                                   const float* vz, const float* zs, const BPParams& p, unsigned long long* count,
+                                   cudaStream_t s);
+cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, const float* d_beta,
+                               const float* d_bidx, const RebinParams& p, int kp, float taps_l1, cudaStream_t s);
+cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
+                             float* y32, __half* y16, const float* row_scale_in, float* row_scale_out, int* err,
+                             cudaStream_t s);
+int tc_choose_bn(int nch);
 cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
                            const float* ws, int nxy, int nzr, cudaStream_t s);
 cudaError_t launch_synth(const wfbp_synth_scan& scan, const wfbp_ellipsoid* d_e, int ne, float* out,

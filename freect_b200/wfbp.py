@@ -33,6 +33,7 @@ _PROTOS = {
     "wfbp_set_views": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "wfbp_get_slices": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "wfbp_last_error": (C.c_char_p, [_VP]),
+    "wfbp_check_device_status": (C.c_int, [_VP]),
     "wfbp_status_string": (C.c_char_p, [C.c_int]),
     "wfbp_rebin": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_filter": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
@@ -185,6 +186,9 @@ class Context:
         except Exception:
             pass
 
+    def check_device_status(self):
+        _check(self._lib.wfbp_check_device_status(self._h), "wfbp_check_device_status", self._h)
+
     @property
     def handle(self):
         return self._h
@@ -243,9 +247,11 @@ class Context:
         if what == "raw":
             return torch.empty((d.n_readings, d.raw_rows, d.raw_channels), dtype=torch.float32, device=dev)
         if what == "rebinned":
-            return torch.empty(d.rebinned_bytes // 4, dtype=torch.float32, device=dev)
+            return torch.empty((d.rebinned_bytes + 3) // 4, dtype=torch.float32, device=dev)
         if what == "filtered":
-            return torch.empty(d.filtered_bytes // 4, dtype=torch.float32, device=dev)
+            if d.precision == 1:
+                return torch.empty((d.n_views, d.n_rows, d.n_channels), dtype=torch.float16, device=dev)
+            return torch.empty((d.n_views, d.n_rows, d.n_channels), dtype=torch.float32, device=dev)
         if what == "row_scales":
             return torch.empty(max(d.row_scale_bytes // 4, 1), dtype=torch.float32, device=dev)
         if what == "native":

@@ -232,6 +232,12 @@ int wfbp_set_views(wfbp_ctx* ctx, const float* tube_angles, const float* table_p
 /* Copies the native / requested slice z lists (as wfbp_slice_locations). */
 int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* requested_z);
 
+/* Reads and clears the context's device-side error word, which kernels
+ * with bounded waits set instead of hanging (synchronous). Returns
+ * WFBP_ERR_TIMEOUT if a wait gave up since the last check. No counterpart
+ * in the reference, which has no device-side waits. */
+int wfbp_check_device_status(wfbp_ctx* ctx);
+
 /* Last error message of this context (never NULL). */
 const char* wfbp_last_error(const wfbp_ctx* ctx);
 const char* wfbp_status_string(int status);

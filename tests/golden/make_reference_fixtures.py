@@ -9,7 +9,8 @@ and stores inputs and outputs as .npz files:
   ref_<case>.npz   raw frames, tube angles, table positions, the reference's
                    filtered projections, native volume and final volume
   tex_probe.npz    hardware bilinear texture samples at random coordinates
-                   (pins the texture unit's fractional-weight rounding)
+  tex_ramp.npz     samples of ramp textures on a fine grid of coordinates:
+                   the texture unit's effective fractional weights
 
 Usage (needs a GPU): python tests/golden/make_reference_fixtures.py [outdir]
 """
@@ -90,6 +91,25 @@ def tex_probe(lib, seed=5, w=37, h=23, n=20000):
     return dict(img=img, xy=xy, out=out)
 
 
+def tex_ramp_probe(lib, w=16, h=16, steps=4096):
+    """Ramp textures T = i (along x) and T = j (along y), sampled on a fine
+    grid of fractional coordinates: the outputs are the texture unit's
+    effective interpolation weights."""
+    ramp_x = np.tile(np.arange(w, dtype=np.float32), (h, 1))
+    ramp_y = np.tile(np.arange(h, dtype=np.float32)[:, None], (1, w))
+    f = (np.arange(steps, dtype=np.float64) / steps).astype(np.float32)
+    xs = (np.float32(5.5) + f).astype(np.float32)
+    xy_x = np.stack([xs, np.full(steps, 7.75, np.float32)], 1)
+    xy_y = np.stack([np.full(steps, 7.75, np.float32), xs], 1)
+    ox = np.zeros(steps, np.float32)
+    oy = np.zeros(steps, np.float32)
+    if lib.ref_shim_tex_probe(O.fp(ramp_x), w, h, O.fp(np.ascontiguousarray(xy_x)), steps, O.fp(ox)) != 0:
+        raise RuntimeError("tex ramp probe x failed")
+    if lib.ref_shim_tex_probe(O.fp(ramp_y), w, h, O.fp(np.ascontiguousarray(xy_y)), steps, O.fp(oy)) != 0:
+        raise RuntimeError("tex ramp probe y failed")
+    return dict(coord=xs, out_x=ox, out_y=oy)
+
+
 def main(outdir):
     os.makedirs(outdir, exist_ok=True)
     lib = load_shim()
@@ -99,6 +119,7 @@ def main(outdir):
         np.savez_compressed(os.path.join(outdir, "ref_%s.npz" % name), **res)
         print(name, spec.V, spec.nr, spec.nch, res["volume"].shape, float(np.nanmean(res["volume"])))
     np.savez_compressed(os.path.join(outdir, "tex_probe.npz"), **tex_probe(lib))
+    np.savez_compressed(os.path.join(outdir, "tex_ramp.npz"), **tex_ramp_probe(lib))
     print("wrote", outdir)
 
 

@@ -45,12 +45,15 @@ def test_fixtures_present():
     assert os.path.exists(os.path.join(GOLD, "tex_probe.npz"))
 
 
-def test_texture_unit_weights_are_8bit_round_to_nearest():
+def test_texture_unit_weights_closest_to_8bit_round_to_nearest():
+    # Among simple models of the texture unit's linear filter, 8-bit
+    # round-to-nearest fractional weights are closest to the hardware; none
+    # is exact (residual ~2e-3 RMS on unit-variance texels).
     d = np.load(os.path.join(GOLD, "tex_probe.npz"))
     img, xy, hw = d["img"], d["xy"], d["out"]
-    err = {r: np.abs(tex_emulate(img, xy, r) - hw).max() for r in ("nearest", "truncate", "exact")}
-    assert err["nearest"] < 2e-3, err
-    assert err["nearest"] <= err["truncate"] and err["nearest"] < err["exact"], err
+    rms = {r: float(np.sqrt(np.mean((tex_emulate(img, xy, r) - hw) ** 2))) for r in ("nearest", "truncate", "exact")}
+    assert rms["nearest"] < rms["exact"] < rms["truncate"], rms
+    assert rms["nearest"] < 3e-3, rms
 
 
 def _spec_for(name):
@@ -65,18 +68,32 @@ def test_oracle_transcript_matches_reference_kernels(orc, path):
     d = np.load(path)
     raw = d["raw"]
     cg, gp = orc.configure_geometry(spec.meta(), d["table"])
+    tube, table = spec.views()
+    assert np.array_equal(tube, d["tube"]) and np.array_equal(table, d["table"])
+    # (1) backprojection transcript on the reference's own filtered rows:
+    #     equal to the reference kernel to FP32 rounding
+    rp = spec.recon_config()
+    zn, zr = orc.slice_locations(cg, rp)
+    assert np.array_equal(zn, d["z_native"]) and np.array_equal(zr, d["z_req"])
+    gp.n_slices_native, gp.n_slices_requested = zn.size, zr.size
+    vn = orc.backproject_ref32(cg, rp, gp, d["filtered"], tube, table, zn)
+    rms, mx, n = orc.hu_error(vn, d["native"])
+    assert np.array_equal(np.isnan(vn), np.isnan(d["native"]))  # same voxels without coverage
+    assert n == np.isfinite(vn).sum() and rms < 0.005 and mx < 0.05, (rms, mx)
+    vol = orc.thicken_ref32(rp, d["native"], zn, zr)
+    assert np.allclose(vol, d["volume"], rtol=1e-5, atol=1e-7, equal_nan=True)
+    # (2) rebin + filter: the texture unit's filter is modelled by 8-bit
+    #     round-to-nearest weights (not exact; see the probe test above)
     filt = orc.rebin_filter_ref32(cg, raw, d["taps_fft"], q8=True)
     scale = np.abs(d["filtered"]).max()
-    diff = np.abs(filt - d["filtered"])
-    # cuFFT's FP32 rounding vs the oracle's double FFT, plus rare texel
-    # fraction flips from asinf/contraction ulps
-    assert np.mean(diff < 1e-5 * scale) > 0.999
-    assert diff.max() < 2e-3 * scale
+    rel = np.abs(filt - d["filtered"]) / scale
+    assert rel.max() < 5e-3 and np.percentile(rel, 99) < 1e-3
+    # (3) whole path within a fraction of the parity budget (0.5 HU RMS / 2 HU max)
     ref = orc.reconstruct_ref32(spec, raw, taps_half=None, q8=True)
     rms, mx, n = orc.hu_error(ref["volume"], d["volume"])
-    assert n == d["volume"].size
-    assert rms < 0.05 and mx < 0.5, (rms, mx)
-    # and the exact-weight FP64 oracle is within the parity budget of the reference
+    assert n == np.isfinite(d["volume"]).sum()
+    assert rms < 0.25 and mx < 1.0, (rms, mx)
+    # exact weights (the FP64 oracle) miss the 2 HU max budget on some inputs
     r64 = orc.reconstruct_f64(spec, raw)
     rms64, mx64, _ = orc.hu_error(r64["volume"], d["volume"])
     assert rms64 < 0.5, (rms64, mx64)

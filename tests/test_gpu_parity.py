@@ -51,8 +51,9 @@ def test_rebin_matches_oracle(orc, tiny, q8):
     ref = orc.rebin_ref32(cg, raw, q8=bool(q8))
     scale = np.abs(ref).max()
     d = np.abs(got - ref)
-    # identical formula; contraction / asinf ulps can move a texel fraction
-    assert np.mean(d < 1e-5 * scale) > 0.999
+    # identical formula; contraction / asinf ulps can move a texel fraction,
+    # which with 8-bit weights is a full 1/256 step
+    assert np.mean(d < 1e-5 * scale) > (0.99 if q8 else 0.999)
     assert d.max() < (1.0 / 128 if q8 else 1e-3) * scale
     ref64 = orc.rebin_f64(cg, raw)
     if not q8:
@@ -223,6 +224,8 @@ def test_fp32_form_vs_reference_kernels(orc, path):
     vol = ctx.alloc("volume")
     ctx.run(dev(d["raw"]), vol)
     torch.cuda.synchronize()
-    rms, mx, n = orc.hu_error(vol.cpu().numpy(), d["volume"])
-    assert n == d["volume"].size
+    got = vol.cpu().numpy()
+    rms, mx, n = orc.hu_error(got, d["volume"])
+    assert np.array_equal(np.isnan(got), np.isnan(d["volume"]))
+    assert n == np.isfinite(d["volume"]).sum()
     assert rms <= 0.5 and mx <= 2.0, (rms, mx)
