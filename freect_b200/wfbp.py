@@ -41,6 +41,7 @@ _PROTOS = {
     "wfbp_thicken": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_run": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_run_host": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_run_static": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_synth_project": (C.c_int, [C.POINTER(T.SynthScan), C.POINTER(T.Ellipsoid), C.c_int, _VP, _VP]),
 }
 
@@ -225,6 +226,12 @@ class Context:
 
     def run(self, raw, volume, stream=None):
         _check(self._lib.wfbp_run(self._h, _dptr(raw), _dptr(volume), _stream(stream)), "wfbp_run", self._h)
+
+    def run_static(self, raw, volume, stream=None):
+        """wfbp_run with the intermediates in the library's static device
+        array (no allocation; small geometries only)."""
+        _check(self._lib.wfbp_run_static(self._h, _dptr(raw), _dptr(volume), _stream(stream)), "wfbp_run_static",
+               self._h)
 
     def run_host(self, raw_host, volume_host=None, stream=None):
         """raw_host: float32 array (numpy or pinned torch CPU tensor); returns the volume."""

@@ -275,6 +275,30 @@ int wfbp_thicken(wfbp_ctx* ctx, const float* volume_native, float* volume, void*
  * raw (device) -> volume (device), with context-owned intermediates. */
 int wfbp_run(wfbp_ctx* ctx, const float* raw, float* volume, void* stream);
 
+/* wfbp_run without any device allocation. No counterpart in the reference.
+ *
+ * wfbp_run allocates its intermediates (rebinned rows, filtered rows, row
+ * scales, native-thickness volume) with cudaMalloc on first use. Callers that
+ * must not allocate -- an application whose device memory all belongs to its
+ * own pool or caching allocator, a scanner pipeline held to a fixed memory
+ * budget fixed at start-up, a latency-critical loop that cannot take
+ * cudaMalloc's implicit synchronisation -- call this instead: the
+ * intermediates live in one static device array of WFBP_STATIC_SCRATCH_BYTES
+ * that every GPU which loads the library holds until the process exits.
+ *   - Geometries whose intermediates exceed WFBP_STATIC_SCRATCH_BYTES are
+ *     rejected with WFBP_ERR_INVALID_ARG and a message (wfbp_last_error).
+ *   - The first call on a device looks up the array's device address on that
+ *     device (cudaGetSymbolAddress); make that first call before any stream
+ *     capture begins.
+ *   - All calls on one device share the array: calls that overlap on the GPU
+ *     (other streams, other contexts, other threads) race; serialise them.
+ *   - Each stage overwrites its whole region, so no state carries over from
+ *     the previous call.
+ * The context itself is created (and allocates its tables) beforehand with
+ * wfbp_ctx_create; this call allocates nothing. */
+#define WFBP_STATIC_SCRATCH_BYTES (32u << 20)
+int wfbp_run_static(wfbp_ctx* ctx, const float* raw, float* volume, void* stream);
+
 /* RunReconstruction from host memory: H2D of the raw readings, the four
  * stages, D2H of the final volume (ReconstructionMachine.cu:246,423),
  * synchronous on return. Pinned host buffers overlap the copies with the
