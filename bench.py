@@ -225,7 +225,8 @@ def main():
     cg, gp = wfbp.configure_geometry(spec.meta(), table)
     rp = spec.recon_config()
     prec = T.PRECISION_MIXED if args.precision == "mixed" else T.PRECISION_FP32
-    ext = wfbp.make_ext(precision=prec, filter_window=spec.window, tex_weights=1 if prec == T.PRECISION_FP32 else 0)
+    ext = wfbp.make_ext(precision=prec, filter_window=spec.window, tex_weights=1 if prec == T.PRECISION_FP32 else 0,
+                        filtered_layout=T.LAYOUT_BACKPROJECTION)
     ctx = wfbp.Context(cg, rp, ext, device=local)
     ctx.set_views(tube, table)
     d = ctx.dims

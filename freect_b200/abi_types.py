@@ -107,7 +107,8 @@ class Ext(C.Structure):
         ("n_user_taps", C.c_int),
         ("tex_weights", C.c_int),
         ("bp_slab", C.c_int),
-        ("reserved", C.c_int * 7),
+        ("filtered_layout", C.c_int),
+        ("reserved", C.c_int * 6),
     ]
 
 
@@ -158,9 +159,6 @@ class SynthScan(C.Structure):
         ("i0", C.c_double),
         ("seed", C.c_ulonglong),
         ("ffs_mode", C.c_int),
-        ("ffs_dphi", C.c_double),
-        ("ffs_dz", C.c_double),
-        ("ffs_dr", C.c_double),
     ]
 
 
@@ -174,4 +172,6 @@ FILTER_REFERENCE = 0
 FILTER_SHEPP_LOGAN = 1
 FILTER_USER = 2
 FFS_NONE, FFS_PHI, FFS_Z, FFS_PHIZ = 0, 1, 2, 3
+LAYOUT_REFERENCE = 0
+LAYOUT_BACKPROJECTION = 1
 EXT_VERSION = 1

@@ -34,12 +34,11 @@ constexpr uint32_t TC_TMEM_COLS = 256;
 constexpr long long SPIN_LIMIT = 1ll << 26;
 
 struct TcParams {
-  int M;          // rows of X (V * nr)
+  int M;          // rows of X (V * nrv)
   int nch;        // valid output channels
   int BN;         // N tile
   int kblocks;    // Kp / 64
   int np;         // padded N (rows of one B plane)
-  int out_fp16;   // 1: FP16 + row scales, 0: FP32
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -116,8 +115,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcParams p,
-              float* __restrict__ y32, __half* __restrict__ y16, const float* __restrict__ row_scale,
-              float* __restrict__ row_scale_out, int* __restrict__ err) {
+              TcOutArgs o, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t a_bytes = TC_BM * TC_BK * 2;          // 16 KB per plane
@@ -128,6 +126,7 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   uint64_t* done = empty + TC_STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   __shared__ int s_fail;
+  __shared__ float s_xchg[4][16];  // row 32w of each warp, for the pairs of the warp above
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * p.BN;
@@ -204,34 +203,60 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   __syncthreads();
   const bool failed = *((volatile int*)&s_fail) != 0;
   if (!failed) {
+    // row m of the tile: view v = m / nrv, row i = m % nrv (rows i >= nr are zero padding)
     const int m = m0 + warp * 32 + lane;
+    const int v = m / o.nrv, i = m % o.nrv;
+    const bool row_ok = m < p.M && i < o.nr;
+    float inv = 1.0f;
+    if (o.mode == TC_OUT_F16_ROWS && row_ok) {
+      inv = 1.0f / o.row_scale_in[m];
+      if (blockIdx.y == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
+    } else if (o.mode == TC_OUT_PAIRS && m < p.M) {
+      inv = 1.0f / o.view_scale[v];
+    }
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    const float inv = (p.out_fp16 && m < p.M) ? 1.0f / row_scale[m] : 1.0f;
-    if (p.out_fp16 && blockIdx.y == 0 && m < p.M && row_scale_out) row_scale_out[m] = row_scale[m];
     for (int c = 0; c < p.BN; c += 16) {
-      float v[16];
-      tmem_ld16(trow + (uint32_t)c, v);
+      float val[16];
+      tmem_ld16(trow + (uint32_t)c, val);
       const int n = n0 + c;
-      if (m >= p.M || n >= p.nch) continue;
-      if (p.out_fp16) {
-        __half* dst = y16 + (size_t)m * p.nch + n;
+      if (o.mode == TC_OUT_PAIRS) {
+        // partner row i + 1 lives in the next lane, or in lane 0 of the next warp
+        if (lane == 0) {
+#pragma unroll
+          for (int k = 0; k < 16; k++) s_xchg[warp][k] = val[k];
+        }
+        __syncthreads();
+        float nxt[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+          const float dn = __shfl_down_sync(0xffffffffu, val[k], 1);
+          nxt[k] = lane < 31 ? dn : (warp < 3 ? s_xchg[warp + 1][k] : 0.0f);
+        }
+        __syncthreads();
+        if (row_ok) {
+          const bool last = (i == o.nr - 1);
+          for (int k = 0; k < 16 && n + k < p.nch; k++) {
+            const __half2 h = __floats2half2_rn(val[k] * inv, last ? 0.0f : nxt[k] * inv);
+            o.pairs[((size_t)v * p.nch + (n + k)) * o.nrp + i] = *reinterpret_cast<const uint32_t*>(&h);
+          }
+        }
+        continue;
+      }
+      if (!row_ok || n >= p.nch) continue;
+      if (o.mode == TC_OUT_F16_ROWS) {
+        __half* dst = o.y16 + ((size_t)v * o.nr + i) * p.nch + n;
         if (n + 16 <= p.nch && ((p.nch & 7) == 0)) {
           __align__(16) __half h[16];
 #pragma unroll
-          for (int i = 0; i < 16; i++) h[i] = __float2half_rn(v[i] * inv);
+          for (int k = 0; k < 16; k++) h[k] = __float2half_rn(val[k] * inv);
           reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<uint4*>(h)[0];
           reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<uint4*>(h)[1];
         } else {
-          for (int i = 0; i < 16 && n + i < p.nch; i++) dst[i] = __float2half_rn(v[i] * inv);
+          for (int k = 0; k < 16 && n + k < p.nch; k++) dst[k] = __float2half_rn(val[k] * inv);
         }
       } else {
-        float* dst = y32 + (size_t)m * p.nch + n;
-        if (n + 16 <= p.nch && ((p.nch & 3) == 0)) {
-#pragma unroll
-          for (int i = 0; i < 16; i += 4) reinterpret_cast<float4*>(dst)[i / 4] = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-        } else {
-          for (int i = 0; i < 16 && n + i < p.nch; i++) dst[i] = v[i];
-        }
+        float* dst = o.y32 + (size_t)m * p.nch + n;
+        for (int k = 0; k < 16 && n + k < p.nch; k++) dst[k] = val[k];
       }
     }
   } else if (warp == 0 && lane == 0) {
@@ -247,11 +272,9 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+}  // namespace
 
-EncodeTiledFn encode_fn() {
+EncodeTiledFn wfbp_encode_tiled_fn() {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     void* p = nullptr;
@@ -263,9 +286,11 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+namespace {
+
 // 2-D bf16 map over `rows` rows of `kp` elements, box 64 x box_rows, 128B swizzle.
 bool make_map(CUtensorMap* map, const void* base, uint64_t kp, uint64_t rows, uint32_t box_rows) {
-  EncodeTiledFn fn = encode_fn();
+  EncodeTiledFn fn = wfbp_encode_tiled_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {kp, rows};
   cuuint64_t strides[1] = {kp * 2};
@@ -294,8 +319,7 @@ int tc_choose_bn(int nch) {
 
 // a_planes: bf16 [2][M][kp] (hi then lo); b_planes: bf16 [2][np][kp].
 cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
-                             float* y32, __half* y16, const float* row_scale, float* row_scale_out, int* err,
-                             cudaStream_t s) {
+                             const TcOutArgs& out, int* err, cudaStream_t s) {
   if (bn < 16 || bn > 256 || bn % 16 || kp % TC_BK || np % bn) return cudaErrorInvalidValue;
   CUtensorMap ma, mb;
   if (!make_map(&ma, a_planes, (uint64_t)kp, 2ull * M, TC_BM)) return cudaErrorInvalidValue;
@@ -306,11 +330,11 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
   p.BN = bn;
   p.kblocks = kp / TC_BK;
   p.np = np;
-  p.out_fp16 = y16 != nullptr;
+  if (out.nrv < 1 || TC_BM % out.nrv != 0) return cudaErrorInvalidValue;  // views must not straddle M tiles
   size_t smem = tc_smem_bytes(bn);
   cudaError_t e = cudaFuncSetAttribute(k_toeplitz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((M + TC_BM - 1) / TC_BM), (unsigned)(np / bn));
-  k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(ma, mb, p, y32, y16, row_scale, row_scale_out, err);
+  k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(ma, mb, p, out, err);
   return cudaGetLastError();
 }

@@ -80,6 +80,52 @@ __device__ __forceinline__ float rebin_sample(const float* __restrict__ rawrow, 
   return (1.0f - ax) * (1.0f - ay) * t00 + ax * (1.0f - ay) * t10 + (1.0f - ax) * ay * t01 + ax * ay * t11;
 }
 
+// Flying focal spot (no counterpart in the reference's WFBP): readings cycle
+// through G focal states (the state order of fct_icd's generate_ffs_offset,
+// applications/fct_icd/src/generate_system_matrix_ffs.cpp:242-290: phi bit =
+// state & 1, z bit = state >> 1 when both are on). A reading of phi state sp
+// samples effective channels 2b + sp, of z state sz effective rows 2r + sz.
+// The effective fan sample at fractional effective channel bidx is
+// interpolated between the two effective channels around it, each from its
+// own state's readings, linearly in reading angle between that state's
+// neighbouring readings (so no reading is assigned another reading's angle).
+__device__ __forceinline__ float rebin_sample_ffs(const float* __restrict__ raw, const RebinParams& p, float bidx,
+                                                  float beta, int v, int ie) {
+  if (isnan(bidx)) return 0.0f;
+  const int zs = p.zf ? (ie & 1) : 0, iraw = p.zf ? (ie >> 1) : ie;
+  const float* rawrow = raw + (size_t)(p.nr_raw - 1 - iraw) * p.nch_raw;
+  const size_t vs = (size_t)p.nr_raw * p.nch_raw;
+  const float nf = ((float)(p.G * v) * p.dth - beta) / p.dth;  // fractional reading index
+  const float fx = floorf(bidx);
+  float ax = bidx - fx;
+  if (p.q8) ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
+  float val = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int e = min(max((int)fx + t, 0), p.nch - 1);
+    const float we = t ? ax : 1.0f - ax;
+    const int sp = p.phi ? (e & 1) : 0, b = p.phi ? (e >> 1) : e;
+    const int rho = (p.G == 4) ? sp + 2 * zs : (p.phi ? sp : zs);
+    const float mf = (nf - (float)rho) / (float)p.G, m0 = floorf(mf);
+    float ay = mf - m0;
+    if (p.q8) ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
+    const int ma = min(max((int)m0, 0), p.V - 1), mb = min(max((int)m0 + 1, 0), p.V - 1);
+    const float t0 = __ldg(rawrow + (size_t)(p.G * ma + rho) * vs + (p.nch_raw - 1 - b));
+    const float t1 = __ldg(rawrow + (size_t)(p.G * mb + rho) * vs + (p.nch_raw - 1 - b));
+    val += we * ((1.0f - ay) * t0 + ay * t1);
+  }
+  return val;
+}
+
+// One rebinned sample of output view v, row i (flipped row-sheet index),
+// output channel with table entries (bidx, beta).
+__device__ __forceinline__ float sample_at(const float* __restrict__ raw, const RebinParams& p, float bidx, float beta,
+                                           int v, int i) {
+  if (p.G > 1) return rebin_sample_ffs(raw, p, bidx, beta, v, i);
+  return rebin_sample(raw + (size_t)(p.nr - 1 - i) * p.nch, (size_t)p.nr * p.nch, p.V, p.nch, bidx, beta, v, p.dth,
+                      p.q8);
+}
+
 // grid.x covers [V*nr] output rows (REB_ROWS per block), grid.y covers
 // channel quads; each thread writes 4 consecutive channels with one float4.
 constexpr int REB_ROWS = 4;
@@ -100,21 +146,18 @@ k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float*
   const long row = (long)blockIdx.x * REB_ROWS + tr;
   if (row >= (long)p.V * p.nr) return;
   const int v = (int)(row / p.nr), i = (int)(row % p.nr);
-  const float* rawrow = raw + (size_t)(p.nr - 1 - i) * p.nch;
-  const size_t vs = (size_t)p.nr * p.nch;
   const int c = c_base + tq * 4;
   float* o = out + (size_t)row * p.nch;
   if (c + 3 < p.nch && (p.nch & 3) == 0) {
     float4 r;
-    r.x = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 0], s_beta[tq * 4 + 0], v, p.dth, p.q8);
-    r.y = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 1], s_beta[tq * 4 + 1], v, p.dth, p.q8);
-    r.z = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 2], s_beta[tq * 4 + 2], v, p.dth, p.q8);
-    r.w = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + 3], s_beta[tq * 4 + 3], v, p.dth, p.q8);
+    r.x = sample_at(raw, p, s_bidx[tq * 4 + 0], s_beta[tq * 4 + 0], v, i);
+    r.y = sample_at(raw, p, s_bidx[tq * 4 + 1], s_beta[tq * 4 + 1], v, i);
+    r.z = sample_at(raw, p, s_bidx[tq * 4 + 2], s_beta[tq * 4 + 2], v, i);
+    r.w = sample_at(raw, p, s_bidx[tq * 4 + 3], s_beta[tq * 4 + 3], v, i);
     *reinterpret_cast<float4*>(o + c) = r;
   } else {
     for (int u = 0; u < 4; u++)
-      if (c + u < p.nch)
-        o[c + u] = rebin_sample(rawrow, vs, p.V, p.nch, s_bidx[tq * 4 + u], s_beta[tq * 4 + u], v, p.dth, p.q8);
+      if (c + u < p.nch) o[c + u] = sample_at(raw, p, s_bidx[tq * 4 + u], s_beta[tq * 4 + u], v, i);
   }
 }
 
@@ -141,9 +184,12 @@ cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, 
 // htab[d + NTAB] = h[|d|] so the inner loop needs no index arithmetic.
 constexpr int TF_BM = 128, TF_BN = 128, TF_BK = 16;
 
+// TR = true writes the backprojection layout Y_T[view][channel][row] with
+// rows padded to nrp (row m = view * nr + row).
+template <bool TR>
 __global__ void __launch_bounds__(256)
 k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* __restrict__ taps, long M,
-               int nch) {
+               int nch, int nr, int nrp) {
   extern __shared__ float smem[];
   float* As = smem;                          // [TF_BK][TF_BM + 4]
   float* htab = smem + TF_BK * (TF_BM + 4);  // [2*nch + 1], htab[d + nch] = h[|d|]
@@ -197,22 +243,39 @@ k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* 
   for (int i = 0; i < 8; i++) {
     long m = m0 + ty * 8 + i;
     if (m >= M) continue;
+    const long v = m / nr, row = m % nr;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       int n = n0 + tx + 16 * j;
-      if (n < nch) Y[m * nch + n] = acc[i][j];
+      if (n < nch) {
+        if (TR)
+          Y[((size_t)v * nch + n) * nrp + row] = acc[i][j];
+        else
+          Y[m * nch + n] = acc[i][j];
+      }
     }
   }
 }
 
-cudaError_t launch_filter_f32(const float* x, float* y, const float* d_taps, long rows, int nch, cudaStream_t s) {
+template <bool TR>
+cudaError_t launch_toeplitz_f32(const float* x, float* y, const float* d_taps, long rows, int nch, int nr, int nrp,
+                                cudaStream_t s) {
   size_t smem = sizeof(float) * (TF_BK * (TF_BM + 4) + 2 * nch + 1);
   if (smem > 64 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_toeplitz_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(k_toeplitz_f32<TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((rows + TF_BM - 1) / TF_BM), (unsigned)((nch + TF_BN - 1) / TF_BN));
-  k_toeplitz_f32<<<grid, 256, smem, s>>>(x, y, d_taps, rows, nch);
+  k_toeplitz_f32<TR><<<grid, 256, smem, s>>>(x, y, d_taps, rows, nch, nr, nrp);
   return cudaGetLastError();
+}
+
+cudaError_t launch_filter_f32(const float* x, float* y, const float* d_taps, long rows, int nch, cudaStream_t s) {
+  return launch_toeplitz_f32<false>(x, y, d_taps, rows, nch, 1, 1, s);
+}
+
+cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps, long rows, int nch, int nr, int nrp,
+                                 cudaStream_t s) {
+  return launch_toeplitz_f32<true>(x, yt, d_taps, rows, nch, nr, nrp, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -248,58 +311,66 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // ---------------------------------------------------------------------------
 //
 // Same samples as k_rebin_f32, written as the two BF16 operand planes of the
-// tensor-core Toeplitz filter: hi = bf16(x), lo = bf16(x - hi), rows padded
-// with zeros to kp (a multiple of 64). One CTA per detector row also writes
-// the row's FP16 storage scale: the smallest power of two s with
-// max|x| * sum|h| / s <= 16384, which bounds every filtered value of the row
-// (|y| <= sum|h| max|x|) well inside the FP16 range.
+// tensor-core Toeplitz filter: hi = bf16(x), lo = bf16(x - hi). One CTA per
+// view; the view's rows are padded with zero rows to nrv (a power of two that
+// divides the filter's 128-row tile, so no view straddles a tile) and every
+// row with zeros to kp (a multiple of 64). The CTA also writes the FP16
+// storage scales: per row, the smallest power of two s with
+// max|x| * sum|h| / s <= 16384 (|y| <= sum|h| max|x| bounds every filtered
+// value of the row), and per view the largest of its rows' scales.
 constexpr int RS_THREADS = 256;
 
 __global__ void __launch_bounds__(RS_THREADS)
 k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
-              float* __restrict__ row_scale, const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
-              RebinParams p, int kp, float taps_l1) {
-  __shared__ float s_red[RS_THREADS / 32];
-  const long row = blockIdx.x;
-  const int v = (int)(row / p.nr), i = (int)(row % p.nr);
-  const float* rawrow = raw + (size_t)(p.nr - 1 - i) * p.nch;
-  const size_t vs = (size_t)p.nr * p.nch;
-  float amax = 0.0f;
-  for (int q = threadIdx.x; q < kp / 4; q += RS_THREADS) {
-    const int c = q * 4;
-    float x[4];
+              float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
+              const float* __restrict__ bidx_t, RebinParams p, int kp, int nrv, float taps_l1) {
+  extern __shared__ float s_rowmax[];  // [nrv]
+  const int v = blockIdx.x;
+  for (int i = threadIdx.x; i < nrv; i += RS_THREADS) s_rowmax[i] = 0.0f;
+  __syncthreads();
+  const int quads = kp / 4;
+  for (int e = threadIdx.x; e < nrv * quads; e += RS_THREADS) {
+    const int i = e / quads, c = (e % quads) * 4;
+    float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (i < p.nr) {
 #pragma unroll
-    for (int u = 0; u < 4; u++)
-      x[u] = (c + u < p.nch) ? rebin_sample(rawrow, vs, p.V, p.nch, __ldg(bidx_t + c + u), __ldg(beta_t + c + u), v,
-                                            p.dth, p.q8)
-                             : 0.0f;
+      for (int u = 0; u < 4; u++)
+        if (c + u < p.nch) x[u] = sample_at(raw, p, __ldg(bidx_t + c + u), __ldg(beta_t + c + u), v, i);
+    }
     __align__(8) __nv_bfloat16 hi[4], lo[4];
+    float amax = 0.0f;
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       hi[u] = __float2bfloat16_rn(x[u]);
       lo[u] = __float2bfloat16_rn(x[u] - __bfloat162float(hi[u]));
       amax = fmaxf(amax, fabsf(x[u]));
     }
-    *reinterpret_cast<uint2*>(a_hi + (size_t)row * kp + c) = *reinterpret_cast<uint2*>(hi);
-    *reinterpret_cast<uint2*>(a_lo + (size_t)row * kp + c) = *reinterpret_cast<uint2*>(lo);
+    const size_t row = (size_t)v * nrv + i;
+    *reinterpret_cast<uint2*>(a_hi + row * kp + c) = *reinterpret_cast<uint2*>(hi);
+    *reinterpret_cast<uint2*>(a_lo + row * kp + c) = *reinterpret_cast<uint2*>(lo);
+    if (amax > 0.0f) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), __float_as_int(amax));  // amax >= 0
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x / 32] = amax;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    float m = 0.0f;
-    for (int w = 0; w < RS_THREADS / 32; w++) m = fmaxf(m, s_red[w]);
-    float bound = fmaxf(m * taps_l1, 1e-30f) * (1.0f / 16384.0f);
-    row_scale[row] = exp2f(ceilf(log2f(bound)));
+  __shared__ float s_vmax;
+  if (threadIdx.x == 0) s_vmax = 0.0f;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nrv; i += RS_THREADS) {
+    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
+    const float sc = exp2f(ceilf(log2f(bound)));
+    row_scale[(size_t)v * nrv + i] = sc;
+    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
   }
+  __syncthreads();
+  if (threadIdx.x == 0) view_scale[v] = s_vmax;
 }
 
-cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, const float* d_beta,
-                               const float* d_bidx, const RebinParams& p, int kp, float taps_l1, cudaStream_t s) {
-  const long rows = (long)p.V * p.nr;
+cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
+                               const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
+                               float taps_l1, cudaStream_t s) {
+  const size_t rows = (size_t)p.V * nrv;
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
-  __nv_bfloat16* lo = hi + (size_t)rows * kp;
-  k_rebin_split<<<(unsigned)rows, RS_THREADS, 0, s>>>(raw, hi, lo, row_scale, d_beta, d_bidx, p, kp, taps_l1);
+  __nv_bfloat16* lo = hi + rows * kp;
+  k_rebin_split<<<(unsigned)p.V, RS_THREADS, sizeof(float) * nrv, s>>>(raw, hi, lo, row_scale, view_scale, d_beta,
+                                                                       d_bidx, p, kp, nrv, taps_l1);
   return cudaGetLastError();
 }

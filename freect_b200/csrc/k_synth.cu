@@ -58,31 +58,31 @@ __global__ void k_synth(wfbp_synth_scan s, int ne, float* __restrict__ out) {
   const int r = (int)(row % s.rows);
   const long v = row / s.rows;
   const int nch = s.channels, nr = s.rows;
+  // flying focal spot: reading v of focal state (sp, sz) samples effective
+  // channel 2b + sp and effective row 2rr + sz of a detector with twice the
+  // channels / rows at half the spacing and central channel 2 c0 + 1/2
+  const int phi = (s.ffs_mode & WFBP_FFS_PHI) != 0, zf = (s.ffs_mode & WFBP_FFS_Z) != 0;
+  const int G = (phi ? 2 : 1) * (zf ? 2 : 1);
+  const int rho = (int)(v % G);
+  const int spf = phi ? (G == 4 ? (rho & 1) : rho) : 0, szf = zf ? (G == 4 ? (rho >> 1) : rho) : 0;
+  const int nche = phi ? 2 * nch : nch, nre = zf ? 2 * nr : nr;
+  const double c0e = phi ? 2.0 * s.central_channel + 0.5 : s.central_channel;
+  const double dcole = phi ? 0.5 * s.dcol : s.dcol, drowe = zf ? 0.5 * s.drow : s.drow;
   const double R = s.sid;
-  const double ds = s.dcol * R / s.sdd;
-  const double delta = nch + 1.75 - 2.0 * s.central_channel;
+  const double ds = dcole * R / s.sdd;
+  const double delta = nche + 1.75 - 2.0 * c0e;
   const int b = nch - 1 - k, rr = nr - 1 - r;
-  const double beta = (b - s.central_channel) * s.dcol / s.sdd;
-  double ang = s.angle0 + v * s.dangle;
-  double zs = s.z0 + v * s.dz;
-  double dphi = 0.0, dzf = 0.0, dr = 0.0;
-  if (s.ffs_mode != WFBP_FFS_NONE) {
-    int phase = (s.ffs_mode == WFBP_FFS_PHIZ) ? (int)(v % 4) : (int)(v % 2);
-    int sa = 0, sz = 0;
-    if (s.ffs_mode == WFBP_FFS_PHI) sa = phase ? 1 : -1;
-    if (s.ffs_mode == WFBP_FFS_Z) sz = phase ? 1 : -1;
-    if (s.ffs_mode == WFBP_FFS_PHIZ) { sa = (phase & 1) ? 1 : -1; sz = (phase & 2) ? 1 : -1; }
-    dphi = sa * s.ffs_dphi; dzf = sz * s.ffs_dz; dr = sz * s.ffs_dr;
-  }
-  const double Reff = R + dr;
-  ang += dphi / R;
+  const int be = phi ? 2 * b + spf : b, rre = zf ? 2 * rr + szf : rr;
+  const double beta = (be - c0e) * dcole / s.sdd;
+  const double ang = s.angle0 + v * s.dangle;
+  const double zs = s.z0 + v * s.dz;
   const double theta = ang - beta;
   double sn, cs;
   sincos(theta, &sn, &cs);
-  const double pstar = delta * ds - Reff * sin(beta);
-  const double tt = sqrt(Reff * Reff - pstar * pstar);
-  const double S0 = pstar * sn + tt * cs, S1 = -pstar * cs + tt * sn, S2 = zs + dzf;
-  const double U0 = -cs, U1 = -sn, U2 = (rr - (nr - 1) / 2.0) * s.drow / s.sdd;
+  const double pstar = delta * ds - R * sin(beta);
+  const double tt = sqrt(R * R - pstar * pstar);
+  const double S0 = pstar * sn + tt * cs, S1 = -pstar * cs + tt * sn, S2 = zs;
+  const double U0 = -cs, U1 = -sn, U2 = (rre - (nre - 1) / 2.0) * drowe / s.sdd;
   const double unorm = sqrt(U0 * U0 + U1 * U1 + U2 * U2);
   double p = 0.0;
   for (int n = 0; n < ne; n++) {

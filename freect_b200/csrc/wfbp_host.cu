@@ -81,6 +81,35 @@ int slice_lists(const CTGeometry* cg, const ReconConfig* rp, std::vector<float>&
   return WFBP_OK;
 }
 
+// Effective geometry of a flying-focal-spot scan: readings cycle through G
+// focal states (fct_icd's order, applications/fct_icd/src/
+// generate_system_matrix_ffs.cpp:242-290); one view per G readings, 2x
+// channels (phi) / rows (z) at half the spacing, central channel 2 c0 + 1/2.
+void ffs_effective(const CTGeometry* in, CTGeometry* out) {
+  *out = *in;
+  const int fp = in->ffs_phi ? 2 : 1, fz = in->ffs_z ? 2 : 1, G = fp * fz;
+  out->total_number_of_projections = in->total_number_of_projections / G;
+  out->projections_per_rotation = in->projections_per_rotation / G;
+  out->num_detector_cols = in->num_detector_cols * fp;
+  out->num_detector_cols_padded = 2 * out->num_detector_cols;
+  out->num_detector_cols_padded_fft = next_pow2_at_least(2 * out->num_detector_cols);
+  out->num_detector_rows = in->num_detector_rows * fz;
+  out->num_detector_rows_padded = 2 * out->num_detector_rows;
+  out->detector_pixel_size_col = in->detector_pixel_size_col / fp;
+  out->detector_pixel_size_row = in->detector_pixel_size_row / fz;
+  out->detector_central_col = in->ffs_phi ? 2.0f * in->detector_central_col + 0.5f : in->detector_central_col;
+  out->detector_central_row = ((float)out->num_detector_rows - 1.0f) / 2.0f;
+  out->collimated_slice_width =
+      out->distance_source_to_isocenter * (out->detector_pixel_size_row / out->distance_source_to_detector);
+  const float cone_offset = ((float)(out->num_detector_rows - 1)) / 2.0f;
+  out->theta_cone =
+      2.0f * (float)atan((double)(cone_offset * out->collimated_slice_width / out->distance_source_to_isocenter));
+  out->acquisition_field_of_view =
+      2.0f * out->distance_source_to_isocenter *
+      (float)sin((double)((((float)out->num_detector_cols - 1.0f) / 2.0f) * out->detector_pixel_size_col *
+                          (1.0f / out->distance_source_to_detector)));
+}
+
 int make_taps(const CTGeometry* cg, int window, float c, float a, const float* user, int n_user, float* taps, int n) {
   const float ds = cg->detector_pixel_size_col * cg->distance_source_to_isocenter / cg->distance_source_to_detector;
   if (!(ds > 0)) return WFBP_ERR_INVALID_ARG;
@@ -183,6 +212,96 @@ BPParams bp_params(const wfbp_ctx* ctx) {
   p.ncm2 = (float)(ctx->nch - 2);
   p.dtheta = ctx->gp.two_pi_over_projections_per_rotation;
   return p;
+}
+
+// Stage buffer sizes for a filtered-row layout.
+//   rebinned: FP32 [V][nr][nch], or (mixed) BF16 planes [2][V*nrv][kp], row
+//             scales [V*nrv] and view scales [V], each 256-byte aligned
+//   filtered: reference layout [V][nr][nch] FP32/FP16, or backprojection
+//             layout [V][nch][nrp] of 4-byte elements (FP32 or half2 pairs)
+//   scales:   FP32 [V][nr] row scales (mixed, reference layout) or [V] view
+//             scales (mixed, backprojection layout)
+size_t al256(size_t n) { return (n + 255) & ~size_t(255); }
+
+void stage_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal) {
+  const size_t samples = (size_t)ctx->V * ctx->nr * ctx->nch;
+  const bool bpl = layout == WFBP_LAYOUT_BACKPROJECTION;
+  const size_t bpl_bytes = 4 * (size_t)ctx->V * ctx->nch * (size_t)std::max(ctx->bpt.nrp, 1);
+  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
+    const size_t rows = (size_t)ctx->V * ctx->nrv;
+    *reb = al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t)) + al256(rows * sizeof(float)) +
+           (size_t)ctx->V * sizeof(float);
+    *filt = bpl ? bpl_bytes : sizeof(uint16_t) * samples;
+    *scal = bpl ? (size_t)ctx->V * sizeof(float) : (size_t)ctx->V * ctx->nr * sizeof(float);
+  } else {
+    *reb = sizeof(float) * samples;
+    *filt = bpl ? bpl_bytes : sizeof(float) * samples;
+    *scal = 0;
+  }
+}
+
+template <class P>
+void mixed_scale_ptrs(const wfbp_ctx* ctx, P rebinned, float** row_sc, float** view_sc) {
+  const size_t rows = (size_t)ctx->V * ctx->nrv;
+  uint8_t* b = const_cast<uint8_t*>(reinterpret_cast<const uint8_t*>(rebinned));
+  *row_sc = reinterpret_cast<float*>(b + al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t)));
+  *view_sc = reinterpret_cast<float*>(b + al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t)) +
+                                      al256(rows * sizeof(float)));
+}
+
+// Sizes the TMA-staged backprojection for this geometry: the column tile, the
+// channel window each view needs for it, and the most views of one theta~ that
+// can reach a 32-slice slab. Returns false if no configuration fits in shared
+// memory (the generic kernel is used then).
+bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
+  const int nrp = (ctx->nr + 3) / 4 * 4;
+  const double vx = ctx->rp.recon_fov / ctx->nx, vy = ctx->rp.recon_fov / ctx->ny;
+  const double R = ctx->cg.distance_source_to_isocenter;
+  const double rmax = 0.5 * ctx->cg.acquisition_field_of_view;
+  const double tanc = ctx->gp.tanf_theta_cone;
+  // |z - z_j| <= |A| + l_hat tan for any valid (voxel, view); tighter than z_rot
+  const double cone = (R + rmax) * tanc + (ctx->cg.z_rot / (2 * M_PI)) * asin(std::min(1.0, rmax / R));
+  const double reach = std::min((double)ctx->cg.z_rot, cone) + 1e-3 * (1.0 + fabs(ctx->cg.z_rot));
+  // views per theta~ reaching any 32-slice slab
+  int nv_max = 0;
+  const int nslab = (ctx->nz + 31) / 32;
+  for (int sl = 0; sl < nslab; sl++) {
+    float zmn = 3e38f, zmx = -3e38f;
+    for (int i = sl * 32; i < std::min(ctx->nz, sl * 32 + 32); i++) {
+      zmn = std::min(zmn, ctx->z_native[i]);
+      zmx = std::max(zmx, ctx->z_native[i]);
+    }
+    const float lo = zmn - (float)reach, hi = zmx + (float)reach;
+    for (int t = 0; t < ctx->P2; t++) {
+      int n = 0;
+      for (int k = 0; k < ctx->K; k++) {
+        const float zt = table[t + k * ctx->P2];
+        if (!(zt < lo || zt > hi)) n++;
+      }
+      nv_max = std::max(nv_max, n);
+    }
+  }
+  if (nv_max == 0) nv_max = 1;
+  const int tiles[3][2] = {{16, 16}, {16, 8}, {8, 8}};
+  for (auto& tl : tiles) {
+    BPTile b;
+    b.tx = tl[0];
+    b.ty = tl[1];
+    const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
+    b.W = (int)ceil(ext * ctx->gp.pixel_scale) + 5;
+    b.W = std::max(4, std::min(b.W, 256));
+    b.nrp = nrp;
+    b.nv_max = nv_max;
+    b.slot_bytes = (int)((b.W * nrp * 4 + 127) / 128 * 128);
+    b.reach = (float)reach;
+    const size_t smem = bp_tma_smem_bytes(b, 4);
+    b.smem_bytes = (int)smem;
+    if (smem <= 220 * 1024 && nrp <= 256) {
+      ctx->bpt = b;
+      return true;
+    }
+  }
+  return false;
 }
 
 }  // namespace
@@ -296,7 +415,20 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     e = *ext;
   }
   if (e.precision != WFBP_PRECISION_FP32 && e.precision != WFBP_PRECISION_MIXED) return WFBP_ERR_INVALID_ARG;
-  if (cg->ffs_phi || cg->ffs_z || cg->ffs_diag) return WFBP_ERR_UNSUPPORTED;
+  if (e.filtered_layout != WFBP_LAYOUT_REFERENCE && e.filtered_layout != WFBP_LAYOUT_BACKPROJECTION)
+    return WFBP_ERR_INVALID_ARG;
+  if (e.precision == WFBP_PRECISION_MIXED && cg->num_detector_rows > 128) return WFBP_ERR_UNSUPPORTED;
+  if (cg->ffs_diag) return WFBP_ERR_UNSUPPORTED;
+  // With a flying focal spot the stages work on the effective geometry; the
+  // raw frames keep the reading geometry `cg_read`.
+  const CTGeometry* cg_read = cg;
+  CTGeometry cg_eff;
+  const int G = (cg->ffs_phi ? 2 : 1) * (cg->ffs_z ? 2 : 1);
+  if (G > 1) {
+    if (cg->total_number_of_projections % G || cg->projections_per_rotation % G) return WFBP_ERR_INVALID_ARG;
+    ffs_effective(cg, &cg_eff);
+    cg = &cg_eff;
+  }
   if (cg->projections_per_rotation < 2 || cg->total_number_of_projections <= cg->projections_per_rotation / 2 ||
       cg->num_detector_cols < 4 || cg->num_detector_rows < 2 || rp->nx < 1 || rp->ny < 1 ||
       !(rp->recon_fov > 0) || !(rp->slice_thickness > 0) || !(cg->distance_source_to_isocenter > 0) ||
@@ -308,6 +440,8 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
   wfbp_ctx* ctx = new (std::nothrow) wfbp_ctx();
   if (!ctx) return WFBP_ERR_OOM;
   ctx->cg = *cg;
+  ctx->cg_read = *cg_read;
+  ctx->G = G;
   ctx->rp = *rp;
   ctx->ext = e;
   ctx->device = device;
@@ -315,11 +449,12 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
   ctx->nr = (int)cg->num_detector_rows;
   ctx->nch = (int)cg->num_detector_cols;
   ctx->P = (int)cg->projections_per_rotation;
-  ctx->n_readings = ctx->V;
-  ctx->raw_rows = ctx->nr;
-  ctx->raw_ch = ctx->nch;
+  ctx->n_readings = (int)cg_read->total_number_of_projections;
+  ctx->raw_rows = (int)cg_read->num_detector_rows;
+  ctx->raw_ch = (int)cg_read->num_detector_cols;
   ctx->nx = (int)rp->nx;
   ctx->ny = (int)rp->ny;
+  ctx->bpt.nrp = (ctx->nr + 3) / 4 * 4;
 
   // derived constants (recon_structs.h:69-83) from the given geometry
   const float pi_f = 3.1415926535897f;
@@ -392,6 +527,8 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     // zero-padded to [np][kp]
     const int nch = ctx->nch;
     ctx->tc_kp = (nch + 63) / 64 * 64;
+    ctx->nrv = 1;
+    while (ctx->nrv < ctx->nr) ctx->nrv <<= 1;
     ctx->tc_bn = tc_choose_bn(nch);
     ctx->tc_np = (nch + ctx->tc_bn - 1) / ctx->tc_bn * ctx->tc_bn;
     const size_t plane = (size_t)ctx->tc_np * ctx->tc_kp;
@@ -442,19 +579,8 @@ WFBP_API int wfbp_query(const wfbp_ctx* ctx, wfbp_dims* d) {
   d->n_slices_native = ctx->nz;
   d->n_slices_requested = ctx->nzr;
   d->precision = ctx->ext.precision;
-  const size_t samples = (size_t)ctx->V * ctx->nr * ctx->nch;
   d->raw_bytes = sizeof(float) * (size_t)ctx->n_readings * ctx->raw_rows * ctx->raw_ch;
-  const size_t M = (size_t)ctx->V * ctx->nr;
-  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
-    // split BF16 planes [2][M][kp] followed by the FP32 row scales [M]
-    d->rebinned_bytes = 2 * M * (size_t)ctx->tc_kp * sizeof(uint16_t) + M * sizeof(float);
-    d->filtered_bytes = sizeof(uint16_t) * samples;
-    d->row_scale_bytes = M * sizeof(float);
-  } else {
-    d->rebinned_bytes = sizeof(float) * samples;
-    d->filtered_bytes = sizeof(float) * samples;
-    d->row_scale_bytes = 0;
-  }
+  stage_bytes(ctx, ctx->ext.filtered_layout, &d->rebinned_bytes, &d->filtered_bytes, &d->row_scale_bytes);
   d->native_volume_bytes = sizeof(float) * (size_t)ctx->nz * ctx->nx * ctx->ny;
   d->volume_bytes = sizeof(float) * (size_t)ctx->nzr * ctx->nx * ctx->ny;
   return WFBP_OK;
@@ -467,6 +593,14 @@ WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table
     if (!isfinite(tube[j]) || !isfinite(table[j]))
       return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_views: non-finite angle or table position at reading " +
                                                  std::to_string(j));
+  // one view per G readings (flying focal spot), at the group's first reading
+  std::vector<float> tv(ctx->V), zv(ctx->V);
+  for (int v = 0; v < ctx->V; v++) {
+    tv[v] = tube[(size_t)v * ctx->G];
+    zv[v] = table[(size_t)v * ctx->G];
+  }
+  tube = tv.data();
+  table = zv.data();
   DeviceGuard g(ctx->device);
   float *d_t = nullptr, *d_z = nullptr;
   CUDA_TRY(ctx, cudaMalloc(&d_t, sizeof(float) * ctx->V));
@@ -478,6 +612,9 @@ WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table
   cudaFree(d_t);
   cudaFree(d_z);
   CUDA_TRY(ctx, e);
+  const int nrp = ctx->bpt.nrp;
+  ctx->bp_tma_ok = choose_bp_tile(ctx, std::vector<float>(table, table + ctx->V));
+  ctx->bpt.nrp = nrp;
   ctx->views_set = true;
   return WFBP_OK;
 }
@@ -491,6 +628,13 @@ WFBP_API int wfbp_check_device_status(wfbp_ctx* ctx) {
     cudaMemset(ctx->d_err, 0, sizeof(int));
     return fail(ctx, h, "a bounded device-side wait gave up (tensor-core filter pipeline)");
   }
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_get_geometry(const wfbp_ctx* ctx, CTGeometry* cg, GPUPrecompute* gp) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (cg) *cg = ctx->cg;
+  if (gp) *gp = ctx->gp;
   return WFBP_OK;
 }
 
@@ -513,35 +657,93 @@ WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* s
   p.V = ctx->V;
   p.nr = ctx->nr;
   p.nch = ctx->nch;
-  p.dth = 2.0f * 3.14159265f / (float)ctx->P;  // cuda_kernels.cuh:15
+  p.dth = 2.0f * 3.14159265f / (float)ctx->cg_read.projections_per_rotation;  // cuda_kernels.cuh:15
   p.q8 = ctx->ext.tex_weights ? 1 : 0;
+  p.G = ctx->G;
+  p.phi = ctx->cg_read.ffs_phi ? 1 : 0;
+  p.zf = ctx->cg_read.ffs_z ? 1 : 0;
+  p.nch_raw = ctx->raw_ch;
+  p.nr_raw = ctx->raw_rows;
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
-    const size_t M = (size_t)ctx->V * ctx->nr;
-    float* scales = reinterpret_cast<float*>(static_cast<uint8_t*>(rebinned) + 2 * M * (size_t)ctx->tc_kp * 2);
-    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, scales, ctx->d_chan_beta, ctx->d_chan_bidx, p, ctx->tc_kp,
-                                     ctx->taps_l1, (cudaStream_t)stream));
+    float *row_sc, *view_sc;
+    mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
+    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, row_sc, view_sc, ctx->d_chan_beta, ctx->d_chan_bidx, p,
+                                     ctx->tc_kp, ctx->nrv, ctx->taps_l1, (cudaStream_t)stream));
   } else {
     CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream));
   }
   return WFBP_OK;
 }
 
+namespace {
+
+int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
+  const cudaStream_t s = (cudaStream_t)stream;
+  const bool bpl = layout == WFBP_LAYOUT_BACKPROJECTION;
+  if (bpl && !ctx->bp_tma_ok)
+    return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_filter: no backprojection-layout launch fits this geometry");
+  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
+    if (!scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: mixed precision needs scales");
+    float *row_sc, *view_sc;
+    mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
+    TcOutArgs o;
+    memset(&o, 0, sizeof(o));
+    o.nr = ctx->nr;
+    o.nrv = ctx->nrv;
+    o.nrp = ctx->bpt.nrp;
+    o.row_scale_in = row_sc;
+    o.view_scale = view_sc;
+    if (bpl) {
+      o.mode = TC_OUT_PAIRS;
+      o.pairs = static_cast<uint32_t*>(filtered);
+      CUDA_TRY(ctx, cudaMemcpyAsync(scales, view_sc, sizeof(float) * ctx->V, cudaMemcpyDeviceToDevice, s));
+    } else {
+      o.mode = TC_OUT_F16_ROWS;
+      o.y16 = static_cast<__half*>(filtered);
+      o.row_scale_out = scales;
+    }
+    CUDA_TRY(ctx, launch_filter_tc(rebinned, ctx->d_bplanes, ctx->V * ctx->nrv, ctx->nch, ctx->tc_kp, ctx->tc_np,
+                                   ctx->tc_bn, o, ctx->d_err, s));
+    return WFBP_OK;
+  }
+  if (bpl)
+    CUDA_TRY(ctx, launch_filter_f32_tr((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
+                                       ctx->nch, ctx->nr, ctx->bpt.nrp, s));
+  else
+    CUDA_TRY(ctx, launch_filter_f32((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
+                                    ctx->nch, s));
+  return WFBP_OK;
+}
+
+int do_backproject(wfbp_ctx* ctx, const void* filtered, const float* scales, float* vol,
+                   unsigned long long* update_count, int layout, void* stream) {
+  const cudaStream_t s = (cudaStream_t)stream;
+  BPParams p = bp_params(ctx);
+  const bool mixed = ctx->ext.precision == WFBP_PRECISION_MIXED;
+  if (mixed && !scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject: mixed precision needs scales");
+  if (layout == WFBP_LAYOUT_BACKPROJECTION) {
+    if (!ctx->bp_tma_ok)
+      return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_backproject: no backprojection-layout launch fits this geometry");
+    CUDA_TRY(ctx, launch_backproject_tma(filtered, mixed ? 1 : 0, scales, vol, ctx->d_view_sc, ctx->d_view_z,
+                                         ctx->d_z_native, p, ctx->bpt, update_count, ctx->d_err, s));
+    return WFBP_OK;
+  }
+  if (mixed)
+    CUDA_TRY(ctx, launch_backproject_f16((const __half*)filtered, scales, vol, ctx->d_view_sc, ctx->d_view_z,
+                                         ctx->d_z_native, p, update_count, s));
+  else
+    CUDA_TRY(ctx, launch_backproject_f32((const float*)filtered, vol, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native,
+                                         p, update_count, s));
+  return WFBP_OK;
+}
+
+}  // namespace
+
 WFBP_API int wfbp_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* row_scales, void* stream) {
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (!rebinned || !filtered) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: null buffer");
   DeviceGuard g(ctx->device);
-  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
-    if (!row_scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: mixed precision needs row_scales");
-    const int M = ctx->V * ctx->nr;
-    const float* sc_in = reinterpret_cast<const float*>(static_cast<const uint8_t*>(rebinned) +
-                                                        2 * (size_t)M * (size_t)ctx->tc_kp * 2);
-    CUDA_TRY(ctx, launch_filter_tc(rebinned, ctx->d_bplanes, M, ctx->nch, ctx->tc_kp, ctx->tc_np, ctx->tc_bn, nullptr,
-                                   (__half*)filtered, sc_in, row_scales, ctx->d_err, (cudaStream_t)stream));
-    return WFBP_OK;
-  }
-  CUDA_TRY(ctx, launch_filter_f32((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
-                                  ctx->nch, (cudaStream_t)stream));
-  return WFBP_OK;
+  return do_filter(ctx, rebinned, filtered, row_scales, ctx->ext.filtered_layout, stream);
 }
 
 WFBP_API int wfbp_backproject(wfbp_ctx* ctx, const void* filtered, const float* row_scales, float* vol,
@@ -550,16 +752,7 @@ WFBP_API int wfbp_backproject(wfbp_ctx* ctx, const void* filtered, const float* 
   if (!filtered || !vol) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject: null buffer");
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_backproject: wfbp_set_views not called");
   DeviceGuard g(ctx->device);
-  BPParams p = bp_params(ctx);
-  if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
-    if (!row_scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject: mixed precision needs row_scales");
-    CUDA_TRY(ctx, launch_backproject_f16((const __half*)filtered, row_scales, vol, ctx->d_view_sc, ctx->d_view_z,
-                                         ctx->d_z_native, p, update_count, (cudaStream_t)stream));
-    return WFBP_OK;
-  }
-  CUDA_TRY(ctx, launch_backproject_f32((const float*)filtered, vol, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p,
-                                       update_count, (cudaStream_t)stream));
-  return WFBP_OK;
+  return do_backproject(ctx, filtered, row_scales, vol, update_count, ctx->ext.filtered_layout, stream);
 }
 
 WFBP_API int wfbp_thicken(wfbp_ctx* ctx, const float* vn, float* vol, void* stream) {
@@ -572,13 +765,19 @@ WFBP_API int wfbp_thicken(wfbp_ctx* ctx, const float* vn, float* vol, void* stre
 }
 
 namespace {
+// wfbp_run's own layout: the backprojection layout whenever a launch fits.
+int run_layout(const wfbp_ctx* ctx) {
+  return ctx->bp_tma_ok ? WFBP_LAYOUT_BACKPROJECTION : WFBP_LAYOUT_REFERENCE;
+}
+
 int ensure_scratch(wfbp_ctx* ctx) {
-  wfbp_dims d;
-  wfbp_query(ctx, &d);
-  if (!ctx->s_rebinned) CUDA_TRY(ctx, cudaMalloc(&ctx->s_rebinned, d.rebinned_bytes));
-  if (!ctx->s_filtered) CUDA_TRY(ctx, cudaMalloc(&ctx->s_filtered, d.filtered_bytes));
-  if (!ctx->s_vol_native) CUDA_TRY(ctx, cudaMalloc(&ctx->s_vol_native, d.native_volume_bytes));
-  if (!ctx->s_scales && d.row_scale_bytes) CUDA_TRY(ctx, cudaMalloc(&ctx->s_scales, d.row_scale_bytes));
+  size_t reb = 0, filt = 0, scal = 0;
+  stage_bytes(ctx, run_layout(ctx), &reb, &filt, &scal);
+  const size_t nat = sizeof(float) * (size_t)ctx->nz * ctx->nx * ctx->ny;
+  if (!ctx->s_rebinned) CUDA_TRY(ctx, cudaMalloc(&ctx->s_rebinned, reb));
+  if (!ctx->s_filtered) CUDA_TRY(ctx, cudaMalloc(&ctx->s_filtered, filt));
+  if (!ctx->s_vol_native) CUDA_TRY(ctx, cudaMalloc(&ctx->s_vol_native, nat));
+  if (!ctx->s_scales && scal) CUDA_TRY(ctx, cudaMalloc(&ctx->s_scales, scal));
   return WFBP_OK;
 }
 }  // namespace
@@ -590,9 +789,10 @@ WFBP_API int wfbp_run(wfbp_ctx* ctx, const float* raw, float* vol, void* stream)
   DeviceGuard g(ctx->device);
   int st = ensure_scratch(ctx);
   if (st) return st;
+  const int lay = run_layout(ctx);
   if ((st = wfbp_rebin(ctx, raw, ctx->s_rebinned, stream))) return st;
-  if ((st = wfbp_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, stream))) return st;
-  if ((st = wfbp_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, stream))) return st;
+  if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, stream))) return st;
+  if ((st = do_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, lay, stream))) return st;
   return wfbp_thicken(ctx, ctx->s_vol_native, vol, stream);
 }
 

@@ -1,6 +1,7 @@
 // Internal declarations of the B200 WFBP library (not part of the ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
@@ -33,14 +34,36 @@ struct BPParams {
   float dtheta;              // two_pi_over_projections_per_rotation
 };
 
+// Launch configuration of the TMA-staged backprojection (k_bp_tma.cu),
+// sized on the host per geometry.
+struct BPTile {
+  int tx, ty;        // column tile (tx * ty = 16 consumer warps * columns per warp)
+  int W;             // channels staged per view (TMA box)
+  int nrp;           // rows per channel in the backprojection layout (multiple of 4)
+  int nv_max;        // view slots per stage
+  int slot_bytes;    // bytes per view slot (multiple of 128)
+  float reach;       // slab-level half width of the table-position prefilter (mm)
+  int smem_bytes;    // dynamic shared memory of the launch
+};
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn wfbp_encode_tiled_fn();
+
 struct RebinParams {
-  int V, nr, nch;            // views, rows, channels (no FFS)
-  float dth;                 // 2*3.14159265f / P  (cuda_kernels.cuh:15)
+  int V, nr, nch;            // output views, rows, channels (effective ones with FFS)
+  float dth;                 // 2*3.14159265f / readings per rotation (cuda_kernels.cuh:15)
   int q8;                    // 8-bit fractional weights
+  int G;                     // readings per view: 1, or 2 / 4 with a flying focal spot
+  int phi, zf;               // FFS in channel / row direction
+  int nch_raw, nr_raw;       // raw frame shape
 };
 
 struct wfbp_ctx {
-  CTGeometry cg;
+  CTGeometry cg;                    // geometry of the views the stages work on (effective one with FFS)
+  CTGeometry cg_read;               // geometry of the raw readings (== cg without FFS)
+  int G = 1;                        // readings per view
   ReconConfig rp;
   GPUPrecompute gp;
   wfbp_ext ext;
@@ -68,9 +91,14 @@ struct wfbp_ctx {
 
   // mixed precision: Toeplitz operand planes for the tensor-core filter
   int tc_kp = 0, tc_np = 0, tc_bn = 0;
+  int nrv = 0;                      // rows per view in the operand planes (power of two >= nr)
   float taps_l1 = 0.0f;             // sum over |d| < nch of |h[d]|
   void* d_bplanes = nullptr;        // bf16 [2][tc_np][tc_kp]
   int* d_err = nullptr;             // device-side error word (bounded waits)
+
+  // TMA-staged backprojection (backprojection layout [V][nch][nrp])
+  bool bp_tma_ok = false;
+  BPTile bpt;
 
   // context-owned scratch for wfbp_run / wfbp_run_host
   void* s_rebinned = nullptr;
@@ -98,11 +126,29 @@ cudaError_t launch_backproject_f32(const float* D, float* vol, const float2* sc,
 cudaError_t launch_backproject_f16(const __half* D, const float* scales, float* vol, const float2* sc,
                                    const float* vz, const float* zs, const BPParams& p, unsigned long long* count,
                                    cudaStream_t s);
-cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, const float* d_beta,
-                               const float* d_bidx, const RebinParams& p, int kp, float taps_l1, cudaStream_t s);
+cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
+                               const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
+                               float taps_l1, cudaStream_t s);
+// Output modes of the tensor-core filter epilogue.
+enum TcOut { TC_OUT_F32 = 0, TC_OUT_F16_ROWS = 1, TC_OUT_PAIRS = 2 };
+struct TcOutArgs {
+  int mode;
+  int nr, nrv, nrp;             // valid rows per view, rows per view in the planes, rows in the pairs layout
+  float* y32;                   // TC_OUT_F32: [V*nrv][nch]
+  __half* y16;                  // TC_OUT_F16_ROWS: [V][nr][nch]
+  uint32_t* pairs;              // TC_OUT_PAIRS: [V][nch][nrp] half2 (row i, row i+1)
+  const float* row_scale_in;    // [V*nrv]
+  float* row_scale_out;         // [V][nr]
+  const float* view_scale;      // [V]
+};
 cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
-                             float* y32, __half* y16, const float* row_scale_in, float* row_scale_out, int* err,
-                             cudaStream_t s);
+                             const TcOutArgs& out, int* err, cudaStream_t s);
+cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps, long rows, int nch, int nr, int nrp,
+                                 cudaStream_t s);
+size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);
+cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
+                                   const float2* sc, const float* vz, const float* zs, const BPParams& p,
+                                   const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s);
 int tc_choose_bn(int nch);
 cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
                            const float* ws, int nxy, int nzr, cudaStream_t s);

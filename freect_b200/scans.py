@@ -196,6 +196,27 @@ def rows64(seed=0):
                     n_random=20)
 
 
+def ffs(seed=0):
+    """Flying focal spot in phi and z: 736 ch x 32 rows (0.6 mm), 2304 readings
+    per rotation (1152 views/rotation x 2 focal positions) cycling through
+    the 4 focal states, 8 rotations, pitch 0.8; 1472 effective channels x 64
+    effective rows, 576 views/rotation after merging. 40 seeded ellipsoids,
+    I0 1.5e5, 512^2 x 200 slices 0.75 mm thick at a 0.5 mm pitch (200 x 0.75 mm
+    would exceed the 123 mm scanned), 500 mm FOV."""
+    return ScanSpec("ffs", sid=595.0, sdd=1085.6, nch=736, dbeta=0.0011844, c0=366.25, nr=32, row_iso=0.6,
+                    P=2304, rotations=8, feed=0.8 * 32 * 0.6, i0=1.5e5, nx=512, ny=512, fov=500.0,
+                    slice_thickness=0.75, slice_pitch=0.5, n_slices=200, window=T.FILTER_REFERENCE,
+                    phantom="body_random", seed=seed, n_random=40, ffs_mode=T.FFS_PHIZ)
+
+
+def tiny_ffs(seed=0, mode=T.FFS_PHIZ, nch=64, nr=4, P=128, rotations=3, nx=32, n_slices=4):
+    """Reduced flying-focal-spot scan for tests."""
+    spec = tiny(seed=seed, nch=nch, nr=nr, P=P, rotations=rotations, nx=nx, n_slices=n_slices)
+    spec.name = "tiny_ffs"
+    spec.ffs_mode = mode
+    return spec
+
+
 def tiny(seed=0, nch=96, nr=8, P=96, rotations=3, nx=32, n_slices=4, window=T.FILTER_REFERENCE):
     """Reduced scan for CPU tests: the small scanner with a coarser detector."""
     scale = 672.0 / nch
@@ -205,4 +226,4 @@ def tiny(seed=0, nch=96, nr=8, P=96, rotations=3, nx=32, n_slices=4, window=T.FI
                     seed=seed)
 
 
-WORKLOADS = {"small": small, "rows64": rows64, "tiny": tiny}
+WORKLOADS = {"small": small, "rows64": rows64, "ffs": ffs, "tiny": tiny}

@@ -32,6 +32,7 @@ _PROTOS = {
     "wfbp_query": (C.c_int, [_VP, C.POINTER(T.Dims)]),
     "wfbp_set_views": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "wfbp_get_slices": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "wfbp_get_geometry": (C.c_int, [_VP, C.POINTER(T.CTGeometry), C.POINTER(T.GPUPrecompute)]),
     "wfbp_last_error": (C.c_char_p, [_VP]),
     "wfbp_check_device_status": (C.c_int, [_VP]),
     "wfbp_status_string": (C.c_char_p, [C.c_int]),
@@ -144,7 +145,7 @@ def filter_taps(cg, window=T.FILTER_REFERENCE, c=1.0, a=1.0, n=None):
 
 
 def make_ext(precision=T.PRECISION_FP32, filter_window=T.FILTER_REFERENCE, filter_c=1.0, filter_a=1.0,
-             user_taps=None, tex_weights=0, bp_slab=0):
+             user_taps=None, tex_weights=0, bp_slab=0, filtered_layout=T.LAYOUT_REFERENCE):
     e = T.Ext()
     e.version = T.EXT_VERSION
     e.precision = precision
@@ -153,6 +154,7 @@ def make_ext(precision=T.PRECISION_FP32, filter_window=T.FILTER_REFERENCE, filte
     e.filter_a = filter_a
     e.tex_weights = tex_weights
     e.bp_slab = bp_slab
+    e.filtered_layout = filtered_layout
     if user_taps is not None:
         arr = np.ascontiguousarray(user_taps, dtype=np.float32)
         e._taps_keepalive = arr
@@ -186,6 +188,12 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def geometry(self):
+        """(CTGeometry, GPUPrecompute) the stages work on (effective ones with FFS)."""
+        cg, gp = T.CTGeometry(), T.GPUPrecompute()
+        _check(self._lib.wfbp_get_geometry(self._h, C.byref(cg), C.byref(gp)), "wfbp_get_geometry", self._h)
+        return cg, gp
 
     def check_device_status(self):
         _check(self._lib.wfbp_check_device_status(self._h), "wfbp_check_device_status", self._h)
@@ -256,6 +264,8 @@ class Context:
         if what == "rebinned":
             return torch.empty((d.rebinned_bytes + 3) // 4, dtype=torch.float32, device=dev)
         if what == "filtered":
+            if self.ext.filtered_layout == T.LAYOUT_BACKPROJECTION:
+                return torch.empty(d.filtered_bytes // 4, dtype=torch.float32, device=dev)
             if d.precision == 1:
                 return torch.empty((d.n_views, d.n_rows, d.n_channels), dtype=torch.float16, device=dev)
             return torch.empty((d.n_views, d.n_rows, d.n_channels), dtype=torch.float32, device=dev)

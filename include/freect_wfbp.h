@@ -146,6 +146,18 @@ enum wfbp_filter_window {
   WFBP_FILTER_USER = 2        /* caller-provided symmetric taps h[0..n-1] */
 };
 
+/* Layout of the filtered projections at the wfbp_filter / wfbp_backproject
+ * boundary. REFERENCE keeps the reference's [view][row][channel] FP32 (or
+ * FP16 + per-row scales); BACKPROJECTION is the channel-major layout the
+ * TMA-staged backprojection reads: [view][channel][nrp] FP32, or half2 pairs
+ * (row r, row r+1) with one power-of-two scale per view, nrp = nr rounded up
+ * to a multiple of 4. wfbp_run always uses BACKPROJECTION internally when the
+ * geometry allows it. */
+enum wfbp_layout {
+  WFBP_LAYOUT_REFERENCE = 0,
+  WFBP_LAYOUT_BACKPROJECTION = 1
+};
+
 enum wfbp_ffs_mode {
   WFBP_FFS_NONE = 0,
   WFBP_FFS_PHI = 1,
@@ -166,7 +178,8 @@ typedef struct wfbp_ext {
   int tex_weights;            /* 1: rebin uses 8-bit fractional bilinear weights like the
                                  texture unit the reference samples through (cuda_kernels.cuh:36) */
   int bp_slab;                /* 0 = default; native slices per backprojection slab */
-  int reserved[7];
+  int filtered_layout;        /* wfbp_layout of the stage API (default REFERENCE) */
+  int reserved[6];
 } wfbp_ext;
 
 /* Sizes of every stage buffer a context expects (bytes unless noted). */
@@ -183,7 +196,8 @@ typedef struct wfbp_dims {
   size_t raw_bytes;           /* float [n_readings][raw_rows][raw_channels] */
   size_t rebinned_bytes;      /* stage-1 output (FP32 [V][nr][nch], or the split BF16 operand planes) */
   size_t filtered_bytes;      /* stage-2 output (FP32 or FP16 [V][nr][nch]) */
-  size_t row_scale_bytes;     /* FP32 [V][nr] (MIXED only, else 0) */
+  size_t row_scale_bytes;     /* FP32 scales: [V][nr] (MIXED, REFERENCE layout) or [V]
+                                 (MIXED, BACKPROJECTION layout), else 0 */
   size_t native_volume_bytes; /* FP32 [nz_native][ny][nx] */
   size_t volume_bytes;        /* FP32 [nz_requested][ny][nx] */
 } wfbp_dims;
@@ -228,6 +242,14 @@ int wfbp_query(const wfbp_ctx* ctx, wfbp_dims* dims);
 /* Per-view tube angles and table positions, host arrays of n_readings floats
  * (ReconstructionMachine.cu:96-102). Builds the FP64 per-view tables. */
 int wfbp_set_views(wfbp_ctx* ctx, const float* tube_angles, const float* table_positions);
+
+/* The geometry the stages work on: the caller's CTGeometry, or for a flying
+ * focal spot scan its effective geometry (one view per focal-state cycle,
+ * 2x channels / rows at half the spacing, central channel 2 c0 + 1/2), and
+ * the GPUPrecompute derived from it (recon_structs.h:69-83). No counterpart
+ * in the reference, whose fct_wfbp ignores the FFS fields
+ * (recon_structs.h:26-29). */
+int wfbp_get_geometry(const wfbp_ctx* ctx, CTGeometry* cg, GPUPrecompute* gp);
 
 /* Copies the native / requested slice z lists (as wfbp_slice_locations). */
 int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* requested_z);
@@ -325,10 +347,11 @@ typedef struct wfbp_synth_scan {
   double z0, dz;              /* table position of reading 0, signed step per reading (mm) */
   double i0;                  /* incident photons (0 = noiseless line integrals) */
   unsigned long long seed;
-  int ffs_mode;               /* wfbp_ffs_mode */
-  double ffs_dphi;            /* phi-FFS: +- source shift along the tangent (mm) */
-  double ffs_dz;              /* z-FFS: +- source shift along z (mm) */
-  double ffs_dr;              /* z-FFS: +- radial source shift (mm) */
+  int ffs_mode;               /* wfbp_ffs_mode: reading n has focal state n % G (G = 4 for
+                                 PHIZ: phi bit = state & 1, z bit = state >> 1; G = 2 otherwise)
+                                 and samples the effective channels 2b + phi bit and rows
+                                 2r + z bit of a detector with twice the channels / rows at
+                                 half the spacing and central channel 2 c0 + 1/2 */
 } wfbp_synth_scan;
 
 /* Line integrals (and Poisson noise, log transform) through the ellipsoid

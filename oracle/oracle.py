@@ -53,6 +53,12 @@ def load():
             "orc_thicken_f64": (None, [R, _D, _D, C.c_int, _D, C.c_int, _D]),
             "orc_synth_project": (C.c_int, [C.POINTER(T.SynthScan), C.POINTER(T.Ellipsoid), C.c_int, _F]),
             "orc_voxelize": (None, [C.POINTER(T.Ellipsoid), C.c_int, R, _D, C.c_int, C.c_double, C.c_int, _D]),
+            "orc_ffs_effective": (C.c_int, [G, G]),
+            "orc_rebin_ffs_f64": (C.c_int, [G, _F, _D]),
+            "orc_thicken_adjoint_f64": (None, [R, _D, _D, C.c_int, _D, C.c_int, _D]),
+            "orc_backproject_adjoint_f64": (None, [G, R, _D, _D, _D, _D, C.c_int, _D]),
+            "orc_taps_gradient_f64": (None, [C.c_int, C.c_long, _D, _D, C.c_int, _D]),
+            "orc_rebin_adjoint_f64": (None, [G, _D, _D]),
         }
         for name, (res, args) in protos.items():
             f = getattr(lib, name)
@@ -252,13 +258,40 @@ def reconstruct_ref32(spec, raw, taps_half=None, q8=False):
     return dict(cg=cg, gp=gp, rp=rp, filtered=filt, native=vn, volume=vol, z_native=zn, z_req=zr)
 
 
+def ffs_effective(cg):
+    """effective geometry of a flying-focal-spot scan (one view per state cycle)"""
+    ce = T.CTGeometry()
+    st = load().orc_ffs_effective(C.byref(cg), C.byref(ce))
+    if st:
+        raise ValueError("orc_ffs_effective: readings not a multiple of the focal states")
+    return ce
+
+
+def rebin_ffs_f64(cg, raw):
+    ce = ffs_effective(cg)
+    out = np.zeros((int(ce.total_number_of_projections), int(ce.num_detector_rows), int(ce.num_detector_cols)),
+                   np.float64)
+    r = _f(raw)
+    st = load().orc_rebin_ffs_f64(C.byref(cg), fp(r), dp(out))
+    if st:
+        raise ValueError("orc_rebin_ffs_f64: status %d" % st)
+    return out
+
+
 def reconstruct_f64(spec, raw, taps_half=None):
-    """FP64 oracle of the same algorithm."""
+    """FP64 oracle of the same algorithm (effective geometry with FFS)."""
     tube, table = spec.views()
     cg, gp = configure_geometry(spec.meta(), table)
     rp = spec.recon_config()
-    half = taps_f64(cg, spec.window) if taps_half is None else np.asarray(taps_half, np.float64)
-    reb = rebin_f64(cg, raw)
+    if cg.ffs_phi or cg.ffs_z:
+        G = (2 if cg.ffs_phi else 1) * (2 if cg.ffs_z else 1)
+        reb = rebin_ffs_f64(cg, raw)
+        cg = ffs_effective(cg)
+        tube, table = tube[::G].copy(), table[::G].copy()
+        half = taps_f64(cg, spec.window) if taps_half is None else np.asarray(taps_half, np.float64)
+    else:
+        half = taps_f64(cg, spec.window) if taps_half is None else np.asarray(taps_half, np.float64)
+        reb = rebin_f64(cg, raw)
     filt = filter_f64(reb, half)
     zn, zr = slice_locations(cg, rp)
     vn, n_updates = backproject_f64(cg, rp, filt, tube.astype(np.float64), table.astype(np.float64), zn)
@@ -276,3 +309,65 @@ def hu_error(a, b, mu_water=0.019):
     if d.size == 0:
         return float("nan"), float("nan"), 0
     return float(np.sqrt(np.mean(d * d))), float(np.max(np.abs(d))), int(m.sum())
+
+
+# --------------------------------------------------------------------------
+# adjoints and the FP64 gradient of an image loss
+# --------------------------------------------------------------------------
+
+def thicken_adjoint_f64(rp, g_vol, z_native, z_req):
+    gv, zn, zr = _d(g_vol), _d(z_native), _d(z_req)
+    out = np.zeros((zn.size,) + gv.shape[1:], np.float64)
+    load().orc_thicken_adjoint_f64(C.byref(rp), dp(gv), dp(zn), zn.size, dp(zr), zr.size, dp(out))
+    return out
+
+
+def backproject_adjoint_f64(cg, rp, g_native, tube, table, slices):
+    gn, t, z, sl = _d(g_native), _d(tube), _d(table), _d(slices)
+    out = np.zeros((int(cg.total_number_of_projections), int(cg.num_detector_rows), int(cg.num_detector_cols)),
+                   np.float64)
+    load().orc_backproject_adjoint_f64(C.byref(cg), C.byref(rp), dp(gn), dp(t), dp(z), dp(sl), sl.size, dp(out))
+    return out
+
+
+def taps_gradient_f64(g_filtered, rebinned, ntaps):
+    g, x = _d(g_filtered), _d(rebinned)
+    nch = g.shape[-1]
+    out = np.zeros(ntaps, np.float64)
+    load().orc_taps_gradient_f64(nch, g.size // nch, dp(g), dp(x), ntaps, dp(out))
+    return out
+
+
+def rebin_adjoint_f64(cg, g_rebinned):
+    g = _d(g_rebinned)
+    out = np.zeros((int(cg.total_number_of_projections), int(cg.num_detector_rows), int(cg.num_detector_cols)),
+                   np.float64)
+    load().orc_rebin_adjoint_f64(C.byref(cg), dp(g), dp(out))
+    return out
+
+
+def loss_and_grad_f64(spec, raw, taps_half, target, ntaps):
+    """L = mean over finite voxels of (vol - target)^2 for the FP64 path with
+    filter taps `taps_half`; returns (L, dL/draw, dL/dtaps[:ntaps], vol)."""
+    tube, table = spec.views()
+    cg, gp = configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    taps = np.asarray(taps_half, np.float64)
+    x = rebin_f64(cg, raw)
+    y = filter_f64(x, taps)
+    zn, zr = slice_locations(cg, rp)
+    t64, z64 = tube.astype(np.float64), table.astype(np.float64)
+    vn, _ = backproject_f64(cg, rp, y, t64, z64, zn)
+    vol = thicken_f64(rp, vn, zn, zr)
+    m = np.isfinite(vol)
+    n = m.sum()
+    diff = np.where(m, vol - target, 0.0)
+    L = float((diff[m] ** 2).sum() / n)
+    g_vol = 2.0 * diff / n
+    g_vn = thicken_adjoint_f64(rp, g_vol, zn, zr)
+    g_vn[~np.isfinite(vn)] = 0.0
+    g_y = backproject_adjoint_f64(cg, rp, g_vn, t64, z64, zn)
+    g_x = filter_f64(g_y, taps)
+    g_raw = rebin_adjoint_f64(cg, g_x)
+    g_taps = taps_gradient_f64(g_y, x, ntaps)
+    return L, g_raw, g_taps, vol

@@ -826,42 +826,36 @@ static double chord_sum(const wfbp_ellipsoid* e, int ne, const double S[3], cons
  * the parallel direction is theta = angle_v - beta, the in-plane ray is
  * x sin(theta) - y cos(theta) = (nch + 1.75 - 2 c0) ds - R sin(beta), the
  * source sits on it at radius R, and flipped row rr = nr-1-r rises with
- * slope (rr - (nr-1)/2) drow/sdd per mm of in-plane distance. Flying focal
- * spots displace the source of each reading (see the FFS notes in the
- * product's rebin). */
+ * slope (rr - (nr-1)/2) drow/sdd per mm of in-plane distance. With a flying
+ * focal spot the same holds on the effective detector (2x channels / rows at
+ * half the spacing, central channel 2 c0 + 1/2), where reading v of focal
+ * state (sp, sz) samples effective channel 2b + sp and effective row
+ * 2 rr + sz (see orc_ffs_effective). */
 static void synth_ray(const wfbp_synth_scan* s, long v, int r, int k, double S[3], double U[3]) {
   int nch = s->channels, nr = s->rows;
+  const int phi = (s->ffs_mode & WFBP_FFS_PHI) != 0, zf = (s->ffs_mode & WFBP_FFS_Z) != 0;
+  const int G = (phi ? 2 : 1) * (zf ? 2 : 1);
+  const int rho = (int)(v % G);
+  const int sp = phi ? (G == 4 ? (rho & 1) : rho) : 0, sz = zf ? (G == 4 ? (rho >> 1) : rho) : 0;
+  const int nche = phi ? 2 * nch : nch, nre = zf ? 2 * nr : nr;
+  const double c0e = phi ? 2.0 * s->central_channel + 0.5 : s->central_channel;
+  const double dcole = phi ? 0.5 * s->dcol : s->dcol, drowe = zf ? 0.5 * s->drow : s->drow;
   double R = s->sid;
-  double ds = s->dcol * R / s->sdd;
-  double delta = nch + 1.75 - 2.0 * s->central_channel;
+  double ds = dcole * R / s->sdd;
+  double delta = nche + 1.75 - 2.0 * c0e;
   int b = nch - 1 - k, rr = nr - 1 - r;
-  double beta = (b - s->central_channel) * s->dcol / s->sdd;
+  int be = phi ? 2 * b + sp : b, rre = zf ? 2 * rr + sz : rr;
+  double beta = (be - c0e) * dcole / s->sdd;
   double ang = s->angle0 + v * s->dangle;
   double zs = s->z0 + v * s->dz;
-  double dphi = 0.0, dzf = 0.0, dr = 0.0;
-  if (s->ffs_mode != WFBP_FFS_NONE) {
-    int phase;
-    if (s->ffs_mode == WFBP_FFS_PHIZ) phase = (int)(v % 4);
-    else phase = (int)(v % 2);
-    int sa = 0, sz = 0;
-    if (s->ffs_mode == WFBP_FFS_PHI) sa = phase ? 1 : -1;
-    if (s->ffs_mode == WFBP_FFS_Z) sz = phase ? 1 : -1;
-    if (s->ffs_mode == WFBP_FFS_PHIZ) { sa = (phase & 1) ? 1 : -1; sz = (phase & 2) ? 1 : -1; }
-    dphi = sa * s->ffs_dphi; dzf = sz * s->ffs_dz; dr = sz * s->ffs_dr;
-  }
-  /* phi-FFS: the focal spot moves along the tangent by dphi, i.e. the
-   * source angle changes by dphi/R and every ray of the reading shifts;
-   * modelled as an angular offset of the source */
-  double Reff = R + dr;
-  ang += dphi / R;
   double theta = ang - beta;
   double sn = sin(theta), cs = cos(theta);
-  double pstar = delta * ds - Reff * sin(beta);
-  double t = sqrt(Reff * Reff - pstar * pstar);
+  double pstar = delta * ds - R * sin(beta);
+  double t = sqrt(R * R - pstar * pstar);
   S[0] = pstar * sn + t * cs;
   S[1] = -pstar * cs + t * sn;
-  S[2] = zs + dzf;
-  double slope = (rr - (nr - 1) / 2.0) * s->drow / s->sdd;
+  S[2] = zs;
+  double slope = (rre - (nre - 1) / 2.0) * drowe / s->sdd;
   U[0] = -cs; U[1] = -sn; U[2] = slope;
 }
 
@@ -929,4 +923,261 @@ ORC_EXPORT void orc_voxelize(const wfbp_ellipsoid* e, int ne, const ReconConfig*
                              double dz, int ss, double* out) {
   vox_args a = {e, ne, rp, z, dz, ss, out};
   orc_parallel_for((long)nz * (long)rp->ny, 1, vox_body, &a);
+}
+
+/* ------------------------------------------------------------------------ */
+/* flying focal spot (no counterpart in the reference's WFBP)               */
+/* ------------------------------------------------------------------------ */
+/* Readings cycle through the focal states of fct_icd's generate_ffs_offset
+ * (applications/fct_icd/src/generate_system_matrix_ffs.cpp:242-290): with
+ * phi and z FFS, state = reading % 4, phi bit = state & 1, z bit = state >> 1;
+ * with one of them, state = reading % 2. A reading of phi state sp samples
+ * the effective channels 2b + sp (fan angle offset by (sp - 1/2) dbeta/2), a
+ * reading of z state sz the effective rows 2r + sz (half a row). The
+ * effective detector has 2x channels / rows at half the spacing, central
+ * channel 2 c0 + 1/2, and one effective view per G readings (G = number of
+ * states), at the angle and table position of the group's first reading. */
+static int ffs_groups(const CTGeometry* cg) { return (cg->ffs_phi ? 2 : 1) * (cg->ffs_z ? 2 : 1); }
+
+ORC_EXPORT int orc_ffs_effective(const CTGeometry* in, CTGeometry* out) {
+  *out = *in;
+  int G = ffs_groups(in);
+  if (in->total_number_of_projections % G || in->projections_per_rotation % G) return WFBP_ERR_INVALID_ARG;
+  int fp = in->ffs_phi ? 2 : 1, fz = in->ffs_z ? 2 : 1;
+  out->total_number_of_projections = in->total_number_of_projections / G;
+  out->projections_per_rotation = in->projections_per_rotation / G;
+  out->num_detector_cols = in->num_detector_cols * fp;
+  out->num_detector_cols_padded = 2 * out->num_detector_cols;
+  out->num_detector_cols_padded_fft = next_pow2_at_least(2 * out->num_detector_cols);
+  out->num_detector_rows = in->num_detector_rows * fz;
+  out->num_detector_rows_padded = 2 * out->num_detector_rows;
+  out->detector_pixel_size_col = in->detector_pixel_size_col / fp;
+  out->detector_pixel_size_row = in->detector_pixel_size_row / fz;
+  out->detector_central_col = in->ffs_phi ? 2.0f * in->detector_central_col + 0.5f : in->detector_central_col;
+  out->detector_central_row = ((float)out->num_detector_rows - 1.0f) / 2.0f;
+  out->collimated_slice_width =
+      out->distance_source_to_isocenter * (out->detector_pixel_size_row / out->distance_source_to_detector);
+  float cone_offset = ((float)(out->num_detector_rows - 1)) / 2.0f;
+  out->theta_cone = 2.0f * (float)atan((double)(cone_offset * out->collimated_slice_width /
+                                                out->distance_source_to_isocenter));
+  out->acquisition_field_of_view =
+      2.0f * out->distance_source_to_isocenter *
+      (float)sin((double)((((float)out->num_detector_cols - 1.0f) / 2.0f) * out->detector_pixel_size_col *
+                          (1.0f / out->distance_source_to_detector)));
+  return WFBP_OK;
+}
+
+/* FP64 rebin of FFS readings onto the effective parallel grid: the fan
+ * sample at fractional effective channel bidx and reading index
+ * G v - beta/dtheta_reading is interpolated between the two effective
+ * channels around bidx, each from its own focal state's readings (linear in
+ * reading angle between that state's neighbouring readings). out:
+ * [V/G][nr_eff][nch_eff]. */
+typedef struct { const CTGeometry* cg; const CTGeometry* ce; const float* raw; double* out; } rbf_args;
+static void rbf_body(void* a_, long i0, long i1) {
+  rbf_args* a = (rbf_args*)a_;
+  const CTGeometry* cg = a->cg; const CTGeometry* ce = a->ce;
+  const int G = ffs_groups(cg), phi = cg->ffs_phi, zf = cg->ffs_z;
+  const int nch = (int)cg->num_detector_cols, nr = (int)cg->num_detector_rows;
+  const int nche = (int)ce->num_detector_cols, nre = (int)ce->num_detector_rows, Ve = (int)ce->total_number_of_projections;
+  const double dth = 2.0 * M_PI / (double)cg->projections_per_rotation;
+  const double c0e = ce->detector_central_col, dcole = ce->detector_pixel_size_col, sdd = cg->distance_source_to_detector;
+  for (long row = i0; row < i1; row++) {
+    int v = (int)(row / nre), ie = (int)(row % nre);
+    int zs = zf ? (ie & 1) : 0, iraw = zf ? ie >> 1 : ie, rraw = nr - 1 - iraw;
+    for (int c = 0; c < nche; c++) {
+      double p = ((double)c - c0e) * dcole;
+      double beta = asin(p / sdd);
+      double bidx = beta * sdd / dcole + c0e;
+      double val = 0.0;
+      if (!(bidx < 0 || bidx >= (double)nche || isnan(bidx))) {
+        double fx = floor(bidx), ax = bidx - fx;
+        double nf = (double)G * v - beta / dth;
+        for (int t = 0; t < 2; t++) {
+          long e = (long)fx + t;
+          if (e < 0) e = 0;
+          if (e > nche - 1) e = nche - 1;
+          double we = t ? ax : 1.0 - ax;
+          int sp = phi ? (int)(e & 1) : 0;
+          int b = phi ? (int)(e >> 1) : (int)e;
+          int rho = (G == 4) ? sp + 2 * zs : (phi ? sp : zs);
+          double mf = (nf - rho) / G, m0 = floor(mf), ay = mf - m0;
+          for (int u = 0; u < 2; u++) {
+            long m = (long)m0 + u;
+            if (m < 0) m = 0;
+            if (m > Ve - 1) m = Ve - 1;
+            double wy = u ? ay : 1.0 - ay;
+            long n = (long)G * m + rho;
+            val += we * wy * a->raw[((size_t)n * nr + rraw) * nch + (nch - 1 - b)];
+          }
+        }
+      }
+      a->out[row * nche + c] = val;
+    }
+  }
+}
+ORC_EXPORT int orc_rebin_ffs_f64(const CTGeometry* cg, const float* raw, double* out) {
+  CTGeometry ce;
+  int st = orc_ffs_effective(cg, &ce);
+  if (st) return st;
+  rbf_args a = {cg, &ce, raw, out};
+  orc_parallel_for((long)ce.total_number_of_projections * (long)ce.num_detector_rows, 16, rbf_body, &a);
+  return WFBP_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* adjoints (FP64), the transposes of the forward loops above               */
+/* ------------------------------------------------------------------------ */
+
+/* thickening: g_native[n] += w_n / sum(w) * g_vol[r] */
+ORC_EXPORT void orc_thicken_adjoint_f64(const ReconConfig* rp, const double* g_vol, const double* z_native, int nz,
+                                        const double* z_req, int nzr, double* g_native) {
+  size_t plane = rp->nx * rp->ny;
+  memset(g_native, 0, sizeof(double) * plane * nz);
+  for (int r = 0; r < nzr; r++) {
+    double ws = 0.0;
+    for (int i = 0; i < nz; i++) {
+      double w = 1.0 - fabs(z_native[i] - z_req[r]) / rp->slice_thickness;
+      if (w > 0.0) ws += w;
+    }
+    if (!(ws > 0.0)) continue;
+    for (int i = 0; i < nz; i++) {
+      double w = 1.0 - fabs(z_native[i] - z_req[r]) / rp->slice_thickness;
+      if (w <= 0.0) continue;
+      for (size_t px = 0; px < plane; px++) g_native[(size_t)i * plane + px] += w / ws * g_vol[(size_t)r * plane + px];
+    }
+  }
+}
+
+/* backprojection: for every voxel and theta~, the weights W_k/sum(W) of the
+ * forward's normalised average, times dtheta, scatter the voxel's gradient
+ * through each view's bilinear weights. Views are owned by threads (each
+ * thread loops over all voxels for its views), so no two threads write the
+ * same sample. g_filtered: [V][nr][nch]. */
+typedef struct { bp64_geo g; const double* gv; const double* tube; const double* table; const double* slices; int nz;
+                 double* gf; } bpa_args;
+static void bpa_body(void* a_, long t0, long t1) {
+  bpa_args* a = (bpa_args*)a_;
+  const bp64_geo* g = &a->g;
+  size_t nch = (size_t)g->nch, nr = (size_t)g->nr;
+  double* Wk = (double*)malloc(sizeof(double) * g->K);
+  double* pidx = (double*)malloc(sizeof(double) * g->K);
+  double* qidx = (double*)malloc(sizeof(double) * g->K);
+  for (long t = t0; t < t1; t++) { /* theta~ */
+    for (int s = 0; s < a->nz; s++) {
+      double z = a->slices[s];
+      for (int iy = 0; iy < g->ny; iy++) {
+        double y = (iy - 0.5 * (g->ny - 1.0)) * g->fov / g->ny + g->y0;
+        for (int ix = 0; ix < g->nx; ix++) {
+          double x = (ix - 0.5 * (g->nx - 1.0)) * g->fov / g->nx + g->x0;
+          if (x * x + y * y > g->afov_half2) continue;
+          double gvox = a->gv[((size_t)s * g->ny + iy) * g->nx + ix];
+          if (gvox == 0.0) continue;
+          double nf = 0.0;
+          for (int k = 0; k < g->K; k++) {
+            Wk[k] = 0.0;
+            int j = (int)t + k * g->P2;
+            double zt = a->table[j];
+            if (fabs(zt - z) > g->z_rot) continue;
+            double th = a->tube[j], sn = sin(th), cs = cos(th);
+            double p_hat = x * sn - y * cs;
+            double l_hat = sqrt(g->sid2 - p_hat * p_hat) - x * cs - y * sn;
+            double q_hat = (z - zt + g->zr2pi * asin(p_hat / g->sid)) / (l_hat * g->tanc);
+            if (q_hat > 1.0 || q_hat < -1.0) continue;
+            double pi_ = (g->nch + 1.75) - (p_hat * g->pixel_scale + g->c0);
+            double qi = 0.5 * (q_hat + 1.0) * (g->nr - 1.0);
+            if (floor(pi_) < 0 || floor(qi) < 0) continue;
+            if (ceil(pi_) >= g->nch - 1 || ceil(qi) >= g->nr - 1) continue;
+            Wk[k] = w_f64(q_hat);
+            pidx[k] = pi_;
+            qidx[k] = qi;
+            nf += Wk[k];
+          }
+          if (!(nf > 0.0)) continue;
+          for (int k = 0; k < g->K; k++) {
+            if (Wk[k] == 0.0) continue;
+            int j = (int)t + k * g->P2;
+            double c = gvox * g->dtheta * Wk[k] / nf;
+            double pf = floor(pidx[k]), qf = floor(qidx[k]);
+            double wp = pidx[k] - pf, wq = qidx[k] - qf;
+            size_t lo = (size_t)pf + (size_t)qf * nch + (size_t)j * nr * nch, hi = lo + nch;
+            a->gf[lo] += c * (1 - wq) * (1 - wp);
+            a->gf[lo + 1] += c * (1 - wq) * wp;
+            a->gf[hi] += c * wq * (1 - wp);
+            a->gf[hi + 1] += c * wq * wp;
+          }
+        }
+      }
+    }
+  }
+  free(Wk); free(pidx); free(qidx);
+}
+ORC_EXPORT void orc_backproject_adjoint_f64(const CTGeometry* cg, const ReconConfig* rp, const double* g_native,
+                                            const double* tube, const double* table, const double* slices, int nz,
+                                            double* g_filtered) {
+  bpa_args a;
+  bp64_geo_init(&a.g, cg, rp, table);
+  a.gv = g_native; a.tube = tube; a.table = table; a.slices = slices; a.nz = nz; a.gf = g_filtered;
+  memset(g_filtered, 0, sizeof(double) * cg->total_number_of_projections * cg->num_detector_rows * cg->num_detector_cols);
+  /* threads own theta~ values: views theta~ + k P/2 belong to exactly one thread */
+  orc_parallel_for(a.g.P2, 4, bpa_body, &a);
+}
+
+/* tap gradient: dL/dh[d] = sum_rows sum_n g[n] (x[n-d] + x[n+d]) (d > 0), sum g[n] x[n] (d = 0) */
+ORC_EXPORT void orc_taps_gradient_f64(int nch, long rows, const double* g, const double* x, int ntaps, double* out) {
+  for (int d = 0; d < ntaps; d++) {
+    double acc = 0.0;
+    for (long r = 0; r < rows; r++) {
+      const double* gr = g + r * nch;
+      const double* xr = x + r * nch;
+      for (int n = 0; n < nch; n++) {
+        if (d == 0) acc += gr[n] * xr[n];
+        else {
+          if (n - d >= 0) acc += gr[n] * xr[n - d];
+          if (n + d < nch) acc += gr[n] * xr[n + d];
+        }
+      }
+    }
+    out[d] = acc;
+  }
+}
+
+/* rebin (FP64, exact weights, clamp addressing): transpose of rb64_body */
+typedef struct { const CTGeometry* cg; const double* gx; double* graw; } rba_args;
+static void rba_body(void* a_, long i0, long i1) {
+  rba_args* a = (rba_args*)a_;
+  const CTGeometry* cg = a->cg;
+  int nr = (int)cg->num_detector_rows, nch = (int)cg->num_detector_cols, V = (int)cg->total_number_of_projections;
+  double dth = 2.0 * M_PI / (double)cg->projections_per_rotation;
+  double c0 = cg->detector_central_col, dcol = cg->detector_pixel_size_col, sdd = cg->distance_source_to_detector;
+  for (long i = i0; i < i1; i++) { /* rows are independent: raw row nr-1-i */
+    int r_raw = nr - 1 - (int)i;
+    for (int v = 0; v < V; v++) {
+      for (int c = 0; c < nch; c++) {
+        double gval = a->gx[((size_t)v * nr + i) * nch + c];
+        if (gval == 0.0) continue;
+        double p = ((double)c - c0) * dcol;
+        double beta = asin(p / sdd);
+        double bidx = beta * sdd / dcol + c0;
+        if (bidx < 0 || bidx >= (double)nch || isnan(bidx)) continue;
+        double aidx = (double)v - beta / dth;
+        double fx = floor(bidx), fy = floor(aidx);
+        double ax = bidx - fx, ay = aidx - fy;
+        long xs[2] = {(long)fx, (long)fx + 1}, ys[2] = {(long)fy, (long)fy + 1};
+        double wx[2] = {1 - ax, ax}, wy[2] = {1 - ay, ay};
+        for (int u = 0; u < 2; u++) {
+          long xx = xs[u] < 0 ? 0 : (xs[u] > nch - 1 ? nch - 1 : xs[u]);
+          for (int t = 0; t < 2; t++) {
+            long yy = ys[t] < 0 ? 0 : (ys[t] > V - 1 ? V - 1 : ys[t]);
+            a->graw[((size_t)yy * nr + r_raw) * nch + (nch - 1 - xx)] += gval * wx[u] * wy[t];
+          }
+        }
+      }
+    }
+  }
+}
+ORC_EXPORT void orc_rebin_adjoint_f64(const CTGeometry* cg, const double* g_rebinned, double* g_raw) {
+  rba_args a = {cg, g_rebinned, g_raw};
+  memset(g_raw, 0, sizeof(double) * cg->total_number_of_projections * cg->num_detector_rows * cg->num_detector_cols);
+  orc_parallel_for((long)cg->num_detector_rows, 1, rba_body, &a);
 }

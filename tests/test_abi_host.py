@@ -106,3 +106,21 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(wfbp, "_LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(ImportError):
         wfbp.load()
+
+
+def test_ffs_geometry_and_validation(lib, orc):
+    # FFS readings: the context derives the effective geometry; a reading
+    # count that is not a multiple of the focal states is rejected before
+    # any device work
+    spec = scans.tiny_ffs(mode=T.FFS_PHIZ, nch=64, nr=8, P=256)
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    assert cg.ffs_phi and cg.ffs_z
+    ce = orc.ffs_effective(cg)
+    assert ce.num_detector_cols == 128 and ce.num_detector_rows == 16
+    assert ce.total_number_of_projections == spec.V // 4 and ce.projections_per_rotation == 64
+    assert ce.detector_central_col == pytest.approx(2 * spec.c0 + 0.5)
+    bad = T.CTGeometry.from_buffer_copy(cg)
+    bad.total_number_of_projections -= 1
+    h = C.c_void_p()
+    assert lib.wfbp_ctx_create(C.byref(bad), C.byref(spec.recon_config()), None, 0, C.byref(h)) == 1

@@ -98,3 +98,34 @@ def test_mixed_requires_row_scales(orc):
     with pytest.raises(wfbp.WfbpError) as e:
         ctx.filter(reb, filt, None)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("which", ["tiny", "odd"])
+def test_mixed_backprojection_layout_stages(orc, which):
+    # split-BF16 filter writing FP16 row pairs with per-view scales, read by the
+    # TMA-staged backprojection; against the FP64 oracle
+    if which == "tiny":
+        spec = scans.tiny()
+    else:
+        spec = scans.tiny(nch=90, nr=5, P=100, rotations=2.57, nx=33, n_slices=3)
+        spec.ny = 17
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    e = wfbp.make_ext(precision=T.PRECISION_MIXED, filter_window=spec.window, filtered_layout=T.LAYOUT_BACKPROJECTION)
+    ctx = wfbp.Context(cg, spec.recon_config(), e, device=0)
+    ctx.set_views(tube, table)
+    reb, filt, sc, vn, vol = (ctx.alloc(k) for k in ("rebinned", "filtered", "row_scales", "native", "volume"))
+    ctx.rebin(dev(raw), reb)
+    ctx.filter(reb, filt, sc)
+    ctx.backproject(filt, vn, sc)
+    ctx.thicken(vn, vol)
+    torch.cuda.synchronize()
+    ctx.check_device_status()
+    s = sc.cpu().numpy()[: spec.V]
+    assert np.all(s > 0) and np.all(np.log2(s) == np.round(np.log2(s)))
+    r64 = orc.reconstruct_f64(spec, raw)
+    got = vol.cpu().numpy()
+    rms, mx, n = orc.hu_error(got, r64["volume"])
+    assert n == np.isfinite(r64["volume"]).sum()
+    assert rms <= 1.0, (rms, mx)

@@ -229,3 +229,52 @@ def test_fp32_form_vs_reference_kernels(orc, path):
     assert np.array_equal(np.isnan(got), np.isnan(d["volume"]))
     assert n == np.isfinite(d["volume"]).sum()
     assert rms <= 0.5 and mx <= 2.0, (rms, mx)
+
+
+@pytest.mark.parametrize("which", ["tiny", "odd", "small128"])
+def test_backprojection_layout_stages(orc, which):
+    # FP32 form through the stage API with the backprojection layout: the
+    # transposed filter output equals the reference-layout one, and the
+    # TMA-staged backprojection equals the transcript on the same rows.
+    if which == "tiny":
+        spec = scans.tiny()
+    elif which == "odd":
+        spec = scans.tiny(nch=90, nr=5, P=100, rotations=2.57, nx=33, n_slices=3)
+        spec.ny = 17
+    else:
+        spec = scans.small(seed=5)
+        spec.nx = spec.ny = 128
+        spec.n_slices = 6
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    ctx = wfbp.Context(cg, spec.recon_config(), wfbp.make_ext(filter_window=spec.window, tex_weights=1,
+                                                             filtered_layout=T.LAYOUT_BACKPROJECTION), device=0)
+    ctx.set_views(tube, table)
+    reb = ctx.alloc("rebinned")
+    ctx.rebin(dev(raw), reb)
+    filt = ctx.alloc("filtered")
+    ctx.filter(reb, filt)
+    vn = ctx.alloc("native")
+    cnt = torch.zeros(1, dtype=torch.int64, device=DEV)
+    ctx.backproject(filt, vn, update_count=cnt)
+    torch.cuda.synchronize()
+    ctx.check_device_status()
+    nrp = (spec.nr + 3) // 4 * 4
+    ft = filt.cpu().numpy().reshape(spec.V, spec.nch, nrp)[:, :, :spec.nr].transpose(0, 2, 1)
+    ref_reb = orc.rebin_ref32(cg, raw, q8=True)
+    ref_f = orc.filter_f64(ref_reb, wfbp.filter_taps(cg, spec.window).astype(np.float64))
+    # 8-bit weights: a last-ulp difference can move a weight by 1/256
+    assert np.abs(ft - ref_f).max() < 5e-3 * np.abs(ref_f).max()
+    nat, _ = ctx.slices()
+    ref_v = orc.backproject_ref32(cg, ctx.rp, gp, np.ascontiguousarray(ft), tube, table, nat)
+    got = vn.cpu().numpy()
+    rms, mx, n = orc.hu_error(got, ref_v)
+    assert np.array_equal(np.isnan(got), np.isnan(ref_v))
+    # the z cull |z - z_j| <= z_rot is evaluated in row space (q range per
+    # column and view): a slice exactly on the boundary can fall the other
+    # way, which moves that voxel by a fraction of a HU
+    assert rms < 0.05 and mx < 1.0, (rms, mx)
+    _, n64 = orc.backproject_f64(cg, ctx.rp, ft.astype(np.float64), tube.astype(np.float64),
+                                 table.astype(np.float64), nat)
+    assert abs(int(cnt.item()) - n64) <= 1e-4 * n64 + 2
