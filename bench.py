@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-slices", type=int, default=1)
+    ap.add_argument("--no-tune", action="store_true", help="keep the default backprojection configuration")
     return ap.parse_args()
 
 
@@ -196,6 +197,151 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def run_batch(args, rank, world, local, dist):
+    """--workload batch24: 24 seeded uneven scans reconstructed as one batch
+    (mixed form: per-scan rebin + tensor-core filter, ONE persistent
+    backprojection launch over all scans, per-scan thickening, replayed as a
+    CUDA graph), against the same scans as per-scan FP32 launches."""
+    import numpy as np
+    import torch
+    from freect_b200 import abi_types as T
+    from freect_b200 import autotune, scans, wfbp
+
+    dev = torch.device("cuda", local)
+    specs = scans.batch_specs(seed=rank, n=24)
+    ctxs, raws, vols = [], [], []
+    for sp in specs:
+        tube, table = sp.views()
+        cg, gp = wfbp.configure_geometry(sp.meta(), table)
+        c = wfbp.Context(cg, sp.recon_config(), wfbp.make_ext(precision=T.PRECISION_MIXED, filter_window=sp.window),
+                         device=local)
+        c.set_views(tube, table)
+        ctxs.append(c)
+        r = c.alloc("raw")
+        wfbp.synth_project(sp.synth(), sp.ellipsoids(), r)
+        raws.append(r)
+        vols.append(c.alloc("volume"))
+    torch.cuda.synchronize()
+    batch = wfbp.Batch(ctxs)
+    stream = torch.cuda.Stream(device=dev)
+    tuned = None if args.no_tune else autotune.tune_batch(batch, raws, vols, use_cache=False)
+
+    # per-scan FP32 launches (the comparison) and the contributing updates
+    # (counted once per scan by the FP32 form, outside every timed region)
+    updates, fp32_ms, hu = 0, 0.0, []
+    for sp, r, v in zip(specs, raws, vols):
+        tube, table = sp.views()
+        cg, gp = wfbp.configure_geometry(sp.meta(), table)
+        c32 = wfbp.Context(cg, sp.recon_config(), wfbp.make_ext(filter_window=sp.window, tex_weights=1,
+                                                                filtered_layout=T.LAYOUT_BACKPROJECTION),
+                           device=local)
+        c32.set_views(tube, table)
+        reb, flt, vn, v32 = c32.alloc("rebinned"), c32.alloc("filtered"), c32.alloc("native"), c32.alloc("volume")
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        c32.rebin(r, reb)
+        c32.filter(reb, flt)
+        c32.backproject(flt, vn, update_count=cnt)
+        del reb, flt, vn
+        c32.run(r, v32)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c32.run(r, v32)
+        e1.record()
+        torch.cuda.synchronize()
+        fp32_ms += e0.elapsed_time(e1)
+        updates += int(cnt.item())
+        hu.append(v32)
+        c32.close()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batch.run(raws, vols)
+        stream.synchronize()
+        batch.check_device_status()
+        # mixed batch vs FP32 per scan, HU inside the full-coverage mask
+        hu_rms = []
+        for v, v32 in zip(vols, hu):
+            a, b = v.cpu().numpy(), v32.cpu().numpy()
+            m = np.isfinite(a) & np.isfinite(b)
+            hu_rms.append(float(np.sqrt(np.mean(((a[m] - b[m]) * 1000.0 / scans.MU_WATER) ** 2))) if m.any() else None)
+        del hu
+        clocks = ClockSampler(local)
+        clocks.start()
+        time.sleep(0.3)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            batch.run(raws, vols)
+        t1.record(stream)
+        stream.synchronize()
+        clk = clocks.stop()
+    ms = t0.elapsed_time(t1) / args.steps
+    tm = torch.tensor([ms], dtype=torch.float64, device=dev)
+    ua = torch.tensor([float(updates)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ua, op=dist.ReduceOp.SUM)
+    ms = float(tm.item())
+    value = float(ua.item()) / (ms / 1000.0)
+
+    e2e = None
+    if not args.no_e2e:
+        hr = [torch.empty(r.shape, dtype=torch.float32, pin_memory=True) for r in raws]
+        hv = [torch.empty(v.shape, dtype=torch.float32, pin_memory=True) for v in vols]
+        for a, b in zip(hr, raws):
+            a.copy_(b.cpu())
+        h2d = sum(r.numel() * 4 for r in raws)
+        d2h = sum(v.numel() * 4 for v in vols)
+
+        def e2e_step():
+            for a, b in zip(hr, raws):
+                b.copy_(a, non_blocking=True)
+            batch.run(raws, vols)
+            for a, b in zip(hv, vols):
+                a.copy_(b, non_blocking=True)
+
+        with torch.cuda.stream(stream):
+            e2e_step()
+            stream.synchronize()
+            if dist:
+                dist.barrier()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(args.steps):
+                e2e_step()
+            a1.record(stream)
+            stream.synchronize()
+        ems = a0.elapsed_time(a1) / args.steps
+        te = torch.tensor([ems], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        ems = float(te.item())
+        e2e = {"value": float(ua.item()) / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+    n_scans, n_items = batch.size()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16-storage/f32-accumulate",
+            "data": "synthetic (24 seeded uneven helical scans, ellipsoid phantoms, Poisson noise)",
+            "config": {"workload": "batch24", "scans": n_scans, "work_items": n_items,
+                       "shapes": ["%dx%dx%d/%d->%dx%dx%d" % (sp.nch, sp.nr, sp.P, sp.V, sp.nx, sp.ny, sp.n_slices)
+                                  for sp in specs],
+                       "precision": "mixed, one persistent backprojection launch, CUDA graph replay",
+                       "parallelism": "independent batch per GPU",
+                       "l2": "inputs larger than L2 (%.1f GB raw frames)" % (sum(r.numel() for r in raws) * 4 / 1e9),
+                       "bp_config": "%dx%d/%d" % batch.bp_config().key(),
+                       "bp_tuning_ms": tuned["times_ms"] if tuned else None},
+            "updates_per_step": updates, "fp32_per_scan_launches_ms": fp32_ms,
+            "speedup_vs_fp32_per_scan": fp32_ms / ms, "hu_rms_mixed_vs_fp32_per_scan": hu_rms,
+            "gpu_launches": 3 * n_scans + 1, "e2e": e2e, "clocks": clk}
+    batch.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -219,6 +365,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
+    if args.workload == "batch24":
+        run_batch(args, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     spec = scans.WORKLOADS[args.workload](seed=rank)
     tube, table = spec.views()
@@ -246,6 +397,13 @@ def main():
         ctx.backproject(filt, vn, scales, update_count=count)
         ctx.thicken(vn, vol)
 
+    tuned = None
+    if not args.no_tune:
+        # backprojection launch configuration from the autotuner (outside the timed region)
+        from freect_b200 import autotune
+        ctx.rebin(raw, reb)
+        ctx.filter(reb, filt, scales)
+        tuned = autotune.tune_backprojection(ctx, filt, vn, row_scales=scales, use_cache=False)
     step(cnt)  # counts the contributing updates once, outside the timed region
     torch.cuda.synchronize()
     updates = int(cnt.item())
@@ -335,7 +493,10 @@ def main():
             "config": {"workload": spec.name, "channels": spec.nch, "rows": spec.nr, "views": spec.V,
                        "volume": [d.n_slices_requested, d.ny, d.nx], "native_slices": d.n_slices_native,
                        "precision": args.precision, "parallelism": "independent scan per GPU",
-                       "l2": "inputs larger than L2 (2.2 GB raw frames)"},
+                       "l2": "inputs larger than L2 (%.2f GB raw frames, %.2f GB filtered rows)"
+                             % (d.raw_bytes / 1e9, d.filtered_bytes / 1e9),
+                       "bp_config": "%dx%d/%d" % ctx.bp_config().key(),
+                       "bp_tuning_ms": tuned["times_ms"] if tuned else None},
             "s_per_volume": ms / 1000.0, "updates_per_volume": updates, "stage_ms": stage,
             "roofline": roofline, "gpu_launches": 4 * args.steps, "e2e": e2e, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu:

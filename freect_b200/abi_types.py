@@ -135,6 +135,14 @@ class Dims(C.Structure):
     ]
 
 
+class BpConfig(C.Structure):
+    """wfbp_bp_config"""
+    _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("cols_per_step", C.c_int), ("reserved", C.c_int)]
+
+    def key(self):
+        return (self.tile_x, self.tile_y, self.cols_per_step)
+
+
 class Ellipsoid(C.Structure):
     """wfbp_ellipsoid"""
     _fields_ = [(n, C.c_double) for n in ("cx", "cy", "cz", "ax", "ay", "az", "phi", "mu")]

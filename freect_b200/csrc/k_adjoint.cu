@@ -1,0 +1,385 @@
+// Adjoint kernels of the FP32 path (sm_100a): the exact transposes of the
+// forward stages, for gradients with respect to the raw readings and the
+// filter taps. No counterpart in the reference, whose fct_wfbp has no
+// backward pass; each kernel states the forward loop it transposes.
+//
+// None of them uses atomics: every output element is owned by one thread,
+// which gathers the forward contributions that reach it (so results do not
+// depend on scheduling).
+#include "wfbp_internal.h"
+
+#include <math.h>
+
+#include "rebin_sample.cuh"
+
+namespace {
+
+// W(q) exactly as the forward backprojection (k_backproject.cu) evaluates it.
+__device__ __forceinline__ float q_weight_fwd(float qh) {
+  float t = __saturatef(fmaf(fabsf(qh), 2.5f, -1.5f));
+  return fmaf(0.5f, __cosf(3.14159265f * t), 0.5f);
+}
+
+// ---------------------------------------------------------------------------
+// backprojection adjoint
+// ---------------------------------------------------------------------------
+//
+// Forward (k_bp, the reference-layout FP32 backprojection): for voxel
+// (x, y, z) and half-turn angle t, with views j = t + k P/2,
+//   vol += dtheta / sum_k W_k * sum_k W_k * bilinear(D_j; p_idx_j, q_idx_j).
+// The gradient of one filtered sample D[j][r][c] is therefore
+//   sum over voxels of g_vol * dtheta * W_j / sum_k W_k * hat(p_idx_j - c) * hat_row,
+// where hat is the bilinear weight. Ownership: a CTA owns view j and a run of
+// AD_CH channels; thread c owns channel column c of that view and walks the
+// voxels whose p_idx lies within one channel of c (a band around a line
+// through the image, traversed along its longer axis). For each such voxel
+// it visits the slices inside the view's cone, recomputes sum_k W_k from the
+// same expressions as the forward, and adds the two row contributions to its
+// own column in shared memory.
+constexpr int AD_CH = 128;
+
+__device__ __forceinline__ float xcoord(const BPParams& p, int ix) {
+  return ((float)ix - 0.5f * ((float)p.nx - 1.0f)) * p.fov / (float)p.nx + p.x0;
+}
+__device__ __forceinline__ float ycoord(const BPParams& p, int iy) {
+  return ((float)iy - 0.5f * ((float)p.ny - 1.0f)) * p.fov / (float)p.ny + p.y0;
+}
+
+struct ViewGeo {
+  float zt, A, inv, p_idx;
+  bool valid_p;
+};
+
+__device__ __forceinline__ ViewGeo view_geo(const BPParams& p, float x, float y, float2 sc, float zt) {
+  ViewGeo g;
+  g.zt = zt;
+  const float p_hat = x * sc.x - y * sc.y;
+  const float l_hat = sqrtf(p.R2 - p_hat * p_hat) - x * sc.y - y * sc.x;
+  g.A = p.zr2pi * asinf(p.rR * p_hat);
+  g.inv = 1.0f / (l_hat * p.tanc);
+  g.p_idx = p.kp - (p_hat * p.ps + p.c0);
+  const float pf = floorf(g.p_idx);
+  g.valid_p = pf >= 0.0f && ceilf(g.p_idx) <= p.ncm2;
+  return g;
+}
+
+// Q weight of view geometry g at slice z (0 where the forward skips it).
+__device__ __forceinline__ float view_weight(const BPParams& p, const ViewGeo& g, float z, float* q_idx_out) {
+  const float dz = z - g.zt;
+  const float qh = (dz + g.A) * g.inv;
+  const float q_idx = (qh + 1.0f) * p.hn;
+  *q_idx_out = q_idx;
+  const bool ok = g.valid_p && fabsf(dz) <= p.z_rot && q_idx >= 0.0f && q_idx <= p.nrm2;
+  return ok ? q_weight_fwd(qh) : 0.0f;
+}
+
+__global__ void __launch_bounds__(AD_CH)
+k_bp_adjoint(const float* __restrict__ gvol, float* __restrict__ gD, const float2* __restrict__ view_sc,
+             const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, float z0, float dzs) {
+  extern __shared__ float col[];  // [nr][AD_CH], thread c owns column c
+  const int j = blockIdx.y;
+  const int cl = threadIdx.x;
+  const int c = blockIdx.x * AD_CH + cl;
+  for (int r = 0; r < p.nr; r++) col[r * AD_CH + cl] = 0.0f;
+
+  const int t = j % p.P2, kj = j / p.P2;
+  if (kj < p.K && c < p.nch) {
+    const float2 sc = __ldg(view_sc + j);
+    const float zt = __ldg(view_z + j);
+    // p_idx within (c - 1, c + 1) <=> p_hat in this interval (widened; the
+    // exact forward test below decides)
+    const float ph_a = (p.kp - p.c0 - ((float)c + 1.0f)) / p.ps, ph_b = (p.kp - p.c0 - ((float)c - 1.0f)) / p.ps;
+    const float marg = 0.5f / p.ps + 1e-3f * p.fov / (float)p.nx;
+    const float plo = fminf(ph_a, ph_b) - marg, phi = fmaxf(ph_a, ph_b) + marg;
+    const float sx = p.fov / (float)p.nx, sy = p.fov / (float)p.ny;
+    const float nxm = 0.5f * ((float)p.nx - 1.0f), nym = 0.5f * ((float)p.ny - 1.0f);
+    const bool along_y = fabsf(sc.x) >= fabsf(sc.y);  // p_hat = x sin - y cos: solve for x per row y
+    const int n_outer = along_y ? p.ny : p.nx;
+    for (int o = 0; o < n_outer; o++) {
+      int i_lo, i_hi;
+      if (along_y) {
+        const float y = ycoord(p, o);
+        float xa = (plo + y * sc.y) / sc.x, xb = (phi + y * sc.y) / sc.x;
+        if (xa > xb) { const float tt = xa; xa = xb; xb = tt; }
+        i_lo = max(0, (int)floorf((xa - p.x0) / sx + nxm) - 1);
+        i_hi = min(p.nx - 1, (int)ceilf((xb - p.x0) / sx + nxm) + 1);
+      } else {
+        const float x = xcoord(p, o);
+        float ya = (x * sc.x - phi) / sc.y, yb = (x * sc.x - plo) / sc.y;
+        if (ya > yb) { const float tt = ya; ya = yb; yb = tt; }
+        i_lo = max(0, (int)floorf((ya - p.y0) / sy + nym) - 1);
+        i_hi = min(p.ny - 1, (int)ceilf((yb - p.y0) / sy + nym) + 1);
+      }
+      for (int in = i_lo; in <= i_hi; in++) {
+        const int ix = along_y ? in : o, iy = along_y ? o : in;
+        const float x = xcoord(p, ix), y = ycoord(p, iy);
+        if (x * x + y * y > p.fov_half2) continue;  // cuda_kernels.cuh:220
+        const ViewGeo g = view_geo(p, x, y, sc, zt);
+        if (!g.valid_p) continue;
+        const float pf = floorf(g.p_idx), wp = g.p_idx - pf;
+        float hp;
+        if ((int)pf == c) hp = 1.0f - wp;
+        else if ((int)pf + 1 == c) hp = wp;
+        else continue;
+        if (hp == 0.0f) continue;
+        // slices that can pass this view's tests: |z - zt| <= z_rot and
+        // q_idx in [0, nr-2], a z interval around zt - A
+        const float za = zt - g.A - 1.0f / g.inv, zb = zt - g.A + (p.nrm2 / p.hn - 1.0f) / g.inv;
+        const float zlo = fmaxf(fminf(za, zb), zt - p.z_rot), zhi = fminf(fmaxf(za, zb), zt + p.z_rot);
+        if (zlo > zhi) continue;
+        int s_lo, s_hi;
+        if (p.nz == 1 || dzs == 0.0f) {
+          s_lo = 0;
+          s_hi = p.nz - 1;
+        } else {
+          float fa = (zlo - z0) / dzs, fb = (zhi - z0) / dzs;
+          if (fa > fb) { const float tt = fa; fa = fb; fb = tt; }
+          s_lo = max(0, (int)floorf(fa) - 2);
+          s_hi = min(p.nz - 1, (int)ceilf(fb) + 2);
+        }
+        for (int s = s_lo; s <= s_hi; s++) {
+          const float z = __ldg(zslices + s);
+          float q_idx;
+          const float Wj = view_weight(p, g, z, &q_idx);
+          if (Wj == 0.0f) continue;
+          const float gv = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix);
+          if (gv == 0.0f) continue;
+          // sum of the weights of all half turns, in the forward's order
+          float aw = 0.0f;
+          for (int k = 0; k < p.K; k++) {
+            const int jj = t + k * p.P2;
+            if (jj == j) {
+              aw += Wj;
+              continue;
+            }
+            const float ztk = __ldg(view_z + jj);
+            if (!(fabsf(z - ztk) <= p.z_rot)) continue;
+            const ViewGeo gk = view_geo(p, x, y, __ldg(view_sc + jj), ztk);
+            float qk;
+            aw += view_weight(p, gk, z, &qk);
+          }
+          const float cval = gv * (p.dtheta * (1.0f / aw)) * Wj * hp;  // cuda_kernels.cuh:283
+          const float qf = floorf(q_idx), wq = q_idx - qf;
+          const int r = min(max((int)qf, 0), p.nr - 2);
+          col[r * AD_CH + cl] += cval * (1.0f - wq);
+          col[(r + 1) * AD_CH + cl] += cval * wq;
+        }
+      }
+    }
+  }
+  if (c < p.nch) {
+    float* out = gD + (size_t)j * p.nr * p.nch + c;
+    for (int r = 0; r < p.nr; r++) out[(size_t)r * p.nch] = col[r * AD_CH + cl];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// thickening adjoint
+// ---------------------------------------------------------------------------
+// Forward: vol[r] = sum_n w_rn vol_n / ws_r over the CSR of requested slice r.
+// Transposed CSR (built on the host): native slice n lists (r, w_rn / ws_r).
+__global__ void k_thicken_adjoint(const float* __restrict__ gvol, float* __restrict__ gvn, const int* __restrict__ off,
+                                  const int* __restrict__ ridx, const float* __restrict__ w, int nxy, int nz) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)nxy * nz) return;
+  const int n = (int)(i / nxy);
+  const long px = i % nxy;
+  float acc = 0.0f;
+  for (int e = off[n]; e < off[n + 1]; e++) acc = fmaf(w[e], gvol[(size_t)ridx[e] * nxy + px], acc);
+  gvn[i] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// rebin adjoint
+// ---------------------------------------------------------------------------
+// Forward (rebin_sample, k_stages.cu): output sample (v, i, c) is the
+// bilinear texel sample of raw row nr-1-i at sheet column bidx[c] and sheet
+// view aidx(v, c), clamp addressing, sheet column x <- raw channel nch-1-x.
+// Column lists: sheet column x receives weight wx from channel c when one of
+// c's two clamped column taps is x (both taps, when they clamp to the same
+// column). Built once per context by k_rebin_adj_cols.
+__global__ void k_rebin_adj_cols(const float* __restrict__ bidx_t, int nch, int q8, int* __restrict__ cnt,
+                                 int* __restrict__ cidx, float* __restrict__ cw, int maxl, int* __restrict__ err) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= nch) return;
+  int n = 0;
+  // bidx is monotone in c with slope >= 1, so the channels reaching x lie near x
+  for (int c = 0; c < nch; c++) {
+    const float b = bidx_t[c];
+    if (isnan(b)) continue;
+    const float xb = (b + 0.5f) - 0.5f;
+    const float fx = floorf(xb);
+    float ax = xb - fx;
+    if (q8) ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
+    const int x0 = min(max((int)fx, 0), nch - 1), x1 = min(max((int)fx + 1, 0), nch - 1);
+    float wgt = 0.0f;
+    if (x0 == x) wgt += 1.0f - ax;
+    if (x1 == x) wgt += ax;
+    if (x0 != x && x1 != x) continue;
+    if (n == maxl) {
+      atomicOr(err, 0x400);
+      break;
+    }
+    cidx[x * maxl + n] = c;
+    cw[x * maxl + n] = wgt;
+    n++;
+  }
+  cnt[x] = n;
+}
+
+// Weight with which sheet view y enters output view v's sample of channel
+// (fan angle beta): the transposed row taps of rebin_sample.
+__device__ __forceinline__ float rebin_view_weight(int v, int y, float beta, float dth, int V, int q8, int voff) {
+  const float theta = (float)(v + voff) * dth;
+  const float alpha = theta - beta;
+  const float aidx = alpha / dth;
+  const float yb = (aidx + 0.5f) - 0.5f;
+  const float fy = floorf(yb);
+  float ay = yb - fy;
+  if (q8) ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
+  const int y0 = min(max((int)fy - voff, 0), V - 1), y1 = min(max((int)fy + 1 - voff, 0), V - 1);
+  float w = 0.0f;
+  if (y0 == y) w += 1.0f - ay;
+  if (y1 == y) w += ay;
+  return w;
+}
+
+// One thread per raw sample (reading y, raw row, raw channel).
+__global__ void k_rebin_adjoint(const float* __restrict__ gR, float* __restrict__ graw, const float* __restrict__ beta_t,
+                                const int* __restrict__ cnt, const int* __restrict__ cidx, const float* __restrict__ cw,
+                                int maxl, RebinParams p) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)p.V * p.nr * p.nch;
+  if (i >= total) return;
+  const int xr = (int)(i % p.nch);
+  const int rr = (int)((i / p.nch) % p.nr);
+  const int y = (int)(i / ((long)p.nch * p.nr));
+  const int x = p.nch - 1 - xr;   // sheet column
+  const int row = p.nr - 1 - rr;  // sheet row index i of the output
+  float acc = 0.0f;
+  const int n = cnt[x];
+  for (int e = 0; e < n; e++) {
+    const int c = cidx[x * maxl + e];
+    const float wx = cw[x * maxl + e];
+    const float beta = __ldg(beta_t + c);
+    const float sh = beta / p.dth;  // aidx ~ v - sh
+    int v_lo = (int)floorf((float)y + sh) - 2, v_hi = (int)ceilf((float)y + sh) + 2;
+    if (y == 0) v_lo = 0;            // every view whose taps clamp to the first reading
+    if (y == p.V - 1) v_hi = p.V - 1;  // ... or to the last
+    if (y == 0) v_hi = max(v_hi, (int)ceilf(sh) + 2);
+    if (y == p.V - 1) v_lo = min(v_lo, (int)floorf((float)(p.V - 1) + sh) - 2);
+    v_lo = max(v_lo, 0);
+    v_hi = min(v_hi, p.V - 1);
+    float sum = 0.0f;
+    for (int v = v_lo; v <= v_hi; v++) {
+      const float wy = rebin_view_weight(v, y, beta, p.dth, p.V, p.q8, p.voff);
+      if (wy != 0.0f) sum = fmaf(wy, __ldg(gR + ((size_t)v * p.nr + row) * p.nch + c), sum);
+    }
+    acc = fmaf(wx, sum, acc);
+  }
+  graw[i] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// filter-tap gradient, with the rebinned rows recomputed on the fly
+// ---------------------------------------------------------------------------
+// Forward: y[n] = sum_m h[|n - m|] x[m] over the nch channels of each row.
+// dL/dh[0] = sum_rows sum_n g[n] x[n]; dL/dh[d] = sum_rows sum_n g[n] (x[n-d] + x[n+d]).
+// A CTA takes TG_ROWS rows, recomputes their rebinned samples x from the raw
+// readings into shared memory (nothing of the rebinned array is stored), and
+// each thread correlates them with the incoming gradient rows for its taps.
+// Per-CTA partial sums are reduced in a fixed order by k_taps_reduce.
+constexpr int TG_ROWS = 8;
+constexpr int TG_THREADS = 128;
+
+__global__ void __launch_bounds__(TG_THREADS)
+k_taps_grad(const float* __restrict__ raw, const float* __restrict__ gY, const float* __restrict__ beta_t,
+            const float* __restrict__ bidx_t, RebinParams p, int ntaps, float* __restrict__ partial) {
+  extern __shared__ float sm[];
+  float* xs = sm;                        // [TG_ROWS][nch]
+  float* gs = sm + TG_ROWS * p.nch;      // [TG_ROWS][nch]
+  const long m0 = (long)blockIdx.x * TG_ROWS;
+  const long M = (long)p.V * p.nr;
+  const int rows = (int)min((long)TG_ROWS, M - m0);
+  for (int e = threadIdx.x; e < rows * p.nch; e += TG_THREADS) {
+    const int rr = e / p.nch, c = e % p.nch;
+    const long m = m0 + rr;
+    const int v = (int)(m / p.nr), i = (int)(m % p.nr);
+    xs[e] = wfbp_rebin_sample(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v, i);
+    gs[e] = __ldg(gY + m * p.nch + c);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < ntaps; d += TG_THREADS) {
+    float acc = 0.0f;
+    for (int rr = 0; rr < rows; rr++) {
+      const float* xr = xs + rr * p.nch;
+      const float* gr = gs + rr * p.nch;
+      if (d == 0) {
+        for (int n = 0; n < p.nch; n++) acc = fmaf(gr[n], xr[n], acc);
+      } else {
+        for (int n = d; n < p.nch; n++) acc = fmaf(gr[n], xr[n - d], acc);
+        for (int n = 0; n + d < p.nch; n++) acc = fmaf(gr[n], xr[n + d], acc);
+      }
+    }
+    partial[(size_t)blockIdx.x * ntaps + d] = acc;
+  }
+}
+
+__global__ void k_taps_reduce(const float* __restrict__ partial, int nblk, int ntaps, float* __restrict__ out) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= ntaps) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblk; b++) acc += (double)partial[(size_t)b * ntaps + d];
+  out[d] = (float)acc;
+}
+
+}  // namespace
+
+cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
+                              const BPParams& p, float z0, float dzs, cudaStream_t s) {
+  dim3 grid((unsigned)((p.nch + AD_CH - 1) / AD_CH), (unsigned)p.V);
+  const size_t smem = (size_t)p.nr * AD_CH * sizeof(float);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_bp_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_bp_adjoint<<<grid, AD_CH, smem, s>>>(gvol, gD, sc, vz, zs, p, z0, dzs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_thicken_adjoint(const float* gvol, float* gvn, const int* off, const int* ridx, const float* w,
+                                   int nxy, int nz, cudaStream_t s) {
+  const long n = (long)nxy * nz;
+  k_thicken_adjoint<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gvol, gvn, off, ridx, w, nxy, nz);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rebin_adj_cols(const float* bidx, int nch, int q8, int* cnt, int* cidx, float* cw, int maxl,
+                                  int* err, cudaStream_t s) {
+  k_rebin_adj_cols<<<(nch + 127) / 128, 128, 0, s>>>(bidx, nch, q8, cnt, cidx, cw, maxl, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rebin_adjoint(const float* gR, float* graw, const float* beta, const int* cnt, const int* cidx,
+                                 const float* cw, int maxl, const RebinParams& p, cudaStream_t s) {
+  const long n = (long)p.V * p.nr * p.nch;
+  k_rebin_adjoint<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gR, graw, beta, cnt, cidx, cw, maxl, p);
+  return cudaGetLastError();
+}
+
+int taps_grad_blocks(const RebinParams& p) { return (int)(((long)p.V * p.nr + TG_ROWS - 1) / TG_ROWS); }
+
+cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float* beta, const float* bidx,
+                                 const RebinParams& p, int ntaps, float* partial, float* out, cudaStream_t s) {
+  const int nblk = taps_grad_blocks(p);
+  const size_t smem = (size_t)2 * TG_ROWS * p.nch * sizeof(float);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_taps_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_taps_grad<<<nblk, TG_THREADS, smem, s>>>(raw, gY, beta, bidx, p, ntaps, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_taps_reduce<<<(ntaps + 127) / 128, 128, 0, s>>>(partial, nblk, ntaps, out);
+  return cudaGetLastError();
+}

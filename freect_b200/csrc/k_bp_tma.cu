@@ -36,9 +36,7 @@
 
 namespace {
 
-constexpr int BT_CWARPS = 16;                    // consumer warps
-constexpr int BT_THREADS = (BT_CWARPS + 1) * 32;  // + producer warp
-constexpr int BT_STAGES = 2;
+constexpr int BT_THREADS = (BT_CWARPS + 1) * 32;  // consumer warps + producer warp
 constexpr long long BT_SPIN = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -80,40 +78,68 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// W(q) of cuda_kernels.cuh:79-93 as a function of the row coordinate
-// q = (q_hat + 1) hn: |q_hat| = |q - hn| / hn.
-__device__ __forceinline__ float q_weight_row(float q, float hn, float k1) {
-  float t = __saturatef(fmaf(fabsf(q - hn), k1, -1.5f));
-  return fmaf(0.5f, __cosf(3.14159265f * t), 0.5f);
-}
-
-struct __align__(16) Geo {
-  float bq, cq, qlo, qhi;  // q(z) = bq z + cq; valid for qlo <= q <= qhi
-  int base;                // element offset of (channel pf, row 0) in the stage buffer
-  float wp;                // channel weight
-  float sv;                // per-view scale (FP16 rows) or 1
-  float pad;
+// Geometry of a pair of columns for one view, stored so that three 16-byte
+// shared-memory loads give both columns' fields as float2 operands of the
+// packed FP32x2 instructions (FFMA2 / FADD2 / FMUL2).
+struct __align__(16) GeoP {
+  float2 bq, cq;    // q(z) = bq z + cq
+  float2 qlo, qhi;  // valid for qlo <= q <= qhi
+  int2 addr;        // shared-memory byte offset of (channel pf, row 0) of the view's slot
+  float2 wp;        // FP32 rows: channel weight; half2 pairs: bits of the half2 (wp, wp)
 };
 
-template <typename T, int CPW, bool COUNT>
-__global__ void __launch_bounds__(BT_THREADS, 1)
-k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
-         const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
-         BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err) {
-  constexpr int TILE = BT_CWARPS * CPW;  // columns per CTA
-  extern __shared__ __align__(128) uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  uint8_t* slots = smem;  // [STAGES][nv_max][slot_bytes]
-  int2* vinfo = reinterpret_cast<int2*>(slots + (size_t)BT_STAGES * bt.nv_max * bt.slot_bytes);  // [STAGES][nv_max]
-  int* nvs = reinterpret_cast<int*>(vinfo + BT_STAGES * bt.nv_max);                             // [STAGES] (+pad)
-  Geo* geo = reinterpret_cast<Geo*>(nvs + 4);                                                  // [warps][nv_max][CPW]
-  uint64_t* full = reinterpret_cast<uint64_t*>(geo + BT_CWARPS * bt.nv_max * CPW);
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// Shared memory of a CTA: the mbarriers and small words at fixed offsets
+// (they persist across the tiles of a persistent launch), then the regions
+// of bp_smem_layout for the tile's scan.
+constexpr int BT_OFF_NVS = 64;  // int [16]: [0..1] views per stage, [8] failure flag, [9] next item
+
+__device__ __forceinline__ void bp_init_barriers(uint8_t* smem) {
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  if (threadIdx.x == 0) {
+    reinterpret_cast<int*>(smem + BT_OFF_NVS)[8] = 0;
+    for (int s = 0; s < BT_STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&full[BT_STAGES + s], BT_CWARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// One column tile (bt.tx x bt.ty columns, 32 slices from slab bz) of one scan.
+// `ring` counts the theta~ steps this CTA has run through its two-stage
+// ring before this tile (stage = ring & 1, phase = (ring >> 1) & 1), so a
+// persistent CTA continues the barriers' phases from tile to tile. Returns
+// the number of ring steps the tile used: p.P2, or 0 for a tile entirely
+// outside the reconstruction FOV (whose voxels are written as 0, the value
+// the reference leaves there). A bounded wait that gave up sets the failure
+// word (the CTA must stop).
+template <typename T, int CPW, int CU, bool COUNT>
+__device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __restrict__ view_scale,
+                                        float* __restrict__ vol, const float2* __restrict__ view_sc,
+                                        const float* __restrict__ view_z, const float* __restrict__ zslices,
+                                        const BPParams& p, const BPTile& bt, int bx, int by, int bz,
+                                        unsigned long long* __restrict__ count, int* __restrict__ err, uint8_t* smem,
+                                        uint32_t ring) {
+  constexpr bool HALF = !std::is_same<T, float>::value;
+  constexpr int NPW = CPW / 2;  // column pairs per warp
+  static_assert(CU % 2 == 0 && CPW % CU == 0, "columns per step must be even and divide the columns per warp");
+  const BpSmem L = bp_smem_layout(bt, CPW);
+  uint8_t* slots = smem + L.slots;                            // [STAGES][nv_max][slot_bytes]
+  int2* vinfo = reinterpret_cast<int2*>(smem + L.vinfo);      // [STAGES][nv_max] (view, first channel)
+  float* vsv = reinterpret_cast<float*>(smem + L.vsv);        // [STAGES][nv_max] per-view scale
+  int* nvs = reinterpret_cast<int*>(smem + BT_OFF_NVS);       // [STAGES] views, [8] failure flag
+  GeoP* geo = reinterpret_cast<GeoP*>(smem + L.geo);          // [warps][nv_max][NPW]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + BT_STAGES;
-  __shared__ int s_fail;
+  volatile int* s_fail = nvs + 8;
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int ix0 = blockIdx.x * bt.tx, iy0 = blockIdx.y * bt.ty;
-  const int s0 = blockIdx.z * 32;
+  const int ix0 = bx * bt.tx, iy0 = by * bt.ty;
+  const int s0 = bz * 32;
 
   // slab z range (all warps compute the same values)
   const int my_s = s0 + lane;
@@ -125,21 +151,29 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
     zmx = fmaxf(zmx, __shfl_xor_sync(0xffffffffu, zmx, o));
   }
 
-  if (threadIdx.x == 0) {
-    s_fail = 0;
-    for (int s = 0; s < BT_STAGES; s++) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], BT_CWARPS);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
-  __syncthreads();
-
   const float nxm = 0.5f * ((float)p.nx - 1.0f), nym = 0.5f * ((float)p.ny - 1.0f);
   auto xcoord = [&](int ix) { return ((float)ix - nxm) * p.fov / (float)p.nx + p.x0; };
   auto ycoord = [&](int iy) { return ((float)iy - nym) * p.fov / (float)p.ny + p.y0; };
-  const size_t slot_elems = (size_t)bt.slot_bytes / sizeof(T);
+
+  {
+    // the voxel centre of the tile nearest the isocentre; with a margin for
+    // rounding, a tile beyond the FOV circle holds no voxel the reference
+    // backprojects (cuda_kernels.cuh:220)
+    const float xa = xcoord(ix0), xb = xcoord(min(ix0 + bt.tx - 1, p.nx - 1));
+    const float ya = ycoord(iy0), yb = ycoord(min(iy0 + bt.ty - 1, p.ny - 1));
+    const float xn = fminf(fmaxf(0.0f, xa), xb), yn = fminf(fmaxf(0.0f, ya), yb);
+    if (xn * xn + yn * yn > p.fov_half2 * 1.0001f + 1e-3f) {
+      if (warp < BT_CWARPS && my_s < p.nz) {
+        const size_t plane = (size_t)p.nx * p.ny;
+        for (int c = 0; c < CPW; c++) {
+          const int tt = warp * CPW + c;
+          const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
+          if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = 0.0f;
+        }
+      }
+      return 0;
+    }
+  }
 
   if (warp == BT_CWARPS) {
     // ---------------- producer ----------------
@@ -150,12 +184,14 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
       const uint32_t view_bytes = (uint32_t)(bt.W * bt.nrp * sizeof(T));
       int issued_upto = 0;
       for (int t = 0; t < p.P2; t++) {
-        const int s = t & 1, u = t >> 1;
+        const uint32_t g = ring + (uint32_t)t;
+        const int s = (int)(g & 1u);
+        const uint32_t u = g >> 1;
         if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1)) {
-          atomicExch(&s_fail, 1);
+          *s_fail = 1;
           break;
         }
-        if (*((volatile int*)&s_fail)) break;
+        if (*s_fail) break;
         int nv = 0;
         for (int k = 0; k < p.K; k++) {
           const int j = t + k * p.P2;
@@ -183,23 +219,27 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
           int c_lo = (int)floorf(idx_min) - 1;
           c_lo = max(0, min(c_lo, p.nch - bt.W));
           vinfo[s * bt.nv_max + nv] = make_int2(j, c_lo);
+          vsv[s * bt.nv_max + nv] = HALF ? __ldg(view_scale + j) : 1.0f;
           nv++;
         }
         nvs[s] = nv;
         mbar_arrive_tx(&full[s], (uint32_t)nv * view_bytes);
         for (int v = 0; v < nv; v++) {
           const int2 vi = vinfo[s * bt.nv_max + v];
-          tma_load_3d(slots + ((size_t)s * bt.nv_max + v) * bt.slot_bytes, &map, &full[s], 0, vi.y, vi.x);
+          tma_load_3d(slots + ((size_t)s * bt.nv_max + v) * bt.slot_bytes, map, &full[s], 0, vi.y, vi.x);
         }
         issued_upto = t + 1;
       }
-      if (*((volatile int*)&s_fail)) {
+      if (*s_fail) {
         atomicExch(err, WFBP_ERR_TIMEOUT);
         // let copies already issued land before the CTA's shared memory goes away
-        for (int t = max(0, issued_upto - BT_STAGES); t < issued_upto; t++) mbar_wait(&full[t & 1], (t >> 1) & 1);
+        for (int t = max(0, issued_upto - BT_STAGES); t < issued_upto; t++) {
+          const uint32_t g = ring + (uint32_t)t;
+          mbar_wait(&full[g & 1u], (g >> 1) & 1u);
+        }
       }
     }
-    return;
+    return p.P2;
   }
 
   // ---------------- consumers ----------------
@@ -208,7 +248,7 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
   for (int c = 0; c < CPW; c++) vacc[c] = 0.0f;
   unsigned long long cnt = 0;
   const float k1 = 2.5f / p.hn;
-  Geo* wgeo = geo + (size_t)warp * bt.nv_max * CPW;
+  GeoP* wgeo = geo + (size_t)warp * bt.nv_max * NPW;
   constexpr int VPP = 32 / CPW;  // views per geometry pass
   const int gc = lane % CPW, gv = lane / CPW;
   const int gt = warp * CPW + gc;  // tile column handled by this lane in geometry passes
@@ -218,16 +258,23 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
   unsigned active_mask = 0;  // bit c: column c of this warp is inside the grid and the FOV
 #pragma unroll
   for (int c = 0; c < CPW; c++) active_mask |= (__shfl_sync(0xffffffffu, gactive ? 1u : 0u, c) & 1u) << c;
+  const int nrpb = bt.nrp * 4;  // bytes between channels of a slot
+  const float2 zl2 = make_float2(zl, zl);
+  const float2 mhn2 = make_float2(-p.hn, -p.hn);
+  const float2 pi2 = make_float2(3.14159265f, 3.14159265f);
+  const float2 half2c = make_float2(0.5f, 0.5f);
+  const unsigned nrm2u = (unsigned)(p.nr - 2);
 
   for (int t = 0; t < p.P2; t++) {
-    const int s = t & 1, u = t >> 1;
-    if (!mbar_wait(&full[s], u & 1)) {
-      atomicExch(&s_fail, 1);
+    const uint32_t g = ring + (uint32_t)t;
+    const int s = (int)(g & 1u);
+    const uint32_t u = g >> 1;
+    if (!mbar_wait(&full[s], u & 1u)) {
+      *s_fail = 1;
       atomicExch(err, WFBP_ERR_TIMEOUT);
       break;
     }
     const int nv = nvs[s];
-    const T* stage = reinterpret_cast<const T*>(slots + (size_t)s * bt.nv_max * bt.slot_bytes);
     // geometry of (column gc, view v) for v = gv, gv + VPP, ...
     for (int v = gv; v < nv; v += VPP) {
       const int2 vi = vinfo[s * bt.nv_max + v];
@@ -245,62 +292,100 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
         atomicOr(err, 0x200);  // channel window too narrow: host sizing violated
         valid = false;
       }
-      Geo g;
-      g.bq = inv * p.hn;
-      g.cq = p.hn * fmaf(A - zt, inv, 1.0f);
-      g.qlo = valid ? fmaxf(0.0f, fmaf(zt - p.z_rot, g.bq, g.cq)) : 3.0e38f;
-      g.qhi = valid ? fminf(p.nrm2, fmaf(zt + p.z_rot, g.bq, g.cq)) : -3.0e38f;
-      g.base = (int)((size_t)v * slot_elems) + (valid ? cofs : 0) * bt.nrp;
-      g.wp = p_idx - pf;
-      g.sv = std::is_same<T, float>::value ? 1.0f : __ldg(view_scale + vi.x);
-      g.pad = 0.0f;
-      wgeo[v * CPW + gc] = g;
+      const float bq = inv * p.hn;
+      const float cq = p.hn * fmaf(A - zt, inv, 1.0f);
+      const float wp = p_idx - pf;
+      float* gf = reinterpret_cast<float*>(wgeo + v * NPW + (gc >> 1)) + (gc & 1);
+      gf[0] = bq;
+      gf[2] = cq;
+      gf[4] = valid ? fmaxf(0.0f, fmaf(zt - p.z_rot, bq, cq)) : 3.0e38f;
+      gf[6] = valid ? fminf(p.nrm2, fmaf(zt + p.z_rot, bq, cq)) : -3.0e38f;
+      reinterpret_cast<int*>(gf)[8] =
+          (int)(L.slots + (size_t)(s * bt.nv_max + v) * bt.slot_bytes) + (valid ? cofs : 0) * nrpb;
+      if constexpr (HALF) {
+        const __half2 w2 = __float2half2_rn(wp);
+        gf[10] = __uint_as_float(*reinterpret_cast<const uint32_t*>(&w2));
+      } else {
+        gf[10] = wp;
+      }
     }
     __syncwarp();
-    // CU columns per step: CU independent accumulation chains per view
-    constexpr int CU = CPW >= 4 ? 4 : CPW;
-    const unsigned nrm2u = (unsigned)(p.nr - 2);
 #pragma unroll
     for (int c0 = 0; c0 < CPW; c0 += CU) {
       if (!((active_mask >> c0) & ((1u << CU) - 1u))) continue;
-      float ag[CU], aw[CU];
+      float2 ag[CU / 2], aw[CU / 2];
 #pragma unroll
-      for (int u = 0; u < CU; u++) { ag[u] = 0.0f; aw[u] = 0.0f; }
+      for (int u2 = 0; u2 < CU / 2; u2++) {
+        ag[u2] = make_float2(0.0f, 0.0f);
+        aw[u2] = make_float2(0.0f, 0.0f);
+      }
       for (int v = 0; v < nv; v++) {
+        float2 sv2 = make_float2(1.0f, 1.0f);
+        if constexpr (HALF) {
+          const float sv = vsv[s * bt.nv_max + v];
+          sv2 = make_float2(sv, sv);
+        }
+        const GeoP* gpv = wgeo + v * NPW + c0 / 2;
 #pragma unroll
-        for (int u = 0; u < CU; u++) {
-          const Geo g = wgeo[v * CPW + c0 + u];
-          const float q = fmaf(zl, g.bq, g.cq);
-          const bool ok = (q >= g.qlo) && (q <= g.qhi);
+        for (int u2 = 0; u2 < CU / 2; u2++) {
+          const GeoP g = gpv[u2];
+          const float2 q = __ffma2_rn(zl2, g.bq, g.cq);
+          const bool okx = (q.x >= g.qlo.x) && (q.x <= g.qhi.x);
+          const bool oky = (q.y >= g.qlo.y) && (q.y <= g.qhi.y);
           // any in-range row for invalid lanes (their weight is 0); NaN -> 0
-          const unsigned r = min((unsigned)__float2int_rz(q), nrm2u);
-          const float wq = q - (float)r;
-          const T* e = stage + g.base + r;
-          float top, bot;
-          if constexpr (std::is_same<T, float>::value) {
-            const float d00 = e[0], d01 = e[1], d10 = e[bt.nrp], d11 = e[bt.nrp + 1];
-            top = fmaf(g.wp, d10 - d00, d00);
-            bot = fmaf(g.wp, d11 - d01, d01);
+          const unsigned rx = min((unsigned)__float2int_rz(q.x), nrm2u);
+          const unsigned ry = min((unsigned)__float2int_rz(q.y), nrm2u);
+          const float2 wq = __fadd2_rn(q, make_float2(-(float)rx, -(float)ry));
+          const uint8_t* ex = smem + g.addr.x + (rx << 2);
+          const uint8_t* ey = smem + g.addr.y + (ry << 2);
+          float2 top, bot;
+          if constexpr (!HALF) {
+            const float2 d00 = make_float2(*reinterpret_cast<const float*>(ex), *reinterpret_cast<const float*>(ey));
+            const float2 d01 =
+                make_float2(*reinterpret_cast<const float*>(ex + 4), *reinterpret_cast<const float*>(ey + 4));
+            const float2 d10 = make_float2(*reinterpret_cast<const float*>(ex + nrpb),
+                                           *reinterpret_cast<const float*>(ey + nrpb));
+            const float2 d11 = make_float2(*reinterpret_cast<const float*>(ex + nrpb + 4),
+                                           *reinterpret_cast<const float*>(ey + nrpb + 4));
+            top = __ffma2_rn(g.wp, __fadd2_rn(d10, neg2(d00)), d00);
+            bot = __ffma2_rn(g.wp, __fadd2_rn(d11, neg2(d01)), d01);
           } else {
-            const uint32_t u0 = e[0], u1 = e[bt.nrp];
-            const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&u0));
-            const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&u1));
-            top = fmaf(g.wp, f1.x - f0.x, f0.x);
-            bot = fmaf(g.wp, f1.y - f0.y, f0.y);
+            // (row r, row r+1) pairs of channels pf and pf+1, interpolated
+            // across channels in half2 arithmetic
+            const __half2 h0x = *reinterpret_cast<const __half2*>(ex);
+            const __half2 h1x = *reinterpret_cast<const __half2*>(ex + nrpb);
+            const __half2 h0y = *reinterpret_cast<const __half2*>(ey);
+            const __half2 h1y = *reinterpret_cast<const __half2*>(ey + nrpb);
+            const uint32_t wbx = __float_as_uint(g.wp.x), wby = __float_as_uint(g.wp.y);
+            const __half2 wpx = *reinterpret_cast<const __half2*>(&wbx);
+            const __half2 wpy = *reinterpret_cast<const __half2*>(&wby);
+            const float2 fx = __half22float2(__hfma2(wpx, __hsub2(h1x, h0x), h0x));
+            const float2 fy = __half22float2(__hfma2(wpy, __hsub2(h1y, h0y), h0y));
+            top = make_float2(fx.x, fy.x);
+            bot = make_float2(fx.y, fy.y);
           }
-          const float gval = fmaf(wq, bot - top, top);
-          const float W = ok ? q_weight_row(q, p.hn, k1) : 0.0f;
-          if constexpr (std::is_same<T, float>::value)
-            ag[u] = fmaf(W, gval, ag[u]);
-          else
-            ag[u] = fmaf(W * g.sv, gval, ag[u]);
-          aw[u] += W;
-          if (COUNT) cnt += ok ? 1 : 0;
+          float2 gval = __ffma2_rn(wq, __fadd2_rn(bot, neg2(top)), top);
+          if constexpr (HALF) gval = __fmul2_rn(gval, sv2);
+          // W(q) of cuda_kernels.cuh:79-93 with |q_hat| = |q - hn| / hn
+          const float2 a = __fadd2_rn(q, mhn2);
+          const float2 tt = __fmul2_rn(make_float2(__saturatef(fmaf(fabsf(a.x), k1, -1.5f)),
+                                                   __saturatef(fmaf(fabsf(a.y), k1, -1.5f))),
+                                       pi2);
+          float2 W = __ffma2_rn(half2c, make_float2(__cosf(tt.x), __cosf(tt.y)), half2c);
+          W.x = okx ? W.x : 0.0f;
+          W.y = oky ? W.y : 0.0f;
+          ag[u2] = __ffma2_rn(W, gval, ag[u2]);
+          aw[u2] = __fadd2_rn(aw[u2], W);
+          if (COUNT) cnt += (okx ? 1 : 0) + (oky ? 1 : 0);
         }
       }
 #pragma unroll
-      for (int u = 0; u < CU; u++)
-        if ((active_mask >> (c0 + u)) & 1u) vacc[c0 + u] += p.dtheta * (1.0f / aw[u]) * ag[u];  // cuda_kernels.cuh:283
+      for (int u2 = 0; u2 < CU / 2; u2++) {
+        const int c = c0 + 2 * u2;
+        // cuda_kernels.cuh:283
+        if ((active_mask >> c) & 1u) vacc[c] += p.dtheta * (1.0f / aw[u2].x) * ag[u2].x;
+        if ((active_mask >> (c + 1)) & 1u) vacc[c + 1] += p.dtheta * (1.0f / aw[u2].y) * ag[u2].y;
+      }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
@@ -321,24 +406,90 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(count, cnt);
   }
+  return p.P2;
 }
 
-template <typename T, int CPW>
+// One tile per CTA: grid (tiles x, tiles y, 32-slice slabs).
+template <typename T, int CPW, int CU, bool COUNT>
+__global__ void __launch_bounds__(BT_THREADS, 1)
+k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
+         const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
+         BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err) {
+  // the dynamic shared memory is the only shared memory of this kernel, so
+  // it starts at the (128-byte aligned) base of the CTA's window
+  extern __shared__ __align__(128) uint8_t smem[];
+  bp_init_barriers(smem);
+  bp_tile<T, CPW, CU, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
+                             blockIdx.z, count, err, smem, 0u);
+}
+
+// Persistent launch over the column tiles of several scans: each CTA takes
+// the next work item (scan, tile x, tile y, slab) from a global counter until
+// the list is exhausted. Items are listed by decreasing estimated cost.
+template <typename T, int CPW, int CU>
+__global__ void __launch_bounds__(BT_THREADS, 1)
+k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items, int n_items,
+               unsigned* __restrict__ next, int* __restrict__ err) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  bp_init_barriers(smem);
+  volatile int* words = reinterpret_cast<volatile int*>(smem + BT_OFF_NVS);
+  uint32_t ring = 0;
+  for (;;) {
+    if (threadIdx.x == 0) words[9] = (int)atomicAdd(next, 1u);
+    __syncthreads();
+    const int it = words[9];
+    if (it >= n_items || words[8] != 0) break;
+    const int4 w = items[it];
+    const BpScan* sd = scans + w.x;
+    const BPParams p = sd->p;
+    const BPTile bt = sd->bt;
+    ring += (uint32_t)bp_tile<T, CPW, CU, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
+                                                 sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring);
+    __syncthreads();  // the tile's shared memory and words[9] are free again
+  }
+}
+
+template <typename T, int CPW, int CU>
 cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                        unsigned long long* count, int* err, cudaStream_t s) {
   dim3 grid((unsigned)((p.nx + bt.tx - 1) / bt.tx), (unsigned)((p.ny + bt.ty - 1) / bt.ty), (unsigned)((p.nz + 31) / 32));
   cudaError_t e;
   if (count) {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt.smem_bytes);
+    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, true><<<grid, BT_THREADS, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt, count, err);
+    k_bp_tma<T, CPW, CU, true><<<grid, BT_THREADS, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt, count,
+                                                                      err);
   } else {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt.smem_bytes);
+    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, false><<<grid, BT_THREADS, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt, count, err);
+    k_bp_tma<T, CPW, CU, false><<<grid, BT_THREADS, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
+                                                                       count, err);
   }
   return cudaGetLastError();
+}
+
+template <typename T, int CPW, int CU>
+cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
+                             int smem_bytes, int grid, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(k_bp_tma_batch<T, CPW, CU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes);
+  if (e != cudaSuccess) return e;
+  k_bp_tma_batch<T, CPW, CU><<<grid, BT_THREADS, smem_bytes, s>>>(scans, items, n_items, next, err);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
+                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
+                        unsigned long long* count, int* err, cudaStream_t s) {
+  const int cpw = bt.tx * bt.ty / BT_CWARPS;
+  if (cpw == 16 && bt.cu == 4) return launch_one<T, 16, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  if (cpw == 16 && bt.cu == 8) return launch_one<T, 16, 8>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  if (cpw == 8 && bt.cu == 4) return launch_one<T, 8, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  if (cpw == 8 && bt.cu == 8) return launch_one<T, 8, 8>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  if (cpw == 4 && bt.cu == 4) return launch_one<T, 4, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -346,35 +497,59 @@ cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* v
 // Shared-memory bytes of one launch configuration.
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes) {
   (void)elem_bytes;
+  return bp_smem_layout(bt, bt.tx * bt.ty / BT_CWARPS).total;
+}
+
+bool bp_tma_supported(const BPTile& bt) {
   const int cpw = bt.tx * bt.ty / BT_CWARPS;
-  return 128 + (size_t)BT_STAGES * bt.nv_max * bt.slot_bytes + (size_t)BT_STAGES * bt.nv_max * sizeof(int2) +
-         4 * sizeof(int) + (size_t)BT_CWARPS * bt.nv_max * cpw * sizeof(Geo) + 2 * BT_STAGES * sizeof(uint64_t);
+  if (bt.tx * bt.ty != cpw * BT_CWARPS) return false;
+  return (cpw == 16 && (bt.cu == 4 || bt.cu == 8)) || (cpw == 8 && (bt.cu == 4 || bt.cu == 8)) ||
+         (cpw == 4 && bt.cu == 4);
+}
+
+cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map) {
+  // 3-D map over [V][nch][nrp] 4-byte elements, box {nrp, W, 1}
+  EncodeTiledFn fn = wfbp_encode_tiled_fn();
+  if (!fn) return cudaErrorNotSupported;
+  cuuint64_t dims[3] = {(cuuint64_t)bt.nrp, (cuuint64_t)p.nch, (cuuint64_t)p.V};
+  cuuint64_t strides[2] = {(cuuint64_t)bt.nrp * 4, (cuuint64_t)bt.nrp * 4 * p.nch};
+  cuuint32_t box[3] = {(cuuint32_t)bt.nrp, (cuuint32_t)bt.W, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, elem_half2 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                  const_cast<void*>(D), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
                                    const float2* sc, const float* vz, const float* zs, const BPParams& p,
                                    const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s) {
-  // 3-D map over [V][nch][nrp] 4-byte elements, box {nrp, W, 1}
-  EncodeTiledFn fn = wfbp_encode_tiled_fn();
-  if (!fn) return cudaErrorNotSupported;
+  if (!bp_tma_supported(bt)) return cudaErrorInvalidValue;
   CUtensorMap map;
-  cuuint64_t dims[3] = {(cuuint64_t)bt.nrp, (cuuint64_t)p.nch, (cuuint64_t)p.V};
-  cuuint64_t strides[2] = {(cuuint64_t)bt.nrp * 4, (cuuint64_t)bt.nrp * 4 * p.nch};
-  cuuint32_t box[3] = {(cuuint32_t)bt.nrp, (cuuint32_t)bt.W, 1};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = fn(&map, elem_half2 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                  const_cast<void*>(D), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  const int cpw = bt.tx * bt.ty / BT_CWARPS;
+  cudaError_t e = bp_tma_encode_map(D, elem_half2, p, bt, &map);
+  if (e != cudaSuccess) return e;
+  if (elem_half2) return launch_elem<uint32_t>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  return launch_elem<float>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+}
+
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, const BpScan* scans, const int4* items,
+                                         int n_items, unsigned* next, int* err, int smem_bytes, int grid,
+                                         cudaStream_t s) {
+#define WFBP_BATCH_CASE(T, C, U)                                                                         \
+  if (cpw == C && cu == U) return launch_batch_one<T, C, U>(scans, items, n_items, next, err, smem_bytes, grid, s);
   if (elem_half2) {
-    if (cpw == 16) return launch_one<uint32_t, 16>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-    if (cpw == 8) return launch_one<uint32_t, 8>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-    if (cpw == 4) return launch_one<uint32_t, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+    WFBP_BATCH_CASE(uint32_t, 16, 4)
+    WFBP_BATCH_CASE(uint32_t, 16, 8)
+    WFBP_BATCH_CASE(uint32_t, 8, 4)
+    WFBP_BATCH_CASE(uint32_t, 8, 8)
+    WFBP_BATCH_CASE(uint32_t, 4, 4)
   } else {
-    if (cpw == 16) return launch_one<float, 16>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-    if (cpw == 8) return launch_one<float, 8>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-    if (cpw == 4) return launch_one<float, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+    WFBP_BATCH_CASE(float, 16, 4)
+    WFBP_BATCH_CASE(float, 16, 8)
+    WFBP_BATCH_CASE(float, 8, 4)
+    WFBP_BATCH_CASE(float, 8, 8)
+    WFBP_BATCH_CASE(float, 4, 4)
   }
+#undef WFBP_BATCH_CASE
   return cudaErrorInvalidValue;
 }

@@ -49,82 +49,7 @@ cudaError_t launch_rebin_tables(float* d_beta, float* d_bidx, int nch, float c0,
 // rebin
 // ---------------------------------------------------------------------------
 //
-// One output sample (v, i, c) of the reference's rebin of row sheet i
-// (cuda_kernels.cuh:11-39) read straight from the raw [reading][row][channel]
-// frames: the host reshape of ReconstructionMachine.cu:153-162 is folded into
-// the index math (sheet row i <- raw row nr-1-i, sheet column b <- raw
-// channel nch-1-b). The bilinear sample follows the texture unit's linear
-// filter with clamp addressing and texel centres at +0.5 (RM.cu:176-180).
-__device__ __forceinline__ float rebin_sample(const float* __restrict__ rawrow, size_t view_stride, int V,
-                                              int nch, float bidx, float beta, int v, float dth, int q8) {
-  if (isnan(bidx)) return 0.0f;
-  float theta = (float)v * dth;
-  float alpha = theta - beta;
-  float aidx = alpha / dth;
-  float xb = (bidx + 0.5f) - 0.5f;
-  float yb = (aidx + 0.5f) - 0.5f;
-  float fx = floorf(xb), fy = floorf(yb);
-  float ax = xb - fx, ay = yb - fy;
-  if (q8) {
-    ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
-    ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
-  }
-  int x0 = (int)fx, y0 = (int)fy;
-  int x1 = min(max(x0 + 1, 0), nch - 1), y1 = min(max(y0 + 1, 0), V - 1);
-  x0 = min(max(x0, 0), nch - 1);
-  y0 = min(max(y0, 0), V - 1);
-  const float* r0 = rawrow + (size_t)y0 * view_stride;
-  const float* r1 = rawrow + (size_t)y1 * view_stride;
-  float t00 = __ldg(r0 + (nch - 1 - x0)), t10 = __ldg(r0 + (nch - 1 - x1));
-  float t01 = __ldg(r1 + (nch - 1 - x0)), t11 = __ldg(r1 + (nch - 1 - x1));
-  return (1.0f - ax) * (1.0f - ay) * t00 + ax * (1.0f - ay) * t10 + (1.0f - ax) * ay * t01 + ax * ay * t11;
-}
-
-// Flying focal spot (no counterpart in the reference's WFBP): readings cycle
-// through G focal states (the state order of fct_icd's generate_ffs_offset,
-// applications/fct_icd/src/generate_system_matrix_ffs.cpp:242-290: phi bit =
-// state & 1, z bit = state >> 1 when both are on). A reading of phi state sp
-// samples effective channels 2b + sp, of z state sz effective rows 2r + sz.
-// The effective fan sample at fractional effective channel bidx is
-// interpolated between the two effective channels around it, each from its
-// own state's readings, linearly in reading angle between that state's
-// neighbouring readings (so no reading is assigned another reading's angle).
-__device__ __forceinline__ float rebin_sample_ffs(const float* __restrict__ raw, const RebinParams& p, float bidx,
-                                                  float beta, int v, int ie) {
-  if (isnan(bidx)) return 0.0f;
-  const int zs = p.zf ? (ie & 1) : 0, iraw = p.zf ? (ie >> 1) : ie;
-  const float* rawrow = raw + (size_t)(p.nr_raw - 1 - iraw) * p.nch_raw;
-  const size_t vs = (size_t)p.nr_raw * p.nch_raw;
-  const float nf = ((float)(p.G * v) * p.dth - beta) / p.dth;  // fractional reading index
-  const float fx = floorf(bidx);
-  float ax = bidx - fx;
-  if (p.q8) ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
-  float val = 0.0f;
-#pragma unroll
-  for (int t = 0; t < 2; t++) {
-    const int e = min(max((int)fx + t, 0), p.nch - 1);
-    const float we = t ? ax : 1.0f - ax;
-    const int sp = p.phi ? (e & 1) : 0, b = p.phi ? (e >> 1) : e;
-    const int rho = (p.G == 4) ? sp + 2 * zs : (p.phi ? sp : zs);
-    const float mf = (nf - (float)rho) / (float)p.G, m0 = floorf(mf);
-    float ay = mf - m0;
-    if (p.q8) ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
-    const int ma = min(max((int)m0, 0), p.V - 1), mb = min(max((int)m0 + 1, 0), p.V - 1);
-    const float t0 = __ldg(rawrow + (size_t)(p.G * ma + rho) * vs + (p.nch_raw - 1 - b));
-    const float t1 = __ldg(rawrow + (size_t)(p.G * mb + rho) * vs + (p.nch_raw - 1 - b));
-    val += we * ((1.0f - ay) * t0 + ay * t1);
-  }
-  return val;
-}
-
-// One rebinned sample of output view v, row i (flipped row-sheet index),
-// output channel with table entries (bidx, beta).
-__device__ __forceinline__ float sample_at(const float* __restrict__ raw, const RebinParams& p, float bidx, float beta,
-                                           int v, int i) {
-  if (p.G > 1) return rebin_sample_ffs(raw, p, bidx, beta, v, i);
-  return rebin_sample(raw + (size_t)(p.nr - 1 - i) * p.nch, (size_t)p.nr * p.nch, p.V, p.nch, bidx, beta, v, p.dth,
-                      p.q8);
-}
+#include "rebin_sample.cuh"
 
 // grid.x covers [V*nr] output rows (REB_ROWS per block), grid.y covers
 // channel quads; each thread writes 4 consecutive channels with one float4.
@@ -150,14 +75,14 @@ k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float*
   float* o = out + (size_t)row * p.nch;
   if (c + 3 < p.nch && (p.nch & 3) == 0) {
     float4 r;
-    r.x = sample_at(raw, p, s_bidx[tq * 4 + 0], s_beta[tq * 4 + 0], v, i);
-    r.y = sample_at(raw, p, s_bidx[tq * 4 + 1], s_beta[tq * 4 + 1], v, i);
-    r.z = sample_at(raw, p, s_bidx[tq * 4 + 2], s_beta[tq * 4 + 2], v, i);
-    r.w = sample_at(raw, p, s_bidx[tq * 4 + 3], s_beta[tq * 4 + 3], v, i);
+    r.x = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 0], s_beta[tq * 4 + 0], v, i);
+    r.y = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 1], s_beta[tq * 4 + 1], v, i);
+    r.z = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 2], s_beta[tq * 4 + 2], v, i);
+    r.w = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 3], s_beta[tq * 4 + 3], v, i);
     *reinterpret_cast<float4*>(o + c) = r;
   } else {
     for (int u = 0; u < 4; u++)
-      if (c + u < p.nch) o[c + u] = sample_at(raw, p, s_bidx[tq * 4 + u], s_beta[tq * 4 + u], v, i);
+      if (c + u < p.nch) o[c + u] = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + u], s_beta[tq * 4 + u], v, i);
   }
 }
 
@@ -335,7 +260,7 @@ k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, _
     if (i < p.nr) {
 #pragma unroll
       for (int u = 0; u < 4; u++)
-        if (c + u < p.nch) x[u] = sample_at(raw, p, __ldg(bidx_t + c + u), __ldg(beta_t + c + u), v, i);
+        if (c + u < p.nch) x[u] = wfbp_rebin_sample(raw, p, __ldg(bidx_t + c + u), __ldg(beta_t + c + u), v, i);
     }
     __align__(8) __nv_bfloat16 hi[4], lo[4];
     float amax = 0.0f;

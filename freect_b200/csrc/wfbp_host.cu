@@ -169,6 +169,13 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_thick_ws);
   free_dev(ctx->d_bplanes);
   free_dev(ctx->d_err);
+  free_dev(ctx->d_thickT_off);
+  free_dev(ctx->d_thickT_idx);
+  free_dev(ctx->d_thickT_w);
+  free_dev(ctx->d_radj_cnt);
+  free_dev(ctx->d_radj_idx);
+  free_dev(ctx->d_radj_w);
+  free_dev(ctx->d_tg_partial);
   free_dev(ctx->s_rebinned);
   free_dev(ctx->s_filtered);
   free_dev(ctx->s_scales);
@@ -253,16 +260,15 @@ void mixed_scale_ptrs(const wfbp_ctx* ctx, P rebinned, float** row_sc, float** v
 // channel window each view needs for it, and the most views of one theta~ that
 // can reach a 32-slice slab. Returns false if no configuration fits in shared
 // memory (the generic kernel is used then).
-bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
-  const int nrp = (ctx->nr + 3) / 4 * 4;
-  const double vx = ctx->rp.recon_fov / ctx->nx, vy = ctx->rp.recon_fov / ctx->ny;
+// Slab-level view reach and the most views of one theta~ that can reach a
+// 32-slice slab; both depend only on the geometry and the table positions.
+void bp_reach(wfbp_ctx* ctx, const std::vector<float>& table) {
   const double R = ctx->cg.distance_source_to_isocenter;
   const double rmax = 0.5 * ctx->cg.acquisition_field_of_view;
   const double tanc = ctx->gp.tanf_theta_cone;
   // |z - z_j| <= |A| + l_hat tan for any valid (voxel, view); tighter than z_rot
   const double cone = (R + rmax) * tanc + (ctx->cg.z_rot / (2 * M_PI)) * asin(std::min(1.0, rmax / R));
   const double reach = std::min((double)ctx->cg.z_rot, cone) + 1e-3 * (1.0 + fabs(ctx->cg.z_rot));
-  // views per theta~ reaching any 32-slice slab
   int nv_max = 0;
   const int nslab = (ctx->nz + 31) / 32;
   for (int sl = 0; sl < nslab; sl++) {
@@ -281,22 +287,40 @@ bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
       nv_max = std::max(nv_max, n);
     }
   }
-  if (nv_max == 0) nv_max = 1;
-  const int tiles[3][2] = {{16, 16}, {16, 8}, {8, 8}};
-  for (auto& tl : tiles) {
+  ctx->bp_reach = (float)reach;
+  ctx->bp_nv_max = std::max(1, nv_max);
+}
+
+// Sizes one TMA backprojection configuration; false if it does not fit.
+bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out) {
+  const double vx = ctx->rp.recon_fov / ctx->nx, vy = ctx->rp.recon_fov / ctx->ny;
+  BPTile b;
+  b.tx = tx;
+  b.ty = ty;
+  b.cu = cu;
+  const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
+  b.W = (int)ceil(ext * ctx->gp.pixel_scale) + 5;
+  b.W = std::max(4, std::min(b.W, 256));
+  b.nrp = (ctx->nr + 3) / 4 * 4;
+  b.nv_max = ctx->bp_nv_max;
+  b.slot_bytes = (int)((b.W * b.nrp * 4 + 127) / 128 * 128);
+  b.reach = ctx->bp_reach;
+  b.smem_bytes = 0;
+  if (!bp_tma_supported(b) || b.nrp > 256 || b.W > ctx->nch) return false;
+  const size_t smem = bp_tma_smem_bytes(b, 4);
+  if (smem > 220 * 1024) return false;
+  b.smem_bytes = (int)smem;
+  *out = b;
+  return true;
+}
+
+const int kBpCandidates[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 8, 4}, {16, 8, 8}, {8, 16, 4}, {8, 16, 8}, {8, 8, 4}};
+
+bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
+  bp_reach(ctx, table);
+  for (auto& c : kBpCandidates) {
     BPTile b;
-    b.tx = tl[0];
-    b.ty = tl[1];
-    const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
-    b.W = (int)ceil(ext * ctx->gp.pixel_scale) + 5;
-    b.W = std::max(4, std::min(b.W, 256));
-    b.nrp = nrp;
-    b.nv_max = nv_max;
-    b.slot_bytes = (int)((b.W * nrp * 4 + 127) / 128 * 128);
-    b.reach = (float)reach;
-    const size_t smem = bp_tma_smem_bytes(b, 4);
-    b.smem_bytes = (int)smem;
-    if (smem <= 220 * 1024 && nrp <= 256) {
+    if (size_bp_tile(ctx, c[0], c[1], c[2], &b)) {
       ctx->bpt = b;
       return true;
     }
@@ -399,6 +423,84 @@ WFBP_API const char* wfbp_last_error(const wfbp_ctx* ctx) { return ctx ? ctx->er
 // context
 // ---------------------------------------------------------------------------
 
+namespace {
+// Native / requested slice lists -> thickening weights (cuda_kernels.cuh:
+// 303-317, float arithmetic), their transpose for the adjoint, and the device
+// tables; re-sizes the backprojection launch when the views are known.
+int setup_slices(wfbp_ctx* ctx) {
+  ctx->nz = (int)ctx->z_native.size();
+  ctx->nzr = (int)ctx->z_req.size();
+  ctx->gp.n_slices_native = ctx->nz;
+  ctx->gp.n_slices_requested = ctx->nzr;
+  ctx->thick_off.assign(ctx->nzr + 1, 0);
+  ctx->thick_idx.clear();
+  ctx->thick_w.clear();
+  std::vector<float> ws(ctx->nzr, 0.0f);
+  for (int r = 0; r < ctx->nzr; r++) {
+    ctx->thick_off[r] = (int)ctx->thick_idx.size();
+    float wsum = 0.0f;
+    for (int i = 0; i < ctx->nz; i++) {
+      float w = fmaxf(0.0f, 1.0f - fabsf(ctx->z_native[i] - ctx->z_req[r]) / ctx->rp.slice_thickness);
+      if (w == 0.0f) continue;
+      wsum += w;
+      ctx->thick_idx.push_back(i);
+      ctx->thick_w.push_back(w);
+    }
+    ws[r] = wsum;
+  }
+  ctx->thick_off[ctx->nzr] = (int)ctx->thick_idx.size();
+  // transposed CSR for the adjoint: native slice -> (requested slice, w / sum w)
+  std::vector<int> tT_off(ctx->nz + 1, 0), tT_idx(ctx->thick_idx.size());
+  std::vector<float> tT_w(ctx->thick_idx.size());
+  for (size_t t = 0; t < ctx->thick_idx.size(); t++) tT_off[ctx->thick_idx[t] + 1]++;
+  for (int n = 0; n < ctx->nz; n++) tT_off[n + 1] += tT_off[n];
+  {
+    std::vector<int> fill(tT_off.begin(), tT_off.end() - 1);
+    for (int r = 0; r < ctx->nzr; r++)
+      for (int t = ctx->thick_off[r]; t < ctx->thick_off[r + 1]; t++) {
+        const int n = ctx->thick_idx[t];
+        tT_idx[fill[n]] = r;
+        tT_w[fill[n]] = ctx->thick_w[t] / ws[r];
+        fill[n]++;
+      }
+  }
+  DeviceGuard g(ctx->device);
+  free_dev(ctx->d_z_native);
+  free_dev(ctx->d_thick_off);
+  free_dev(ctx->d_thick_idx);
+  free_dev(ctx->d_thick_w);
+  free_dev(ctx->d_thick_ws);
+  free_dev(ctx->d_thickT_off);
+  free_dev(ctx->d_thickT_idx);
+  free_dev(ctx->d_thickT_w);
+  // the volume sizes may change: the context's own scratch is re-allocated on demand
+  free_dev(ctx->s_vol_native);
+  free_dev(ctx->s_vol);
+  auto up = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
+    cudaError_t e1 = cudaMalloc(dst, bytes > 0 ? bytes : 4);
+    if (e1 != cudaSuccess) return e1;
+    if (src && bytes) return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    return cudaSuccess;
+  };
+  cudaError_t ce = cudaSuccess;
+  if (!ce) ce = up((void**)&ctx->d_z_native, ctx->z_native.data(), sizeof(float) * ctx->nz);
+  if (!ce) ce = up((void**)&ctx->d_thick_off, ctx->thick_off.data(), sizeof(int) * ctx->thick_off.size());
+  if (!ce) ce = up((void**)&ctx->d_thick_idx, ctx->thick_idx.data(), sizeof(int) * ctx->thick_idx.size());
+  if (!ce) ce = up((void**)&ctx->d_thick_w, ctx->thick_w.data(), sizeof(float) * ctx->thick_w.size());
+  if (!ce) ce = up((void**)&ctx->d_thick_ws, ws.data(), sizeof(float) * ws.size());
+  if (!ce) ce = up((void**)&ctx->d_thickT_off, tT_off.data(), sizeof(int) * tT_off.size());
+  if (!ce) ce = up((void**)&ctx->d_thickT_idx, tT_idx.data(), sizeof(int) * tT_idx.size());
+  if (!ce) ce = up((void**)&ctx->d_thickT_w, tT_w.data(), sizeof(float) * tT_w.size());
+  if (ce) return fail(ctx, ce == cudaErrorMemoryAllocation ? WFBP_ERR_OOM : WFBP_ERR_CUDA, "slice tables");
+  if (ctx->views_set) {
+    const int nrp = ctx->bpt.nrp;
+    ctx->bp_tma_ok = choose_bp_tile(ctx, ctx->view_table);
+    ctx->bpt.nrp = nrp;
+  }
+  return WFBP_OK;
+}
+}  // namespace
+
 WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const wfbp_ext* ext, int device,
                              wfbp_ctx** out) {
   if (!cg || !rp || !out) return WFBP_ERR_INVALID_ARG;
@@ -476,31 +578,10 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
 
   int st = slice_lists(cg, rp, ctx->z_native, ctx->z_req);
   if (st) { delete ctx; return st; }
-  ctx->nz = (int)ctx->z_native.size();
-  ctx->nzr = (int)ctx->z_req.size();
-  gp.n_slices_native = ctx->nz;
-  gp.n_slices_requested = ctx->nzr;
 
   ctx->taps.resize(ctx->nch);
   st = make_taps(cg, e.filter_window, e.filter_c, e.filter_a, e.user_taps, e.n_user_taps, ctx->taps.data(), ctx->nch);
   if (st) { delete ctx; return st; }
-
-  // thickening weights (cuda_kernels.cuh:303-317), float arithmetic
-  ctx->thick_off.assign(ctx->nzr + 1, 0);
-  std::vector<float> ws(ctx->nzr, 0.0f);
-  for (int r = 0; r < ctx->nzr; r++) {
-    ctx->thick_off[r] = (int)ctx->thick_idx.size();
-    float wsum = 0.0f;
-    for (int i = 0; i < ctx->nz; i++) {
-      float w = fmaxf(0.0f, 1.0f - fabsf(ctx->z_native[i] - ctx->z_req[r]) / rp->slice_thickness);
-      if (w == 0.0f) continue;
-      wsum += w;
-      ctx->thick_idx.push_back(i);
-      ctx->thick_w.push_back(w);
-    }
-    ws[r] = wsum;
-  }
-  ctx->thick_off[ctx->nzr] = (int)ctx->thick_idx.size();
 
   DeviceGuard g(device);
   auto alloc_copy = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
@@ -515,11 +596,6 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
   if (!ce) ce = alloc_copy((void**)&ctx->d_chan_bidx, nullptr, sizeof(float) * ctx->nch);
   if (!ce) ce = alloc_copy((void**)&ctx->d_view_sc, nullptr, sizeof(float2) * ctx->V);
   if (!ce) ce = alloc_copy((void**)&ctx->d_view_z, nullptr, sizeof(float) * ctx->V);
-  if (!ce) ce = alloc_copy((void**)&ctx->d_z_native, ctx->z_native.data(), sizeof(float) * ctx->nz);
-  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_off, ctx->thick_off.data(), sizeof(int) * ctx->thick_off.size());
-  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_idx, ctx->thick_idx.data(), sizeof(int) * ctx->thick_idx.size());
-  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_w, ctx->thick_w.data(), sizeof(float) * ctx->thick_w.size());
-  if (!ce) ce = alloc_copy((void**)&ctx->d_thick_ws, ws.data(), sizeof(float) * ws.size());
   if (!ce) ce = alloc_copy((void**)&ctx->d_err, nullptr, sizeof(int));
   if (!ce) ce = cudaMemset(ctx->d_err, 0, sizeof(int));
   if (!ce && e.precision == WFBP_PRECISION_MIXED) {
@@ -553,6 +629,12 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     release(ctx);
     delete ctx;
     return code;
+  }
+  st = setup_slices(ctx);
+  if (st) {
+    release(ctx);
+    delete ctx;
+    return st;
   }
   *out = ctx;
   return WFBP_OK;
@@ -612,10 +694,82 @@ WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table
   cudaFree(d_t);
   cudaFree(d_z);
   CUDA_TRY(ctx, e);
+  ctx->view_table.assign(table, table + ctx->V);
   const int nrp = ctx->bpt.nrp;
-  ctx->bp_tma_ok = choose_bp_tile(ctx, std::vector<float>(table, table + ctx->V));
+  ctx->bp_tma_ok = choose_bp_tile(ctx, ctx->view_table);
   ctx->bpt.nrp = nrp;
   ctx->views_set = true;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_set_reading_offset(wfbp_ctx* ctx, int offset) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (offset < 0 || offset % ctx->G != 0)
+    return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_reading_offset: need a non-negative multiple of the readings per view");
+  ctx->reading_offset = offset;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_set_slices(wfbp_ctx* ctx, const float* native_z, int n_native, const float* requested_z,
+                             int n_requested) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!native_z || !requested_z || n_native < 1 || n_requested < 1)
+    return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_slices: need at least one native and one requested slice");
+  for (int i = 0; i < n_native; i++)
+    if (!isfinite(native_z[i])) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_slices: non-finite native z");
+  for (int i = 0; i < n_requested; i++)
+    if (!isfinite(requested_z[i])) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_slices: non-finite requested z");
+  // monotone native list (the backprojection adjoint and the slab planning rely on it)
+  if (n_native >= 2 && !(native_z[1] != native_z[0]))
+    return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_slices: native slices must be strictly monotone");
+  for (int i = 2; i < n_native; i++)
+    if ((native_z[i] - native_z[i - 1]) * (native_z[1] - native_z[0]) <= 0.0f)
+      return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_slices: native slices must be strictly monotone");
+  ctx->z_native.assign(native_z, native_z + n_native);
+  ctx->z_req.assign(requested_z, requested_z + n_requested);
+  return setup_slices(ctx);
+}
+
+WFBP_API int wfbp_bp_configs(const wfbp_ctx* ctx, wfbp_bp_config* out, int cap, int* n) {
+  if (!ctx || !n || cap < 0 || (cap > 0 && !out)) return WFBP_ERR_INVALID_ARG;
+  if (!ctx->views_set) return WFBP_ERR_STATE;
+  int k = 0;
+  for (auto& c : kBpCandidates) {
+    BPTile b;
+    if (!size_bp_tile(ctx, c[0], c[1], c[2], &b)) continue;
+    if (k < cap) {
+      out[k].tile_x = c[0];
+      out[k].tile_y = c[1];
+      out[k].cols_per_step = c[2];
+      out[k].reserved = 0;
+    }
+    k++;
+  }
+  *n = k;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_get_bp_config(const wfbp_ctx* ctx, wfbp_bp_config* c) {
+  if (!ctx || !c) return WFBP_ERR_INVALID_ARG;
+  if (!ctx->views_set) return WFBP_ERR_STATE;
+  if (!ctx->bp_tma_ok) return WFBP_ERR_UNSUPPORTED;
+  c->tile_x = ctx->bpt.tx;
+  c->tile_y = ctx->bpt.ty;
+  c->cols_per_step = ctx->bpt.cu;
+  c->reserved = 0;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* c) {
+  if (!ctx || !c) return WFBP_ERR_INVALID_ARG;
+  if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_set_bp_config: call wfbp_set_views first");
+  BPTile b;
+  if (!size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, &b))
+    return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_set_bp_config: configuration " + std::to_string(c->tile_x) + "x" +
+                                               std::to_string(c->tile_y) + "/" + std::to_string(c->cols_per_step) +
+                                               " is not supported for this geometry");
+  ctx->bpt = b;
+  ctx->bp_tma_ok = true;
   return WFBP_OK;
 }
 
@@ -649,10 +803,8 @@ WFBP_API int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* reques
 // stages
 // ---------------------------------------------------------------------------
 
-WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream) {
-  if (!ctx) return WFBP_ERR_INVALID_ARG;
-  if (!raw || !rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin: null buffer");
-  DeviceGuard g(ctx->device);
+namespace {
+RebinParams rebin_params(const wfbp_ctx* ctx) {
   RebinParams p;
   p.V = ctx->V;
   p.nr = ctx->nr;
@@ -664,6 +816,16 @@ WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* s
   p.zf = ctx->cg_read.ffs_z ? 1 : 0;
   p.nch_raw = ctx->raw_ch;
   p.nr_raw = ctx->raw_rows;
+  p.voff = ctx->reading_offset / ctx->G;
+  return p;
+}
+}  // namespace
+
+WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw || !rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin: null buffer");
+  DeviceGuard g(ctx->device);
+  const RebinParams p = rebin_params(ctx);
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
     float *row_sc, *view_sc;
     mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
@@ -764,6 +926,112 @@ WFBP_API int wfbp_thicken(wfbp_ctx* ctx, const float* vn, float* vol, void* stre
   return WFBP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// adjoints (FP32 form)
+// ---------------------------------------------------------------------------
+
+namespace {
+int require_fp32_views(wfbp_ctx* ctx, const char* what) {
+  if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, std::string(what) + ": wfbp_set_views not called");
+  if (ctx->ext.precision != WFBP_PRECISION_FP32)
+    return fail(ctx, WFBP_ERR_UNSUPPORTED, std::string(what) + ": the adjoints are those of the FP32 form");
+  return WFBP_OK;
+}
+}  // namespace
+
+WFBP_API int wfbp_set_taps(wfbp_ctx* ctx, const float* taps, int n, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!taps || n < 1 || n > ctx->nch)
+    return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_set_taps: need 1 <= n <= channels taps");
+  if (ctx->ext.precision != WFBP_PRECISION_FP32)
+    return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_set_taps: the mixed form bakes its taps into the operand planes");
+  DeviceGuard g(ctx->device);
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_taps, taps, sizeof(float) * n, cudaMemcpyDefault, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_get_taps(wfbp_ctx* ctx, float* taps, void* stream) {
+  if (!ctx || !taps) return WFBP_ERR_INVALID_ARG;
+  DeviceGuard g(ctx->device);
+  CUDA_TRY(ctx, cudaMemcpyAsync(taps, ctx->d_taps, sizeof(float) * ctx->nch, cudaMemcpyDefault, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_thicken_adjoint(wfbp_ctx* ctx, const float* g_volume, float* g_native, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!g_volume || !g_native) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_thicken_adjoint: null buffer");
+  DeviceGuard g(ctx->device);
+  CUDA_TRY(ctx, launch_thicken_adjoint(g_volume, g_native, ctx->d_thickT_off, ctx->d_thickT_idx, ctx->d_thickT_w,
+                                       ctx->nx * ctx->ny, ctx->nz, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, float* g_filtered, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!g_native || !g_filtered) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_backproject_adjoint: null buffer");
+  int st = require_fp32_views(ctx, "wfbp_backproject_adjoint");
+  if (st) return st;
+  DeviceGuard g(ctx->device);
+  const BPParams p = bp_params(ctx);
+  const float z0 = ctx->z_native[0];
+  const float dzs = ctx->nz > 1 ? (ctx->z_native[ctx->nz - 1] - ctx->z_native[0]) / (float)(ctx->nz - 1) : 0.0f;
+  CUDA_TRY(ctx, launch_bp_adjoint(g_native, g_filtered, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, z0, dzs,
+                                  (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_filter_adjoint(wfbp_ctx* ctx, const float* g_filtered, float* g_rebinned, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!g_filtered || !g_rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter_adjoint: null buffer");
+  int st = require_fp32_views(ctx, "wfbp_filter_adjoint");
+  if (st) return st;
+  DeviceGuard g(ctx->device);
+  // the Toeplitz operator h[|n - m|] is symmetric: its transpose is itself
+  CUDA_TRY(ctx, launch_filter_f32(g_filtered, g_rebinned, ctx->d_taps, (long)ctx->V * ctx->nr, ctx->nch,
+                                  (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_rebin_adjoint(wfbp_ctx* ctx, const float* g_rebinned, float* g_raw, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!g_rebinned || !g_raw) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin_adjoint: null buffer");
+  int st = require_fp32_views(ctx, "wfbp_rebin_adjoint");
+  if (st) return st;
+  if (ctx->G != 1) return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_rebin_adjoint: flying focal spot scans");
+  DeviceGuard g(ctx->device);
+  constexpr int kMaxL = 8;
+  if (!ctx->d_radj_cnt) {
+    CUDA_TRY(ctx, cudaMalloc(&ctx->d_radj_cnt, sizeof(int) * ctx->nch));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->d_radj_idx, sizeof(int) * ctx->nch * kMaxL));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->d_radj_w, sizeof(float) * ctx->nch * kMaxL));
+    CUDA_TRY(ctx, launch_rebin_adj_cols(ctx->d_chan_bidx, ctx->nch, ctx->ext.tex_weights ? 1 : 0, ctx->d_radj_cnt,
+                                        ctx->d_radj_idx, ctx->d_radj_w, kMaxL, ctx->d_err, (cudaStream_t)stream));
+  }
+  CUDA_TRY(ctx, launch_rebin_adjoint(g_rebinned, g_raw, ctx->d_chan_beta, ctx->d_radj_cnt, ctx->d_radj_idx,
+                                     ctx->d_radj_w, kMaxL, rebin_params(ctx), (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_filtered, float* g_taps, int n,
+                                void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw || !g_filtered || !g_taps) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_taps_gradient: null buffer");
+  if (n < 1 || n > ctx->nch) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_taps_gradient: need 1 <= n <= channels");
+  int st = require_fp32_views(ctx, "wfbp_taps_gradient");
+  if (st) return st;
+  DeviceGuard g(ctx->device);
+  const RebinParams p = rebin_params(ctx);
+  const size_t need = (size_t)taps_grad_blocks(p) * n;
+  if (need > ctx->tg_partial_n) {
+    free_dev(ctx->d_tg_partial);
+    CUDA_TRY(ctx, cudaMalloc(&ctx->d_tg_partial, sizeof(float) * need));
+    ctx->tg_partial_n = need;
+  }
+  CUDA_TRY(ctx, launch_taps_gradient(raw, g_filtered, ctx->d_chan_beta, ctx->d_chan_bidx, p, n, ctx->d_tg_partial,
+                                     g_taps, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
 namespace {
 // wfbp_run's own layout: the backprojection layout whenever a launch fits.
 int run_layout(const wfbp_ctx* ctx) {
@@ -826,3 +1094,27 @@ WFBP_API int wfbp_synth_project(const wfbp_synth_scan* scan, const wfbp_ellipsoi
   if (e != cudaSuccess) return e == cudaErrorInvalidValue ? WFBP_ERR_INVALID_ARG : WFBP_ERR_CUDA;
   return WFBP_OK;
 }
+
+// ---------------------------------------------------------------------------
+// internal entry points for the other host translation units
+// ---------------------------------------------------------------------------
+
+namespace wfbp_detail {
+int set_error(wfbp_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
+BPParams backprojection_params(const wfbp_ctx* ctx) { return bp_params(ctx); }
+void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal) {
+  stage_bytes(ctx, layout, reb, filt, scal);
+}
+bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out) {
+  return size_bp_tile(ctx, tx, ty, cu, out);
+}
+int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
+  return do_filter(ctx, rebinned, filtered, scales, layout, stream);
+}
+int n_bp_candidates() { return (int)(sizeof(kBpCandidates) / sizeof(kBpCandidates[0])); }
+void bp_candidate(int i, int* tx, int* ty, int* cu) {
+  *tx = kBpCandidates[i][0];
+  *ty = kBpCandidates[i][1];
+  *cu = kBpCandidates[i][2];
+}
+}  // namespace wfbp_detail

@@ -44,7 +44,33 @@ struct BPTile {
   int slot_bytes;    // bytes per view slot (multiple of 128)
   float reach;       // slab-level half width of the table-position prefilter (mm)
   int smem_bytes;    // dynamic shared memory of the launch
+  int cu;            // columns accumulated per step of the view loop (4 or 8)
 };
+
+// Byte offsets of the TMA backprojection's shared-memory regions; the same
+// function sizes the launch on the host and carves the buffer on the device.
+constexpr int BT_CWARPS = 16;  // consumer warps of the TMA backprojection
+constexpr int BT_STAGES = 2;   // view-window ring depth
+struct BpSmem {
+  unsigned slots, vinfo, vsv, geo, total;
+};
+// Bytes 0..127 hold the ring's mbarriers and a few words (fixed across the
+// tiles of a persistent launch); the per-scan regions follow.
+__host__ __device__ inline BpSmem bp_smem_layout(const BPTile& bt, int cpw) {
+  BpSmem L;
+  unsigned o = 128;
+  L.slots = o;  // [STAGES][nv_max][slot_bytes], 128-byte aligned TMA destinations
+  o += (unsigned)(BT_STAGES * bt.nv_max * bt.slot_bytes);
+  L.vinfo = o;
+  o += (unsigned)(BT_STAGES * bt.nv_max * 8);
+  L.vsv = o;
+  o += (unsigned)(BT_STAGES * bt.nv_max * 4);
+  o = (o + 15u) & ~15u;
+  L.geo = o;
+  o += (unsigned)(BT_CWARPS * bt.nv_max * (cpw / 2) * 48);  // column-pair geometry records
+  L.total = o;
+  return L;
+}
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -58,6 +84,7 @@ struct RebinParams {
   int G;                     // readings per view: 1, or 2 / 4 with a flying focal spot
   int phi, zf;               // FFS in channel / row direction
   int nch_raw, nr_raw;       // raw frame shape
+  int voff;                  // index of the first view within the whole scan (wfbp_set_reading_offset / G)
 };
 
 struct wfbp_ctx {
@@ -71,7 +98,9 @@ struct wfbp_ctx {
 
   int V = 0, nr = 0, nch = 0, P = 0, P2 = 0, K = 0, nx = 0, ny = 0, nz = 0, nzr = 0;
   int n_readings = 0, raw_rows = 0, raw_ch = 0;
+  int reading_offset = 0;           // first reading's index within the whole scan
   std::vector<float> z_native, z_req;
+  std::vector<float> view_table;    // table position of each view (host copy)
   std::vector<float> taps;          // symmetric half taps h[0..nch-1]
   std::vector<int> thick_off;       // CSR over requested slices
   std::vector<int> thick_idx;
@@ -88,6 +117,16 @@ struct wfbp_ctx {
   int* d_thick_idx = nullptr;
   float* d_thick_w = nullptr;
   float* d_thick_ws = nullptr;      // [nzr] sum of weights
+  int* d_thickT_off = nullptr;      // transposed CSR over native slices: (requested slice, w / sum w)
+  int* d_thickT_idx = nullptr;
+  float* d_thickT_w = nullptr;
+
+  // adjoints
+  int* d_radj_cnt = nullptr;        // rebin adjoint: per sheet column, the channels reaching it
+  int* d_radj_idx = nullptr;
+  float* d_radj_w = nullptr;
+  float* d_tg_partial = nullptr;    // per-CTA partial tap gradients
+  size_t tg_partial_n = 0;
 
   // mixed precision: Toeplitz operand planes for the tensor-core filter
   int tc_kp = 0, tc_np = 0, tc_bn = 0;
@@ -99,6 +138,8 @@ struct wfbp_ctx {
   // TMA-staged backprojection (backprojection layout [V][nch][nrp])
   bool bp_tma_ok = false;
   BPTile bpt;
+  float bp_reach = 0.0f;            // slab-level view prefilter half width (mm)
+  int bp_nv_max = 1;                // most views of one theta~ reaching a slab
 
   // context-owned scratch for wfbp_run / wfbp_run_host
   void* s_rebinned = nullptr;
@@ -145,12 +186,50 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
                              const TcOutArgs& out, int* err, cudaStream_t s);
 cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps, long rows, int nch, int nr, int nrp,
                                  cudaStream_t s);
+// One scan of a persistent (batched) backprojection launch, in device memory.
+struct alignas(64) BpScan {
+  CUtensorMap map;              // filtered rows [V][nch][nrp], box {nrp, W, 1}
+  BPParams p;
+  BPTile bt;
+  const float* view_scale;      // per-view scales (FP16 row pairs) or null
+  float* vol;                   // native volume
+  const float2* view_sc;
+  const float* view_z;
+  const float* zslices;
+};
+cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map);
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, const BpScan* scans, const int4* items,
+                                         int n_items, unsigned* next, int* err, int smem_bytes, int grid,
+                                         cudaStream_t s);
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);
+bool bp_tma_supported(const BPTile& bt);
 cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
                                    const float2* sc, const float* vz, const float* zs, const BPParams& p,
                                    const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s);
 int tc_choose_bn(int nch);
 cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
                            const float* ws, int nxy, int nzr, cudaStream_t s);
+cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
+                              const BPParams& p, float z0, float dzs, cudaStream_t s);
+cudaError_t launch_thicken_adjoint(const float* gvol, float* gvn, const int* off, const int* ridx, const float* w,
+                                   int nxy, int nz, cudaStream_t s);
+cudaError_t launch_rebin_adj_cols(const float* bidx, int nch, int q8, int* cnt, int* cidx, float* cw, int maxl,
+                                  int* err, cudaStream_t s);
+cudaError_t launch_rebin_adjoint(const float* gR, float* graw, const float* beta, const int* cnt, const int* cidx,
+                                 const float* cw, int maxl, const RebinParams& p, cudaStream_t s);
+int taps_grad_blocks(const RebinParams& p);
+cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float* beta, const float* bidx,
+                                 const RebinParams& p, int ntaps, float* partial, float* out, cudaStream_t s);
 cudaError_t launch_synth(const wfbp_synth_scan& scan, const wfbp_ellipsoid* d_e, int ne, float* out,
                          cudaStream_t s);
+
+// Host helpers of wfbp_host.cu used by the other host translation units.
+namespace wfbp_detail {
+int set_error(wfbp_ctx* ctx, int code, const std::string& msg);
+BPParams backprojection_params(const wfbp_ctx* ctx);
+void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal);
+bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out);
+int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream);
+int n_bp_candidates();
+void bp_candidate(int i, int* tx, int* ty, int* cu);
+}  // namespace wfbp_detail

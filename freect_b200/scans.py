@@ -177,6 +177,20 @@ def make_phantom(spec):
             hu = rng.uniform(-1000, 1500)
             out.append(_E(cx, cy, rng.uniform(-zr, zr), rng.uniform(4, 30), rng.uniform(4, 30), rng.uniform(4, 40),
                           rng.uniform(0, math.pi), MU_WATER * hu / 1000.0))
+    elif spec.phantom == "fov_random":
+        # elliptical water body filling 80 % of the FOV, seeded inserts inside
+        a, b = 0.4 * spec.fov, 0.3 * spec.fov
+        out.append(_E(0, 0, 0, a, b, 1.0e4, 0.0, MU_WATER))
+        zr = 0.5 * spec.V * spec.feed / spec.P
+        r = 0.08 * spec.fov
+        for _ in range(spec.n_random):
+            while True:
+                cx, cy = rng.uniform(-0.85 * a, 0.85 * a), rng.uniform(-0.85 * b, 0.85 * b)
+                if (cx / (0.85 * a)) ** 2 + (cy / (0.85 * b)) ** 2 < 1.0:
+                    break
+            hu = rng.uniform(-1000, 1500)
+            out.append(_E(cx, cy, rng.uniform(-zr, zr), rng.uniform(0.2, 1) * r, rng.uniform(0.2, 1) * r,
+                          rng.uniform(0.2, 1.5) * r, rng.uniform(0, math.pi), MU_WATER * hu / 1000.0))
     else:
         raise ValueError(spec.phantom)
     return out
@@ -196,6 +210,16 @@ def rows64(seed=0):
                     n_random=20)
 
 
+def rows64_short(seed=0):
+    """The rows64 scanner over 2.5 rotations and 60 slices: a profiling-size
+    case of the same kernels (about 1.5 GB on the device)."""
+    spec = rows64(seed=seed)
+    spec.name = "rows64_short"
+    spec.rotations = 2.5
+    spec.n_slices = 60
+    return spec
+
+
 def ffs(seed=0):
     """Flying focal spot in phi and z: 736 ch x 32 rows (0.6 mm), 2304 readings
     per rotation (1152 views/rotation x 2 focal positions) cycling through
@@ -207,6 +231,42 @@ def ffs(seed=0):
                     P=2304, rotations=8, feed=0.8 * 32 * 0.6, i0=1.5e5, nx=512, ny=512, fov=500.0,
                     slice_thickness=0.75, slice_pitch=0.5, n_slices=200, window=T.FILTER_REFERENCE,
                     phantom="body_random", seed=seed, n_random=40, ffs_mode=T.FFS_PHIZ)
+
+
+def batch_specs(seed=0, n=24, reduced=False):
+    """Uneven helical scans with seeded shapes: rows in {16, 32, 64} (0.6 mm),
+    672-888 channels, 984-1160 views/rotation, 2-12 rotations, pitch 0.5-1.5,
+    200-500 mm FOV, 256^2 or 512^2 matrix, 0.75-1.5 mm slices, I0 5e4-3e5, an
+    elliptical body with seeded inserts. The scanner is the small one's (SID
+    595, SDD 1085.6) with the fan spacing set for a 520 mm acquisition FOV.
+    Slices cover the scan's central (rotations - 1.5) turns of table feed.
+    reduced=True shrinks every scan (channels / 4, rows / 4, views / 8, at
+    most 3 rotations, 64^2 matrix, at most 4 slices) for tests."""
+    rng = np.random.default_rng(7919 * seed + 17)
+    out = []
+    for i in range(n):
+        rows = int(rng.choice([16, 32, 64]))
+        nch = int(rng.integers(672, 889))
+        P = int(rng.integers(984, 1161))
+        rot = int(rng.integers(2, 13))
+        pitch = float(rng.uniform(0.5, 1.5))
+        fov = float(rng.uniform(200.0, 500.0))
+        mat = int(rng.choice([256, 512]))
+        thick = float(rng.uniform(0.75, 1.5))
+        i0 = float(rng.uniform(5e4, 3e5))
+        if reduced:
+            rows, nch, P, rot, mat = max(4, rows // 4), nch // 4, P // 8, min(rot, 3), 64
+        row_iso = 0.6 if not reduced else 2.4
+        feed = pitch * rows * row_iso
+        n_slices = max(2, int((rot - 1.5) * feed / thick))
+        if reduced:
+            n_slices = min(n_slices, 4)
+        dbeta = 2.0 * math.asin(260.0 / 595.0) / (nch - 1)
+        out.append(ScanSpec("batch%d" % i, sid=595.0, sdd=1085.6, nch=nch, dbeta=dbeta, c0=0.5 * (nch - 1) + 0.25,
+                            nr=rows, row_iso=row_iso, P=P, rotations=rot, feed=feed, i0=i0, nx=mat, ny=mat, fov=fov,
+                            slice_thickness=thick, slice_pitch=thick, n_slices=n_slices, window=T.FILTER_REFERENCE,
+                            phantom="fov_random", seed=1000 * seed + i, n_random=12))
+    return out
 
 
 def tiny_ffs(seed=0, mode=T.FFS_PHIZ, nch=64, nr=4, P=128, rotations=3, nx=32, n_slices=4):
@@ -226,4 +286,4 @@ def tiny(seed=0, nch=96, nr=8, P=96, rotations=3, nx=32, n_slices=4, window=T.FI
                     seed=seed)
 
 
-WORKLOADS = {"small": small, "rows64": rows64, "ffs": ffs, "tiny": tiny}
+WORKLOADS = {"small": small, "rows64": rows64, "rows64_short": rows64_short, "ffs": ffs, "tiny": tiny}

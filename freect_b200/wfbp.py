@@ -32,7 +32,12 @@ _PROTOS = {
     "wfbp_query": (C.c_int, [_VP, C.POINTER(T.Dims)]),
     "wfbp_set_views": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "wfbp_get_slices": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "wfbp_set_reading_offset": (C.c_int, [_VP, C.c_int]),
+    "wfbp_set_slices": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float), C.c_int]),
     "wfbp_get_geometry": (C.c_int, [_VP, C.POINTER(T.CTGeometry), C.POINTER(T.GPUPrecompute)]),
+    "wfbp_bp_configs": (C.c_int, [_VP, C.POINTER(T.BpConfig), C.c_int, C.POINTER(C.c_int)]),
+    "wfbp_get_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
+    "wfbp_set_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
     "wfbp_last_error": (C.c_char_p, [_VP]),
     "wfbp_check_device_status": (C.c_int, [_VP]),
     "wfbp_status_string": (C.c_char_p, [C.c_int]),
@@ -43,6 +48,22 @@ _PROTOS = {
     "wfbp_run": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_run_host": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_run_static": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_set_taps": (C.c_int, [_VP, _VP, C.c_int, _VP]),
+    "wfbp_get_taps": (C.c_int, [_VP, _VP, _VP]),
+    "wfbp_thicken_adjoint": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_backproject_adjoint": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_filter_adjoint": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_rebin_adjoint": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_taps_gradient": (C.c_int, [_VP, _VP, _VP, _VP, C.c_int, _VP]),
+    "wfbp_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(_VP)]),
+    "wfbp_batch_destroy": (C.c_int, [_VP]),
+    "wfbp_batch_run": (C.c_int, [_VP, C.POINTER(_VP), C.POINTER(_VP), _VP]),
+    "wfbp_batch_size": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "wfbp_batch_bp_configs": (C.c_int, [_VP, C.POINTER(T.BpConfig), C.c_int, C.POINTER(C.c_int)]),
+    "wfbp_batch_get_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
+    "wfbp_batch_set_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
+    "wfbp_batch_check_device_status": (C.c_int, [_VP]),
+    "wfbp_batch_last_error": (C.c_char_p, [_VP]),
     "wfbp_synth_project": (C.c_int, [C.POINTER(T.SynthScan), C.POINTER(T.Ellipsoid), C.c_int, _VP, _VP]),
 }
 
@@ -209,12 +230,46 @@ class Context:
                                          req.ctypes.data_as(C.POINTER(C.c_float))), "wfbp_get_slices", self._h)
         return nat, req
 
+    def set_reading_offset(self, offset):
+        """Index of this context's first reading within the whole scan."""
+        _check(self._lib.wfbp_set_reading_offset(self._h, int(offset)), "wfbp_set_reading_offset", self._h)
+
+    def set_slices(self, native_z, requested_z):
+        """Explicit native / requested slice lists (e.g. a z-slab of a larger scan)."""
+        n, npp = _fptr(native_z)
+        r, rpp = _fptr(requested_z)
+        _check(self._lib.wfbp_set_slices(self._h, npp, n.size, rpp, r.size), "wfbp_set_slices", self._h)
+        d = T.Dims()
+        _check(self._lib.wfbp_query(self._h, C.byref(d)), "wfbp_query", self._h)
+        self.dims = d
+
     def set_views(self, tube_angles, table_positions):
         t, tp = _fptr(tube_angles)
         z, zp = _fptr(table_positions)
         if t.size < self.dims.n_readings or z.size < self.dims.n_readings:
             raise ValueError("need %d tube angles and table positions" % self.dims.n_readings)
         _check(self._lib.wfbp_set_views(self._h, tp, zp), "wfbp_set_views", self._h)
+
+    # ---- backprojection launch configuration ----
+    def bp_configs(self):
+        """Backprojection configurations that fit this geometry (after set_views)."""
+        n = C.c_int()
+        _check(self._lib.wfbp_bp_configs(self._h, None, 0, C.byref(n)), "wfbp_bp_configs", self._h)
+        arr = (T.BpConfig * max(n.value, 1))()
+        _check(self._lib.wfbp_bp_configs(self._h, arr, n.value, C.byref(n)), "wfbp_bp_configs", self._h)
+        return [arr[i] for i in range(n.value)]
+
+    def bp_config(self):
+        c = T.BpConfig()
+        _check(self._lib.wfbp_get_bp_config(self._h, C.byref(c)), "wfbp_get_bp_config", self._h)
+        return c
+
+    def set_bp_config(self, config):
+        if isinstance(config, (tuple, list)):
+            c = T.BpConfig()
+            c.tile_x, c.tile_y, c.cols_per_step = config
+            config = c
+        _check(self._lib.wfbp_set_bp_config(self._h, C.byref(config)), "wfbp_set_bp_config", self._h)
 
     # ---- stages (torch CUDA tensors) ----
     def rebin(self, raw, rebinned, stream=None):
@@ -254,6 +309,38 @@ class Context:
                self._h)
         return volume_host
 
+    # ---- adjoints (FP32 form; reference-layout FP32 buffers) ----
+    def set_taps(self, taps, stream=None):
+        """Overwrites h[0..n-1] of the filter's half taps (CUDA float32 tensor)."""
+        _check(self._lib.wfbp_set_taps(self._h, _dptr(taps), int(taps.numel()), _stream(stream)), "wfbp_set_taps",
+               self._h)
+
+    def get_taps(self, stream=None):
+        import torch
+        out = torch.empty(self.dims.n_channels, dtype=torch.float32, device=torch.device("cuda", self.device))
+        _check(self._lib.wfbp_get_taps(self._h, _dptr(out), _stream(stream)), "wfbp_get_taps", self._h)
+        return out
+
+    def thicken_adjoint(self, g_volume, g_native, stream=None):
+        _check(self._lib.wfbp_thicken_adjoint(self._h, _dptr(g_volume), _dptr(g_native), _stream(stream)),
+               "wfbp_thicken_adjoint", self._h)
+
+    def backproject_adjoint(self, g_native, g_filtered, stream=None):
+        _check(self._lib.wfbp_backproject_adjoint(self._h, _dptr(g_native), _dptr(g_filtered), _stream(stream)),
+               "wfbp_backproject_adjoint", self._h)
+
+    def filter_adjoint(self, g_filtered, g_rebinned, stream=None):
+        _check(self._lib.wfbp_filter_adjoint(self._h, _dptr(g_filtered), _dptr(g_rebinned), _stream(stream)),
+               "wfbp_filter_adjoint", self._h)
+
+    def rebin_adjoint(self, g_rebinned, g_raw, stream=None):
+        _check(self._lib.wfbp_rebin_adjoint(self._h, _dptr(g_rebinned), _dptr(g_raw), _stream(stream)),
+               "wfbp_rebin_adjoint", self._h)
+
+    def taps_gradient(self, raw, g_filtered, g_taps, stream=None):
+        _check(self._lib.wfbp_taps_gradient(self._h, _dptr(raw), _dptr(g_filtered), _dptr(g_taps),
+                                            int(g_taps.numel()), _stream(stream)), "wfbp_taps_gradient", self._h)
+
     # ---- allocation helpers ----
     def alloc(self, what, device=None):
         import torch
@@ -276,6 +363,72 @@ class Context:
         if what == "volume":
             return torch.empty((d.n_slices_requested, d.ny, d.nx), dtype=torch.float32, device=dev)
         raise ValueError(what)
+
+
+class Batch:
+    """Several scans reconstructed together (wfbp_batch): per-scan rebin and
+    filter, one persistent backprojection launch over all scans, per-scan
+    thickening, captured into a CUDA graph and replayed."""
+
+    def __init__(self, contexts):
+        self._lib = load()
+        self.contexts = list(contexts)  # the contexts must outlive the batch
+        arr = (_VP * len(self.contexts))(*[c.handle.value for c in self.contexts])
+        self._h = C.c_void_p()
+        st = self._lib.wfbp_batch_create(arr, len(self.contexts), C.byref(self._h))
+        if st != 0:
+            raise WfbpError(st, "wfbp_batch_create")
+
+    def _check(self, st, what):
+        if st != 0:
+            m = self._lib.wfbp_batch_last_error(self._h)
+            raise WfbpError(st, what + (": " + m.decode() if m else ""))
+
+    def close(self):
+        if self._h:
+            self._lib.wfbp_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def size(self):
+        a, b = C.c_int(), C.c_int()
+        self._check(self._lib.wfbp_batch_size(self._h, C.byref(a), C.byref(b)), "wfbp_batch_size")
+        return a.value, b.value
+
+    def run(self, raws, volumes, stream=None):
+        n = len(self.contexts)
+        if len(raws) != n or len(volumes) != n:
+            raise ValueError("need one raw and one volume tensor per scan")
+        ra = (_VP * n)(*[_dptr(r).value for r in raws])
+        va = (_VP * n)(*[_dptr(v).value for v in volumes])
+        self._check(self._lib.wfbp_batch_run(self._h, ra, va, _stream(stream)), "wfbp_batch_run")
+
+    def bp_configs(self):
+        n = C.c_int()
+        self._check(self._lib.wfbp_batch_bp_configs(self._h, None, 0, C.byref(n)), "wfbp_batch_bp_configs")
+        arr = (T.BpConfig * max(n.value, 1))()
+        self._check(self._lib.wfbp_batch_bp_configs(self._h, arr, n.value, C.byref(n)), "wfbp_batch_bp_configs")
+        return [arr[i] for i in range(n.value)]
+
+    def bp_config(self):
+        c = T.BpConfig()
+        self._check(self._lib.wfbp_batch_get_bp_config(self._h, C.byref(c)), "wfbp_batch_get_bp_config")
+        return c
+
+    def set_bp_config(self, config):
+        if isinstance(config, (tuple, list)):
+            c = T.BpConfig()
+            c.tile_x, c.tile_y, c.cols_per_step = config
+            config = c
+        self._check(self._lib.wfbp_batch_set_bp_config(self._h, C.byref(config)), "wfbp_batch_set_bp_config")
+
+    def check_device_status(self):
+        self._check(self._lib.wfbp_batch_check_device_status(self._h), "wfbp_batch_check_device_status")
 
 
 def synth_project(scan, ellipsoids, out, stream=None):

@@ -254,6 +254,39 @@ int wfbp_get_geometry(const wfbp_ctx* ctx, CTGeometry* cg, GPUPrecompute* gp);
 /* Copies the native / requested slice z lists (as wfbp_slice_locations). */
 int wfbp_get_slices(const wfbp_ctx* ctx, float* native_z, float* requested_z);
 
+/* Index of the context's first reading within the whole scan (default 0),
+ * for a context that holds a window of a scan's readings: the rebin samples
+ * reading v at the whole scan's index angle (v + offset) 2 pi / P
+ * (rebin_kernel, cuda_kernels.cuh:15-20), so the window rebins exactly like
+ * the whole scan. A multiple of the readings per view. No counterpart in
+ * the reference. */
+int wfbp_set_reading_offset(wfbp_ctx* ctx, int offset);
+
+/* Replaces the slice lists that wfbp_ctx_create derived from ReconConfig
+ * (ReconstructionMachine.cu:107-137) with explicit ones: native z (strictly
+ * monotone) and requested z. Used to reconstruct a z-slab of a scan with
+ * exactly the slice positions of the whole scan's lists (sharding across
+ * GPUs); the thickening weights and the backprojection launch are rebuilt.
+ * No counterpart in the reference. */
+int wfbp_set_slices(wfbp_ctx* ctx, const float* native_z, int n_native, const float* requested_z,
+                    int n_requested);
+
+/* Launch configuration of the backprojection in the backprojection layout
+ * (no counterpart in the reference, whose backproject_kernel launch is a
+ * fixed 16x16-thread block per voxel tile, ReconstructionMachine.cu:347-351).
+ * A CTA covers tile_x * tile_y voxel columns and 32 native slices;
+ * cols_per_step columns are accumulated per pass over a view window.
+ * wfbp_set_views picks a default; an autotuner lists the configurations that
+ * fit this geometry, times them and sets the fastest. All need set_views. */
+typedef struct wfbp_bp_config {
+  int tile_x, tile_y;
+  int cols_per_step;
+  int reserved;
+} wfbp_bp_config;
+int wfbp_bp_configs(const wfbp_ctx* ctx, wfbp_bp_config* out, int cap, int* n);
+int wfbp_get_bp_config(const wfbp_ctx* ctx, wfbp_bp_config* config);
+int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* config);
+
 /* Reads and clears the context's device-side error word, which kernels
  * with bounded waits set instead of hanging (synchronous). Returns
  * WFBP_ERR_TIMEOUT if a wait gave up since the last check. No counterpart
@@ -326,6 +359,75 @@ int wfbp_run_static(wfbp_ctx* ctx, const float* raw, float* volume, void* stream
  * synchronous on return. Pinned host buffers overlap the copies with the
  * stages. */
 int wfbp_run_host(wfbp_ctx* ctx, const float* raw_host, float* volume_host, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched scans (no counterpart in the reference, which reconstructs one   */
+/* scan per run, main.cpp:60-66)                                            */
+/* ------------------------------------------------------------------------ */
+
+/* A batch of scans of any shapes, one context each (same device, same
+ * precision, views set, backprojection layout supported). wfbp_batch_run
+ * rebins and filters every scan with its own launches, backprojects ALL
+ * scans in one persistent launch whose CTAs take (scan, column tile, slab)
+ * work items from a list sorted by estimated cost, and thickens per scan.
+ * The chain is captured into a CUDA graph on the first call and replayed
+ * while the raw / volume pointers stay the same (new pointers: recaptured).
+ * The batch owns the intermediates; the contexts must outlive it.
+ * stream NULL: runs on an internal stream, synchronous on return. */
+typedef struct wfbp_batch wfbp_batch;
+int wfbp_batch_create(wfbp_ctx* const* ctxs, int n, wfbp_batch** out);
+int wfbp_batch_destroy(wfbp_batch* batch);
+int wfbp_batch_run(wfbp_batch* batch, const float* const* raws, float* const* volumes, void* stream);
+int wfbp_batch_size(const wfbp_batch* batch, int* n_scans, int* n_items);
+/* Backprojection configurations that fit every scan of the batch, and the
+ * one in use (the autotuner times them and sets the fastest; setting one
+ * drops the captured graph). */
+int wfbp_batch_bp_configs(const wfbp_batch* batch, wfbp_bp_config* out, int cap, int* n);
+int wfbp_batch_get_bp_config(const wfbp_batch* batch, wfbp_bp_config* config);
+int wfbp_batch_set_bp_config(wfbp_batch* batch, const wfbp_bp_config* config);
+/* Reads and clears the batch's device-side error word (synchronous). */
+int wfbp_batch_check_device_status(wfbp_batch* batch);
+const char* wfbp_batch_last_error(const wfbp_batch* batch);
+
+/* ------------------------------------------------------------------------ */
+/* Adjoints of the FP32 form (no counterpart in the reference, which has no */
+/* backward pass). Each is the exact transpose of its forward stage, with   */
+/* every output element owned by one thread (no atomics, deterministic).    */
+/* Buffers are FP32 device arrays in the reference layout; all need         */
+/* wfbp_set_views and a context with WFBP_PRECISION_FP32.                   */
+/* ------------------------------------------------------------------------ */
+
+/* Overwrites taps h[0..n-1] of the context's symmetric half taps (device or
+ * host pointer, stream-ordered copy) -- the learnable part of the filter.
+ * The taps start as generate_filter's (ReconstructionMachine.cu:478-513)
+ * or the ext's window; wfbp_get_taps reads all n_channels of them. */
+int wfbp_set_taps(wfbp_ctx* ctx, const float* taps, int n, void* stream);
+int wfbp_get_taps(wfbp_ctx* ctx, float* taps, void* stream);
+
+/* Transpose of wfbp_thicken: g_volume [nz_requested][ny][nx] ->
+ * g_native [nz_native][ny][nx]. */
+int wfbp_thicken_adjoint(wfbp_ctx* ctx, const float* g_volume, float* g_native, void* stream);
+
+/* Transpose of wfbp_backproject (reference layout, FP32):
+ * g_native [nz_native][ny][nx] -> g_filtered [V][nr][nch]. Voxels the
+ * forward leaves NaN (no contributing view) contribute nothing. */
+int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, float* g_filtered, void* stream);
+
+/* Transpose of wfbp_filter (FP32): the Toeplitz operator is symmetric, so
+ * this filters g_filtered [V][nr][nch] with the same taps. */
+int wfbp_filter_adjoint(wfbp_ctx* ctx, const float* g_filtered, float* g_rebinned, void* stream);
+
+/* Transpose of wfbp_rebin: g_rebinned [V][nr][nch] -> g_raw
+ * [n_readings][raw_rows][raw_channels], with the context's texel weights.
+ * Not for flying-focal-spot scans (WFBP_ERR_UNSUPPORTED). */
+int wfbp_rebin_adjoint(wfbp_ctx* ctx, const float* g_rebinned, float* g_raw, void* stream);
+
+/* Gradient of the filter taps: g_taps[d] = sum over rows of
+ * sum_n g[n] (x[n-d] + x[n+d]) (d > 0; sum_n g[n] x[n] for d = 0), d < n,
+ * where x are the rebinned rows, recomputed from `raw` inside the kernel
+ * (nothing of the rebinned array is stored) and g = g_filtered. */
+int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_filtered, float* g_taps, int n,
+                       void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic scans (test-data generator; no counterpart in the reference)    */

@@ -44,6 +44,7 @@ def load():
             "orc_filter_taps_f64": (None, [G, C.c_int, C.c_double, C.c_double, _D, C.c_int]),
             "orc_rebin_ref32": (None, [G, _F, C.c_int, _F]),
             "orc_rebin_f64": (None, [G, _F, _D]),
+            "orc_rebin_f64_off": (None, [G, _F, C.c_long, _D]),
             "orc_filter_f64": (None, [C.c_int, C.c_long, _D, _D, _D]),
             "orc_filter_f32": (None, [C.c_int, C.c_long, _D, _F, _F]),
             "orc_rebin_filter_ref32": (C.c_int, [G, _F, _F, C.c_int, _F]),
@@ -146,11 +147,13 @@ def rebin_ref32(cg, raw, q8=False):
     return out
 
 
-def rebin_f64(cg, raw):
+def rebin_f64(cg, raw, offset=0):
+    """offset: index of raw's first reading within the whole scan (a window
+    is rebinned with the whole scan's index angles)."""
     V, nr, nch = int(cg.total_number_of_projections), int(cg.num_detector_rows), int(cg.num_detector_cols)
     out = np.zeros((V, nr, nch), np.float64)
     r = _f(raw)
-    load().orc_rebin_f64(C.byref(cg), fp(r), dp(out))
+    load().orc_rebin_f64_off(C.byref(cg), fp(r), int(offset), dp(out))
     return out
 
 
@@ -346,19 +349,32 @@ def rebin_adjoint_f64(cg, g_rebinned):
     return out
 
 
-def loss_and_grad_f64(spec, raw, taps_half, target, ntaps):
-    """L = mean over finite voxels of (vol - target)^2 for the FP64 path with
-    filter taps `taps_half`; returns (L, dL/draw, dL/dtaps[:ntaps], vol)."""
+def _forward_f64(spec, raw, taps_half):
     tube, table = spec.views()
     cg, gp = configure_geometry(spec.meta(), table)
     rp = spec.recon_config()
-    taps = np.asarray(taps_half, np.float64)
     x = rebin_f64(cg, raw)
-    y = filter_f64(x, taps)
+    y = filter_f64(x, np.asarray(taps_half, np.float64))
     zn, zr = slice_locations(cg, rp)
     t64, z64 = tube.astype(np.float64), table.astype(np.float64)
     vn, _ = backproject_f64(cg, rp, y, t64, z64, zn)
     vol = thicken_f64(rp, vn, zn, zr)
+    return cg, rp, x, y, zn, zr, t64, z64, vn, vol
+
+
+def loss_f64(spec, raw, taps_half, target):
+    """L = mean over finite voxels of (vol - target)^2, FP64 path with the
+    filter taps `taps_half` (exact texel weights)."""
+    vol = _forward_f64(spec, raw, taps_half)[-1]
+    m = np.isfinite(vol)
+    return float(((vol[m] - target[m]) ** 2).sum() / m.sum())
+
+
+def loss_and_grad_f64(spec, raw, taps_half, target, ntaps):
+    """L of loss_f64 and its gradient by the FP64 adjoints: returns
+    (L, dL/draw, dL/dtaps[:ntaps], vol)."""
+    cg, rp, x, y, zn, zr, t64, z64, vn, vol = _forward_f64(spec, raw, taps_half)
+    taps = np.asarray(taps_half, np.float64)
     m = np.isfinite(vol)
     n = m.sum()
     diff = np.where(m, vol - target, 0.0)

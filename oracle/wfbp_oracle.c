@@ -356,8 +356,10 @@ ORC_EXPORT void orc_rebin_ref32(const CTGeometry* cg, const float* raw, int q8, 
   orc_parallel_for(rows, 64, rb32_body, &a);
 }
 
-/* FP64 rebin: exact bilinear weights, clamp addressing, all views. */
-typedef struct { const CTGeometry* cg; const float* raw; double* out; } rb64_args;
+/* FP64 rebin: exact bilinear weights, clamp addressing, all views. `off`:
+ * index of the first reading within the whole scan (a window of readings is
+ * rebinned with the whole scan's index angles, rebin_kernel CK:15-20). */
+typedef struct { const CTGeometry* cg; const float* raw; double* out; long off; } rb64_args;
 static void rb64_body(void* a_, long i0, long i1) {
   rb64_args* a = (rb64_args*)a_;
   const CTGeometry* cg = a->cg;
@@ -371,12 +373,12 @@ static void rb64_body(void* a_, long i0, long i1) {
       double p = ((double)c - c0) * dcol;
       double beta = asin(p / sdd);
       double bidx = beta * sdd / dcol + c0;
-      double aidx = (double)v - beta / dth;
+      double aidx = (double)(v + a->off) - beta / dth;
       double val = 0.0;
       if (!(bidx < 0 || bidx >= (double)nch || isnan(bidx))) {
         double fx = floor(bidx), fy = floor(aidx);
         double ax = bidx - fx, ay = aidx - fy;
-        long x0 = (long)fx, y0 = (long)fy, x1 = x0 + 1, y1 = y0 + 1;
+        long x0 = (long)fx, y0 = (long)fy - a->off, x1 = x0 + 1, y1 = y0 + 1;
         if (x0 < 0) x0 = 0; if (x0 > nch - 1) x0 = nch - 1;
         if (x1 < 0) x1 = 0; if (x1 > nch - 1) x1 = nch - 1;
         if (y0 < 0) y0 = 0; if (y0 > V - 1) y0 = V - 1;
@@ -391,11 +393,12 @@ static void rb64_body(void* a_, long i0, long i1) {
     }
   }
 }
-ORC_EXPORT void orc_rebin_f64(const CTGeometry* cg, const float* raw, double* out) {
-  rb64_args a = {cg, raw, out};
+ORC_EXPORT void orc_rebin_f64_off(const CTGeometry* cg, const float* raw, long off, double* out) {
+  rb64_args a = {cg, raw, out, off};
   long rows = (long)cg->total_number_of_projections * (long)cg->num_detector_rows;
   orc_parallel_for(rows, 64, rb64_body, &a);
 }
+ORC_EXPORT void orc_rebin_f64(const CTGeometry* cg, const float* raw, double* out) { orc_rebin_f64_off(cg, raw, 0, out); }
 
 /* ------------------------------------------------------------------------ */
 /* filter                                                                    */
@@ -659,7 +662,8 @@ static void bp64_geo_init(bp64_geo* g, const CTGeometry* cg, const ReconConfig* 
   double afov = 2.0 * g->sid * sin(((g->nch - 1.0) / 2.0) * g->dcol / g->sdd);
   g->afov_half2 = 0.25 * afov * afov;
   int P = (int)cg->projections_per_rotation;
-  g->z_rot = fabs(table[P] - table[0]);
+  (void)table;
+  g->z_rot = (double)cg->z_rot;  /* ConfigureCTGeometry's |z[P] - z[0]| (RM.cu:64) */
   g->zr2pi = g->z_rot / (2.0 * M_PI);
   g->tanc = tan(theta_cone / 2.0);
   g->pixel_scale = g->sdd / (g->sid * g->dcol);

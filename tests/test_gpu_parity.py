@@ -278,3 +278,45 @@ def test_backprojection_layout_stages(orc, which):
     _, n64 = orc.backproject_f64(cg, ctx.rp, ft.astype(np.float64), tube.astype(np.float64),
                                  table.astype(np.float64), nat)
     assert abs(int(cnt.item()) - n64) <= 1e-4 * n64 + 2
+
+
+@pytest.mark.parametrize("precision", [T.PRECISION_FP32, T.PRECISION_MIXED])
+def test_bp_configs_identical_and_tuner(orc, tmp_path, precision):
+    # every launch configuration computes the same per-voxel sums in the same
+    # order, so the volumes are bit-identical; the autotuner picks one of them
+    from freect_b200 import autotune
+    spec = scans.small(seed=7)
+    spec.nx = spec.ny = 96
+    spec.n_slices = 40
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    ctx = wfbp.Context(cg, spec.recon_config(), wfbp.make_ext(precision=precision, filter_window=spec.window,
+                                                             filtered_layout=T.LAYOUT_BACKPROJECTION), device=0)
+    ctx.set_views(tube, table)
+    reb, filt, sc = ctx.alloc("rebinned"), ctx.alloc("filtered"), ctx.alloc("row_scales")
+    ctx.rebin(dev(raw), reb)
+    ctx.filter(reb, filt, sc)
+    cfgs = ctx.bp_configs()
+    assert len(cfgs) >= 4
+    vols = []
+    for c in cfgs:
+        ctx.set_bp_config(c)
+        assert ctx.bp_config().key() == c.key()
+        vn = ctx.alloc("native")
+        ctx.backproject(filt, vn, sc)
+        torch.cuda.synchronize()
+        ctx.check_device_status()
+        vols.append(vn.cpu().numpy())
+    assert np.isfinite(vols[0]).any()
+    for c, v in zip(cfgs[1:], vols[1:]):
+        assert np.array_equal(v, vols[0], equal_nan=True), c.key()
+    with pytest.raises(wfbp.WfbpError):
+        ctx.set_bp_config((16, 16, 16))
+    path = str(tmp_path / "tune.json")
+    vn = ctx.alloc("native")
+    r1 = autotune.tune_backprojection(ctx, filt, vn, row_scales=sc, path=path)
+    assert not r1["cached"] and r1["config"] in [c.key() for c in cfgs]
+    assert len(r1["times_ms"]) == len(cfgs)
+    r2 = autotune.tune_backprojection(ctx, filt, vn, row_scales=sc, path=path)
+    assert r2["cached"] and r2["config"] == r1["config"] and ctx.bp_config().key() == r1["config"]

@@ -1,0 +1,108 @@
+"""Z-slab sharding (freect_b200.shard): the plans, and the sharded path run
+as two gloo ranks on CPU with the FP64 oracle as the per-rank engine, its
+slabs gathered to rank 0 and compared with the whole-scan reconstruction
+(bit-identical: each voxel sums the same views in the same order)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from freect_b200 import scans, shard, wfbp
+
+torch = pytest.importorskip("torch")
+
+
+def _geometry(spec):
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    return cg, spec.recon_config(), tube, table
+
+
+@pytest.mark.parametrize("name", ["tiny", "small", "rows64", "ffs"])
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_plan_covers_and_aligns(name, world):
+    spec = scans.WORKLOADS[name]()
+    cg, rp, tube, table = _geometry(spec)
+    nat, req = wfbp.slice_locations(cg, rp)
+    if world > req.size:
+        pytest.skip("fewer slices than ranks")
+    plans = shard.plan(cg, rp, table, world)
+    G = shard._readings_per_view(cg)
+    V, P = int(cg.total_number_of_projections) // G, int(cg.projections_per_rotation) // G
+    P2 = P // 2
+    K = V // P2
+    zv = np.asarray(table, np.float32)[::G][:V]
+    assert [p.requested for p in plans][0][0] == 0 and plans[-1].requested[1] == req.size
+    for a, b in zip(plans, plans[1:]):
+        assert a.requested[1] == b.requested[0]
+    reach = shard.rebin_reach(cg) // G
+    for p in plans:
+        r0, r1 = p.requested
+        n0, n1 = p.native
+        v0, v1 = p.views
+        assert p.readings == (v0 * G, v1 * G)
+        # every native slice the slab's thickening weights reach is inside
+        w = np.abs(nat[:, None] - req[None, r0:r1]) < rp.slice_thickness
+        assert not w[:n0].any() and not w[n1:].any()
+        # half-turn aligned window, more than one rotation, inside the whole scan's used views
+        assert v0 % P2 == 0 and v1 - v0 > P and v1 <= V
+        Ks = (v1 - v0) // P2
+        assert v0 + Ks * P2 <= K * P2
+        # every view within z_rot of the slab is read by the window's backprojection,
+        # with the rebin's reach inside the window too
+        zlo, zhi = nat[n0:n1].min(), nat[n0:n1].max()
+        need = np.nonzero((zv[:K * P2] >= zlo - cg.z_rot) & (zv[:K * P2] <= zhi + cg.z_rot))[0]
+        assert need[0] - v0 >= min(reach, need[0]) and need[-1] < v0 + Ks * P2
+        assert v1 - 1 - need[-1] >= min(reach, V - 1 - need[-1])
+
+
+def _oracle_slab(orc, cg, rp, tube, table, raw, p):
+    """The slab of plan p through the FP64 oracle, from the window's readings only."""
+    a0, a1 = p.readings
+    scg = shard.sub_geometry(cg, p)
+    nat, req = orc.slice_locations(cg, rp)
+    zn, zr = nat[p.native[0]:p.native[1]], req[p.requested[0]:p.requested[1]]
+    x = orc.rebin_f64(scg, raw[a0:a1], offset=a0)
+    y = orc.filter_f64(x, orc.taps_f64(scg))
+    vn, _ = orc.backproject_f64(scg, rp, y, tube[a0:a1].astype(np.float64), table[a0:a1].astype(np.float64), zn)
+    return orc.thicken_f64(rp, vn, zn, zr)
+
+
+def _rank_main(rank, world, port, result_path):
+    import torch.distributed as dist
+    from oracle import oracle as orc
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        spec = scans.tiny(nch=64, nr=6, P=96, rotations=5, nx=24, n_slices=9)
+        cg, rp, tube, table = _geometry(spec)
+        raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+        plans = shard.plan(cg, rp, table, world)
+        slab = torch.from_numpy(_oracle_slab(orc, cg, rp, tube, table, raw, plans[rank]).copy())
+        whole = shard.gather_slabs(slab, plans, rank)
+        if rank == 0:
+            np.save(result_path, whole.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_oracle_two_ranks_matches_whole(orc, tmp_path):
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "whole.npy")
+    mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
+    got = np.load(out)
+    spec = scans.tiny(nch=64, nr=6, P=96, rotations=5, nx=24, n_slices=9)
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    ref = orc.reconstruct_f64(spec, raw)["volume"]
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref, equal_nan=True)
+    assert np.isfinite(ref).mean() > 0.5
+    # and the plans of 3 ranks, run in one process, stitch to the same volume
+    cg, rp, tube, table = _geometry(spec)
+    parts = [_oracle_slab(orc, cg, rp, tube, table, raw, p) for p in shard.plan(cg, rp, table, 3)]
+    assert np.array_equal(np.concatenate(parts), ref, equal_nan=True)
