@@ -383,3 +383,29 @@ cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float*
   k_taps_reduce<<<(ntaps + 127) / 128, 128, 0, s>>>(partial, nblk, ntaps, out);
   return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// self-test of the bounded waits
+// ---------------------------------------------------------------------------
+#include "wait.cuh"
+
+namespace {
+// Waits on an mbarrier that nothing ever arrives at, with a limit of
+// limit_ns; when the wait gives up (as it must) the error word is set to
+// WFBP_ERR_TIMEOUT, exactly as a stalled pipeline in the production kernels
+// reports itself.
+__global__ void k_selftest_wait(int* err, unsigned long long limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(&bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !wfbp_mbar_wait(&bar, 0, limit_ns)) atomicExch(err, WFBP_ERR_TIMEOUT);
+}
+}  // namespace
+
+cudaError_t launch_selftest_wait(int* err, unsigned long long limit_ns, cudaStream_t s) {
+  k_selftest_wait<<<1, 32, 0, s>>>(err, limit_ns);
+  return cudaGetLastError();
+}

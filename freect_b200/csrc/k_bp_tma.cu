@@ -29,6 +29,7 @@
 // in the error word and stops. Window or slot overflows (which the host's
 // sizing rules out) are recorded as well and the affected samples skipped.
 #include "wfbp_internal.h"
+#include "wait.cuh"
 
 #include <cuda.h>
 
@@ -37,7 +38,6 @@
 namespace {
 
 constexpr int BT_THREADS = (BT_CWARPS + 1) * 32;  // consumer warps + producer warp
-constexpr long long BT_SPIN = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -56,19 +56,8 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < BT_SPIN; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
+// Bounded wait on phase parity (wait.cuh); false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return wfbp_mbar_wait(bar, parity); }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
   asm volatile(

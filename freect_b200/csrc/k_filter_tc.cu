@@ -21,6 +21,7 @@
 // timeout the CTA records an error code, stops issuing work, waits (bounded)
 // for its TMA copies and frees its tensor memory before returning.
 #include "wfbp_internal.h"
+#include "wait.cuh"
 
 #include <cuda.h>
 
@@ -31,7 +32,6 @@ constexpr int TC_BK = 64;  // 64 bf16 = 128 bytes, one swizzle row
 constexpr int TC_STAGES = 2;
 constexpr int TC_THREADS = 128;
 constexpr uint32_t TC_TMEM_COLS = 256;
-constexpr long long SPIN_LIMIT = 1ll << 26;
 
 struct TcParams {
   int M;          // rows of X (V * nrv)
@@ -54,20 +54,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// Bounded wait on phase parity; returns false after SPIN_LIMIT polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < SPIN_LIMIT; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
+// Bounded wait on phase parity (wait.cuh); false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return wfbp_mbar_wait(bar, parity); }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
   asm volatile(

@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <new>
 
+#include <nvtx3/nvToolsExt.h>
+
 #define WFBP_API extern "C" __attribute__((visibility("default")))
 
 namespace {
@@ -382,6 +384,12 @@ WFBP_API int wfbp_configure_geometry(const wfbp_scan_meta* m, const float* table
   gp->tanf_theta_cone = (float)tan((double)(cg->theta_cone / 2.0f));
   gp->pixel_scale = cg->distance_source_to_detector / (cg->distance_source_to_isocenter * cg->detector_pixel_size_col);
   gp->two_pi_over_projections_per_rotation = 2.0f * pi_f / (float)cg->projections_per_rotation;
+  return WFBP_OK;
+}
+
+WFBP_API int wfbp_effective_geometry(const CTGeometry* cg, CTGeometry* eff) {
+  if (!cg || !eff) return WFBP_ERR_INVALID_ARG;
+  ffs_effective(cg, eff);
   return WFBP_OK;
 }
 
@@ -785,6 +793,14 @@ WFBP_API int wfbp_check_device_status(wfbp_ctx* ctx) {
   return WFBP_OK;
 }
 
+WFBP_API int wfbp_selftest_bounded_wait(wfbp_ctx* ctx, int limit_ms, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (limit_ms < 1 || limit_ms > 10000) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_selftest_bounded_wait: limit 1-10000 ms");
+  DeviceGuard g(ctx->device);
+  CUDA_TRY(ctx, launch_selftest_wait(ctx->d_err, (unsigned long long)limit_ms * 1000000ull, (cudaStream_t)stream));
+  return WFBP_OK;
+}
+
 WFBP_API int wfbp_get_geometry(const wfbp_ctx* ctx, CTGeometry* cg, GPUPrecompute* gp) {
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (cg) *cg = ctx->cg;
@@ -1050,18 +1066,60 @@ int ensure_scratch(wfbp_ctx* ctx) {
 }
 }  // namespace
 
+namespace {
+// The four stages on the context's scratch; `ev` (5 events or null) brackets
+// them for the stage timers of the reference's GPUTimer (ReconstructionMachine
+// .cu:239-293,345-361,391-426). NVTX ranges name the stages for profilers.
+int run_stages(wfbp_ctx* ctx, const float* raw, float* vol, void* stream, cudaEvent_t* ev) {
+  const cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_scratch(ctx);
+  if (st) return st;
+  const int lay = run_layout(ctx);
+  nvtxRangePushA("wfbp_run");
+  if (ev) cudaEventRecord(ev[0], s);
+  nvtxRangePushA("rebin");
+  st = wfbp_rebin(ctx, raw, ctx->s_rebinned, stream);
+  nvtxRangePop();
+  if (ev) cudaEventRecord(ev[1], s);
+  nvtxRangePushA("filter");
+  if (!st) st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, stream);
+  nvtxRangePop();
+  if (ev) cudaEventRecord(ev[2], s);
+  nvtxRangePushA("backproject");
+  if (!st) st = do_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, lay, stream);
+  nvtxRangePop();
+  if (ev) cudaEventRecord(ev[3], s);
+  nvtxRangePushA("thicken");
+  if (!st) st = wfbp_thicken(ctx, ctx->s_vol_native, vol, stream);
+  nvtxRangePop();
+  if (ev) cudaEventRecord(ev[4], s);
+  nvtxRangePop();
+  return st;
+}
+}  // namespace
+
 WFBP_API int wfbp_run(wfbp_ctx* ctx, const float* raw, float* vol, void* stream) {
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (!raw || !vol) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_run: null buffer");
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_run: wfbp_set_views not called");
   DeviceGuard g(ctx->device);
-  int st = ensure_scratch(ctx);
+  return run_stages(ctx, raw, vol, stream, nullptr);
+}
+
+WFBP_API int wfbp_run_timed(wfbp_ctx* ctx, const float* raw, float* vol, void* stream, float* stage_ms) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw || !vol || !stage_ms) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_run_timed: null pointer");
+  if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_run_timed: wfbp_set_views not called");
+  DeviceGuard g(ctx->device);
+  cudaEvent_t ev[5] = {};
+  for (auto& e : ev) CUDA_TRY(ctx, cudaEventCreate(&e));
+  int st = run_stages(ctx, raw, vol, stream, ev);
+  cudaError_t ce = cudaEventSynchronize(ev[4]);
+  for (int i = 0; i < 4 && !st && !ce; i++) ce = cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+  for (auto& e : ev) cudaEventDestroy(e);
   if (st) return st;
-  const int lay = run_layout(ctx);
-  if ((st = wfbp_rebin(ctx, raw, ctx->s_rebinned, stream))) return st;
-  if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, stream))) return st;
-  if ((st = do_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, lay, stream))) return st;
-  return wfbp_thicken(ctx, ctx->s_vol_native, vol, stream);
+  CUDA_TRY(ctx, ce);
+  return WFBP_OK;
 }
 
 WFBP_API int wfbp_run_host(wfbp_ctx* ctx, const float* raw_host, float* vol_host, void* stream) {

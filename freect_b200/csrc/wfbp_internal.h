@@ -218,6 +218,7 @@ cudaError_t launch_rebin_adj_cols(const float* bidx, int nch, int q8, int* cnt, 
 cudaError_t launch_rebin_adjoint(const float* gR, float* graw, const float* beta, const int* cnt, const int* cidx,
                                  const float* cw, int maxl, const RebinParams& p, cudaStream_t s);
 int taps_grad_blocks(const RebinParams& p);
+cudaError_t launch_selftest_wait(int* err, unsigned long long limit_ns, cudaStream_t s);
 cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float* beta, const float* bidx,
                                  const RebinParams& p, int ntaps, float* partial, float* out, cudaStream_t s);
 cudaError_t launch_synth(const wfbp_synth_scan& scan, const wfbp_ellipsoid* d_e, int ne, float* out,

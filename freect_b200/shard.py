@@ -61,7 +61,8 @@ def plan(cg, rp, table_positions, world):
     length."""
     G = _readings_per_view(cg)
     table = np.asarray(table_positions, np.float32)
-    nat, req = wfbp.slice_locations(cg, rp)
+    # slice lists follow the geometry the stages work on (effective with FFS)
+    nat, req = wfbp.slice_locations(wfbp.effective_geometry(cg), rp)
     V = int(cg.total_number_of_projections) // G
     P = int(cg.projections_per_rotation) // G
     P2 = P // 2
@@ -106,7 +107,7 @@ def sub_geometry(cg, p):
 def slab_context(cg, rp, ext, tube_angles, table_positions, p, device=0):
     """A context that reconstructs slab `p` from the readings of its window."""
     a0, a1 = p.readings
-    nat, req = wfbp.slice_locations(cg, rp)
+    nat, req = wfbp.slice_locations(wfbp.effective_geometry(cg), rp)
     ctx = wfbp.Context(sub_geometry(cg, p), rp, ext, device=device)
     ctx.set_reading_offset(a0)
     ctx.set_views(np.asarray(tube_angles, np.float32)[a0:a1], np.asarray(table_positions, np.float32)[a0:a1])

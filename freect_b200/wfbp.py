@@ -21,6 +21,7 @@ _VP = C.c_void_p
 _PROTOS = {
     "wfbp_configure_geometry": (C.c_int, [C.POINTER(T.ScanMeta), C.POINTER(C.c_float), C.POINTER(T.CTGeometry),
                                           C.POINTER(T.GPUPrecompute)]),
+    "wfbp_effective_geometry": (C.c_int, [C.POINTER(T.CTGeometry), C.POINTER(T.CTGeometry)]),
     "wfbp_slice_locations": (C.c_int, [C.POINTER(T.CTGeometry), C.POINTER(T.ReconConfig), C.POINTER(C.c_float),
                                        C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int,
                                        C.POINTER(C.c_int)]),
@@ -40,6 +41,7 @@ _PROTOS = {
     "wfbp_set_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
     "wfbp_last_error": (C.c_char_p, [_VP]),
     "wfbp_check_device_status": (C.c_int, [_VP]),
+    "wfbp_selftest_bounded_wait": (C.c_int, [_VP, C.c_int, _VP]),
     "wfbp_status_string": (C.c_char_p, [C.c_int]),
     "wfbp_rebin": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_filter": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
@@ -47,6 +49,7 @@ _PROTOS = {
     "wfbp_thicken": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_run": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_run_host": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "wfbp_run_timed": (C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(C.c_float)]),
     "wfbp_run_static": (C.c_int, [_VP, _VP, _VP, _VP]),
     "wfbp_set_taps": (C.c_int, [_VP, _VP, C.c_int, _VP]),
     "wfbp_get_taps": (C.c_int, [_VP, _VP, _VP]),
@@ -64,6 +67,10 @@ _PROTOS = {
     "wfbp_batch_set_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
     "wfbp_batch_check_device_status": (C.c_int, [_VP]),
     "wfbp_batch_last_error": (C.c_char_p, [_VP]),
+    "wfbp_parse_recon_config": (C.c_int, [C.c_char_p, C.POINTER(T.ReconConfig)]),
+    "wfbp_read_meta": (C.c_int, [C.c_char_p, C.POINTER(T.ScanMeta)]),
+    "wfbp_read_frames": (C.c_int, [C.c_char_p, C.POINTER(T.ScanMeta), C.c_int, C.c_int, _VP, _VP, _VP]),
+    "wfbp_write_scan": (C.c_int, [C.c_char_p, C.POINTER(T.ScanMeta), _VP, _VP, _VP]),
     "wfbp_synth_project": (C.c_int, [C.POINTER(T.SynthScan), C.POINTER(T.Ellipsoid), C.c_int, _VP, _VP]),
 }
 
@@ -143,6 +150,13 @@ def configure_geometry(meta, table_positions):
     return cg, gp
 
 
+def effective_geometry(cg):
+    """The geometry a context's stages work on (effective one with a flying focal spot)."""
+    eff = T.CTGeometry()
+    _check(load().wfbp_effective_geometry(C.byref(cg), C.byref(eff)), "wfbp_effective_geometry")
+    return eff
+
+
 def slice_locations(cg, rp):
     """Native and requested slice z lists (float32), ReconstructionMachine.cu:107-137."""
     lib = load()
@@ -219,6 +233,11 @@ class Context:
     def check_device_status(self):
         _check(self._lib.wfbp_check_device_status(self._h), "wfbp_check_device_status", self._h)
 
+    def selftest_bounded_wait(self, limit_ms=50, stream=None):
+        """Runs a wait that can never complete, bounded to limit_ms."""
+        _check(self._lib.wfbp_selftest_bounded_wait(self._h, int(limit_ms), _stream(stream)),
+               "wfbp_selftest_bounded_wait", self._h)
+
     @property
     def handle(self):
         return self._h
@@ -289,6 +308,13 @@ class Context:
 
     def run(self, raw, volume, stream=None):
         _check(self._lib.wfbp_run(self._h, _dptr(raw), _dptr(volume), _stream(stream)), "wfbp_run", self._h)
+
+    def run_timed(self, raw, volume, stream=None):
+        """wfbp_run with per-stage device times: {rebin, filter, backproject, thicken} in ms."""
+        ms = (C.c_float * 4)()
+        _check(self._lib.wfbp_run_timed(self._h, _dptr(raw), _dptr(volume), _stream(stream), ms), "wfbp_run_timed",
+               self._h)
+        return dict(zip(("rebin", "filter", "backproject", "thicken"), list(ms)))
 
     def run_static(self, raw, volume, stream=None):
         """wfbp_run with the intermediates in the library's static device
@@ -363,6 +389,45 @@ class Context:
         if what == "volume":
             return torch.empty((d.n_slices_requested, d.ny, d.nx), dtype=torch.float32, device=dev)
         raise ValueError(what)
+
+
+def parse_recon_config(path):
+    """fct_wfbp's recon-parameter YAML file -> ReconConfig."""
+    rp = T.ReconConfig()
+    _check(load().wfbp_parse_recon_config(os.fsencode(path), C.byref(rp)), "wfbp_parse_recon_config " + str(path))
+    return rp
+
+
+def read_meta(directory):
+    """meta.yaml of a FreeCT scan directory -> wfbp_scan_meta."""
+    m = T.ScanMeta()
+    _check(load().wfbp_read_meta(os.fsencode(directory), C.byref(m)), "wfbp_read_meta " + str(directory))
+    return m
+
+
+def read_frames(directory, meta, first=0, count=None, out=None):
+    """Readings [first, first+count) of projections.dat: (tube angles, table
+    positions, raw [count][rows][channels]) as float32 arrays. `out` may be a
+    (pinned) float32 torch CPU tensor or numpy array for the raw frames."""
+    count = meta.total_num_projections - first if count is None else count
+    tube = np.zeros(count, np.float32)
+    table = np.zeros(count, np.float32)
+    shape = (count, meta.detector_rows, meta.detector_channels)
+    if out is None:
+        out = np.zeros(shape, np.float32)
+    ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+    _check(load().wfbp_read_frames(os.fsencode(directory), C.byref(meta), int(first), int(count),
+                                   tube.ctypes.data_as(_VP), table.ctypes.data_as(_VP), C.c_void_p(ptr)),
+           "wfbp_read_frames " + str(directory))
+    return tube, table, out
+
+
+def write_scan(directory, meta, tube_angles, table_positions, raw):
+    t, _ = _fptr(tube_angles)
+    z, _ = _fptr(table_positions)
+    r = np.ascontiguousarray(raw, dtype=np.float32)
+    _check(load().wfbp_write_scan(os.fsencode(directory), C.byref(meta), t.ctypes.data_as(_VP),
+                                  z.ctypes.data_as(_VP), r.ctypes.data_as(_VP)), "wfbp_write_scan " + str(directory))
 
 
 class Batch:

@@ -214,6 +214,12 @@ typedef struct wfbp_ctx wfbp_ctx;
 int wfbp_configure_geometry(const wfbp_scan_meta* meta, const float* table_positions,
                             CTGeometry* cg, GPUPrecompute* gp);
 
+/* The geometry the stages of a context created from `cg` work on (host
+ * only): `cg` itself, or with a flying focal spot the effective geometry of
+ * wfbp_get_geometry (one view per focal-state cycle, 2x channels / rows at
+ * half the spacing). Slice lists of a context follow this geometry. */
+int wfbp_effective_geometry(const CTGeometry* cg, CTGeometry* eff);
+
 /* Slice lists of ReconstructionMachine::AllocateKeyArrays
  * (ReconstructionMachine.cu:107-137), float accumulation included.
  * Either output pointer may be NULL to query counts. */
@@ -293,6 +299,14 @@ int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* config);
  * in the reference, which has no device-side waits. */
 int wfbp_check_device_status(wfbp_ctx* ctx);
 
+/* Failure-detection self-test: launches a kernel whose mbarrier wait can
+ * never complete (nothing arrives) with a wall-clock limit of limit_ms
+ * (1-10000); the wait gives up, the kernel sets the context's error word
+ * and returns, so the next wfbp_check_device_status reports
+ * WFBP_ERR_TIMEOUT and the context stays usable. Every production wait
+ * (TMA rings, tensor-core pipeline) is bounded the same way (4 s). */
+int wfbp_selftest_bounded_wait(wfbp_ctx* ctx, int limit_ms, void* stream);
+
 /* Last error message of this context (never NULL). */
 const char* wfbp_last_error(const wfbp_ctx* ctx);
 const char* wfbp_status_string(int status);
@@ -353,6 +367,12 @@ int wfbp_run(wfbp_ctx* ctx, const float* raw, float* volume, void* stream);
  * wfbp_ctx_create; this call allocates nothing. */
 #define WFBP_STATIC_SCRATCH_BYTES (32u << 20)
 int wfbp_run_static(wfbp_ctx* ctx, const float* raw, float* volume, void* stream);
+
+/* wfbp_run, synchronous, with the device time of each stage in ms
+ * (stage_ms[0..3] = rebin, filter, backprojection, thickening), the
+ * reference's per-stage GPUTimer output (ReconstructionMachine.cu:239-293,
+ * 345-361, 391-426). Stages are also marked as NVTX ranges. */
+int wfbp_run_timed(wfbp_ctx* ctx, const float* raw, float* volume, void* stream, float* stage_ms);
 
 /* RunReconstruction from host memory: H2D of the raw readings, the four
  * stages, D2H of the final volume (ReconstructionMachine.cu:246,423),
@@ -428,6 +448,33 @@ int wfbp_rebin_adjoint(wfbp_ctx* ctx, const float* g_rebinned, float* g_raw, voi
  * (nothing of the rebinned array is stored) and g = g_filtered. */
 int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_filtered, float* g_taps, int n,
                        void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Input files (host only)                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* The recon-parameter YAML file of fct_wfbp (parse_config,
+ * applications/fct_wfbp/src/parse_config.cpp:31-63): keys raw_data_dir,
+ * output_dir, start_pos, end_pos, recon_fov, slice_thickness, slice_pitch,
+ * nx, ny, recon_kernel, x_origin, y_origin, tube_angle_offset,
+ * adaptive_filtration_s; absent keys stay 0, slice_pitch 0 becomes
+ * slice_thickness, output_file is "<path>_recon.dat". Flat `key: value`
+ * YAML only (WFBP_ERR_INVALID_ARG otherwise). */
+int wfbp_parse_recon_config(const char* path, ReconConfig* rp);
+
+/* FreeCT 2-file scan format (fct_read: RawDataSet::writeAll,
+ * modules/fct_read/src/RawDataSet.cpp:84-104; FreeCTFrame::readFromFile,
+ * FreeCTDataSet.cpp:8-21): <dir>/meta.yaml and <dir>/projections.dat, one
+ * frame per reading = {float angle, axial, radial; float [rows][channels]}.
+ * wfbp_read_meta fills the scan metadata (flying_focal_spot_mode FFSNONE /
+ * FFSZ / FFSXY / FFSXYZ); wfbp_read_frames reads readings [first,
+ * first+count) into host arrays (tube_angles / table_positions may be
+ * NULL), one seek for the whole window; wfbp_write_scan writes a scan. */
+int wfbp_read_meta(const char* dir, wfbp_scan_meta* meta);
+int wfbp_read_frames(const char* dir, const wfbp_scan_meta* meta, int first, int count, float* tube_angles,
+                     float* table_positions, float* raw);
+int wfbp_write_scan(const char* dir, const wfbp_scan_meta* meta, const float* tube_angles,
+                    const float* table_positions, const float* raw);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic scans (test-data generator; no counterpart in the reference)    */

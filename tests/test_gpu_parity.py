@@ -320,3 +320,14 @@ def test_bp_configs_identical_and_tuner(orc, tmp_path, precision):
     assert len(r1["times_ms"]) == len(cfgs)
     r2 = autotune.tune_backprojection(ctx, filt, vn, row_scales=sc, path=path)
     assert r2["cached"] and r2["config"] == r1["config"] and ctx.bp_config().key() == r1["config"]
+
+
+def test_run_timed_matches_run(orc, tiny):
+    spec, raw = tiny
+    ctx, cg, gp = make_ctx(spec, tex_weights=1)
+    a, b = ctx.alloc("volume"), ctx.alloc("volume")
+    ctx.run(dev(raw), a)
+    ms = ctx.run_timed(dev(raw), b)
+    torch.cuda.synchronize()
+    assert set(ms) == {"rebin", "filter", "backproject", "thicken"} and all(v > 0 for v in ms.values())
+    assert np.array_equal(a.cpu().numpy(), b.cpu().numpy(), equal_nan=True)

@@ -8,6 +8,7 @@ import socket
 import numpy as np
 import pytest
 
+from freect_b200 import abi_types as T
 from freect_b200 import scans, shard, wfbp
 
 torch = pytest.importorskip("torch")
@@ -19,12 +20,21 @@ def _geometry(spec):
     return cg, spec.recon_config(), tube, table
 
 
+def test_effective_geometry_matches_oracle(orc):
+    for mode in (T.FFS_NONE, T.FFS_PHI, T.FFS_Z, T.FFS_PHIZ):
+        spec = scans.tiny_ffs(mode=mode)
+        tube, table = spec.views()
+        cg, _ = wfbp.configure_geometry(spec.meta(), table)
+        eff = wfbp.effective_geometry(cg)
+        assert bytes(eff) == (bytes(cg) if mode == T.FFS_NONE else bytes(orc.ffs_effective(cg)))
+
+
 @pytest.mark.parametrize("name", ["tiny", "small", "rows64", "ffs"])
 @pytest.mark.parametrize("world", [1, 2, 3, 8])
 def test_plan_covers_and_aligns(name, world):
     spec = scans.WORKLOADS[name]()
     cg, rp, tube, table = _geometry(spec)
-    nat, req = wfbp.slice_locations(cg, rp)
+    nat, req = wfbp.slice_locations(wfbp.effective_geometry(cg), rp)
     if world > req.size:
         pytest.skip("fewer slices than ranks")
     plans = shard.plan(cg, rp, table, world)
