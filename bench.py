@@ -6,9 +6,12 @@ rows, 984 views/rotation, 10 rotations, 512 x 512 x 300 slices @ 1 mm),
 through the C ABI. Metric: contributing backprojection voxel-view updates per
 second over the whole step (whole job over all ranks), with s/volume beside
 it. Inputs (2.2 GB raw frames) are larger than L2, so no flush is needed.
+By default both precision forms run: the mixed form is the headline line,
+the FP32 form is reported beside it ("fp32", "mixed_speedup_vs_fp32"), and
+each form's volume is checked in HU against the FP64 oracle on one slab.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision fp32|mixed] [--workload rows64|small]
+                  [--precision both|fp32|mixed] [--workload rows64|small|ffs|batch24|...]
 
 Under torchrun each rank reconstructs its own independently seeded scan
 (weak scaling, no collective on the data path).
@@ -35,12 +38,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp32", "mixed"],
+                    help="both: the mixed form is the headline line, the FP32 form is reported beside it")
     ap.add_argument("--workload", default="rows64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-slices", type=int, default=1)
     ap.add_argument("--no-tune", action="store_true", help="keep the default backprojection configuration")
+    ap.add_argument("--no-hu", action="store_true", help="skip the HU check against the FP64 oracle")
     return ap.parse_args()
 
 
@@ -375,15 +380,97 @@ def main():
     tube, table = spec.views()
     cg, gp = wfbp.configure_geometry(spec.meta(), table)
     rp = spec.recon_config()
-    prec = T.PRECISION_MIXED if args.precision == "mixed" else T.PRECISION_FP32
+    raw = torch.empty((spec.V, spec.nr, spec.nch), dtype=torch.float32, device=dev)
+    wfbp.synth_project(spec.synth(), spec.ellipsoids(), raw)
+    torch.cuda.synchronize()
+    forms = ["mixed", "fp32"] if args.precision == "both" else [args.precision]
+    res = {f: measure_form(args, f, spec, cg, rp, tube, table, raw, dev, stream, dist, local) for f in forms}
+    head = res[forms[0]]
+    line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": head["dtype"],
+            "data": "synthetic (seeded ellipsoid phantom, Poisson noise)",
+            "config": {"workload": spec.name, "channels": spec.nch, "rows": spec.nr, "views": spec.V,
+                       "volume": [head["dims"].n_slices_requested, head["dims"].ny, head["dims"].nx],
+                       "native_slices": head["dims"].n_slices_native, "precision": forms[0],
+                       "parallelism": "independent scan per GPU",
+                       "l2": "inputs larger than L2 (%.2f GB raw frames, %.2f GB filtered rows)"
+                             % (head["dims"].raw_bytes / 1e9, head["dims"].filtered_bytes / 1e9),
+                       "bp_config": head["bp_config"], "bp_tuning_ms": head["tuning"]},
+            "s_per_volume": head["ms"] / 1000.0, "updates_per_volume": head["updates"],
+            "stage_ms": head["stage"], "roofline": head["roofline"], "gpu_launches": 4 * args.steps,
+            "e2e": head["e2e"], "clocks": head["clocks"]}
+    if "hu_vs_fp64" in head:
+        line["hu_vs_fp64"] = head["hu_vs_fp64"]
+    if len(forms) == 2:
+        f32 = res["fp32"]
+        line["fp32"] = {k: f32[k] for k in ("value", "ms", "stage", "roofline", "e2e", "bp_config", "clocks")
+                        if k in f32}
+        if "hu_vs_fp64" in f32:
+            line["fp32"]["hu_vs_fp64"] = f32["hu_vs_fp64"]
+        line["mixed_speedup_vs_fp32"] = {"device": f32["ms"] / head["ms"],
+                                         "e2e": (f32["e2e"]["ms_per_step"] / head["e2e"]["ms_per_step"])
+                                         if head["e2e"] and f32["e2e"] else None}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_baseline(spec, lambda v0, v1: raw[v0:v1].cpu().numpy(), n_slices=args.cpu_slices)
+            full = head["updates"] / cb["t_full_est"]
+            line["cpu_baseline"] = {
+                "value": full, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                "sample": "oracle FP32 transcript: rebin+filter of %d of %d views, backprojection of %d of %d native "
+                          "slices (%d updates) in %.1f s + %.1f s; scaled linearly to the full volume"
+                          % (cb["views"], spec.V, cb["slices"], head["dims"].n_slices_native, cb["updates_sample"],
+                             cb["t_rf_sample"], cb["t_bp_sample"]),
+                "s_per_volume_est": cb["t_full_est"]}
+        except Exception as ex:  # reported, not fatal
+            line["cpu_baseline"] = {"error": repr(ex)}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def hu_vs_fp64(spec, cg, rp, tube, table, raw, vol):
+    """HU error of `vol` against the FP64 oracle on the slab of the middle
+    requested slice: the oracle reconstructs that slab from its own window of
+    readings with the whole scan's slice positions and index angles (the
+    construction of freect_b200.shard), which equals the whole-scan FP64
+    result there. Returns rms, max, voxels."""
+    import numpy as np
+    from freect_b200 import shard
+    from oracle import oracle as O
+    if cg.ffs_phi or cg.ffs_z:
+        return None
+    O.set_threads(os.cpu_count() or 1)
+    nat, req = O.slice_locations(cg, rp)
+    plans = shard.plan(cg, rp, table, req.size)
+    p = plans[req.size // 2]
+    a0, a1 = p.readings
+    scg = shard.sub_geometry(cg, p)
+    t0 = time.perf_counter()
+    x = O.rebin_f64(scg, raw[a0:a1].cpu().numpy(), offset=a0)
+    y = O.filter_f64(x, O.taps_f64(scg, spec.window))
+    zn, zr = nat[p.native[0]:p.native[1]], req[p.requested[0]:p.requested[1]]
+    vn, _ = O.backproject_f64(scg, rp, y, tube[a0:a1].astype(np.float64), table[a0:a1].astype(np.float64), zn)
+    ref = O.thicken_f64(rp, vn, zn, zr)
+    got = vol[p.requested[0]:p.requested[1]].cpu().numpy()
+    rms, mx, n = O.hu_error(got, ref)
+    return {"rms": rms, "max": mx, "voxels": n, "requested_slices": list(p.requested),
+            "oracle_seconds": time.perf_counter() - t0,
+            "note": "FP64 oracle on the slab of the middle requested slice, full-coverage voxels"}
+
+
+def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, local):
+    import torch
+    from freect_b200 import abi_types as T
+    from freect_b200 import wfbp
+    prec = T.PRECISION_MIXED if form == "mixed" else T.PRECISION_FP32
     ext = wfbp.make_ext(precision=prec, filter_window=spec.window, tex_weights=1 if prec == T.PRECISION_FP32 else 0,
                         filtered_layout=T.LAYOUT_BACKPROJECTION)
     ctx = wfbp.Context(cg, rp, ext, device=local)
     ctx.set_views(tube, table)
     d = ctx.dims
-
-    raw = ctx.alloc("raw")
-    wfbp.synth_project(spec.synth(), spec.ellipsoids(), raw)
     reb = ctx.alloc("rebinned")
     filt = ctx.alloc("filtered")
     scales = ctx.alloc("row_scales")
@@ -479,45 +566,23 @@ def main():
 
     hbm, bf16, peak_src = load_peaks()
     elem = 4 if prec == T.PRECISION_FP32 else 2
-    bp_bytes = updates * 4 * elem
-    achieved = bp_bytes / (stage["backproject"] / 1000.0) / 1e9
+    achieved = updates * 4 * elem / (stage["backproject"] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": "backproject", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": None, "peak_source": peak_src,
                 "algorithmic_bytes_per_update": 4 * elem,
-                "note": "4 bilinear taps per contributing update, read through L1/shared memory"}
-
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if prec == T.PRECISION_FP32 else "f16-storage/f32-accumulate",
-            "data": "synthetic (seeded ellipsoid phantom, Poisson noise)",
-            "config": {"workload": spec.name, "channels": spec.nch, "rows": spec.nr, "views": spec.V,
-                       "volume": [d.n_slices_requested, d.ny, d.nx], "native_slices": d.n_slices_native,
-                       "precision": args.precision, "parallelism": "independent scan per GPU",
-                       "l2": "inputs larger than L2 (%.2f GB raw frames, %.2f GB filtered rows)"
-                             % (d.raw_bytes / 1e9, d.filtered_bytes / 1e9),
-                       "bp_config": "%dx%d/%d" % ctx.bp_config().key(),
-                       "bp_tuning_ms": tuned["times_ms"] if tuned else None},
-            "s_per_volume": ms / 1000.0, "updates_per_volume": updates, "stage_ms": stage,
-            "roofline": roofline, "gpu_launches": 4 * args.steps, "e2e": e2e, "clocks": clk}
-    if rank == 0 and world == 1 and not args.no_cpu:
+                "note": "4 bilinear taps per contributing update, read from shared memory after one TMA "
+                        "staging per view window; the kernel is issue-bound (ncu summaries under profiles/)"}
+    out = {"value": value, "ms": ms, "stage": stage, "updates": updates, "e2e": e2e, "clocks": clk,
+           "roofline": roofline, "dims": d, "tuning": tuned["times_ms"] if tuned else None,
+           "bp_config": "%dx%d/%d" % ctx.bp_config().key(),
+           "dtype": "f32" if prec == T.PRECISION_FP32 else "f16-storage/f32-accumulate"}
+    if not args.no_hu and int(os.environ.get("RANK", "0")) == 0:
         try:
-            cb = cpu_baseline(spec, lambda v0, v1: raw[v0:v1].cpu().numpy(), n_slices=args.cpu_slices)
-            full = updates / cb["t_full_est"]
-            line["cpu_baseline"] = {
-                "value": full, "unit": UNIT, "cores": cb["cores"], "kind": "port",
-                "sample": "oracle FP32 transcript: rebin+filter of %d of %d views, backprojection of %d of %d native "
-                          "slices (%d updates) in %.1f s + %.1f s; scaled linearly to the full volume"
-                          % (cb["views"], spec.V, cb["slices"], d.n_slices_native, cb["updates_sample"],
-                             cb["t_rf_sample"], cb["t_bp_sample"]),
-                "s_per_volume_est": cb["t_full_est"]}
+            out["hu_vs_fp64"] = hu_vs_fp64(spec, cg, rp, tube, table, raw, vol)
         except Exception as ex:  # reported, not fatal
-            line["cpu_baseline"] = {"error": repr(ex)}
-    if rank == 0:
-        print(json.dumps(line))
+            out["hu_vs_fp64"] = {"error": repr(ex)}
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    return out
 
 
 if __name__ == "__main__":

@@ -36,7 +36,7 @@ def sources():
 
 def _compile(src, extra):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "freect_wfbp.h"))
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj, ""

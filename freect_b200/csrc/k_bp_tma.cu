@@ -166,66 +166,84 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
 
   if (warp == BT_CWARPS) {
     // ---------------- producer ----------------
-    if (lane == 0) {
-      const float zlo = zmn - bt.reach, zhi = zmx + bt.reach;
-      const float xa = xcoord(ix0), xb = xcoord(min(ix0 + bt.tx - 1, p.nx - 1));
-      const float ya = ycoord(iy0), yb = ycoord(min(iy0 + bt.ty - 1, p.ny - 1));
-      const uint32_t view_bytes = (uint32_t)(bt.W * bt.nrp * sizeof(T));
-      int issued_upto = 0;
-      for (int t = 0; t < p.P2; t++) {
-        const uint32_t g = ring + (uint32_t)t;
-        const int s = (int)(g & 1u);
-        const uint32_t u = g >> 1;
-        if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1)) {
-          *s_fail = 1;
-          break;
-        }
-        if (*s_fail) break;
-        int nv = 0;
-        for (int k = 0; k < p.K; k++) {
-          const int j = t + k * p.P2;
+    // The 32 lanes test the half turns k of theta~ in parallel (lane = k
+    // mod 32), the selected views are compacted in k order with a ballot, and
+    // their copies are issued by as many lanes.
+    const float zlo = zmn - bt.reach, zhi = zmx + bt.reach;
+    const float xa = xcoord(ix0), xb = xcoord(min(ix0 + bt.tx - 1, p.nx - 1));
+    const float ya = ycoord(iy0), yb = ycoord(min(iy0 + bt.ty - 1, p.ny - 1));
+    const uint32_t view_bytes = (uint32_t)(bt.W * bt.nrp * sizeof(T));
+    const unsigned below = (1u << lane) - 1u;
+    int issued_upto = 0;
+    bool failed = false;
+    for (int t = 0; t < p.P2; t++) {
+      const uint32_t g = ring + (uint32_t)t;
+      const int s = (int)(g & 1u);
+      const uint32_t u = g >> 1;
+      int ok = 1;
+      if (lane == 0) ok = (u < 1 || mbar_wait(&empty[s], (u - 1) & 1)) && !*s_fail;
+      if (!__shfl_sync(0xffffffffu, ok, 0)) {
+        failed = true;
+        break;
+      }
+      int nv = 0;
+      for (int kb = 0; kb < p.K; kb += 32) {
+        const int k = kb + lane;
+        const int j = t + k * p.P2;
+        bool sel = false;
+        int c_lo = 0;
+        if (k < p.K) {
           const float zt = __ldg(view_z + j);
-          if (zt < zlo || zt > zhi) continue;
-          if (nv == bt.nv_max) {
-            atomicOr(err, 0x100);  // more views than slots: host sizing violated
-            break;
+          if (!(zt < zlo || zt > zhi)) {
+            const float2 sc = __ldg(view_sc + j);
+            const float p1 = xa * sc.x - ya * sc.y, p2 = xa * sc.x - yb * sc.y;
+            const float p3 = xb * sc.x - ya * sc.y, p4 = xb * sc.x - yb * sc.y;
+            const float pmax = fmaxf(fmaxf(p1, p2), fmaxf(p3, p4));
+            const float pmin = fminf(fminf(p1, p2), fminf(p3, p4));
+            // rows this tile can use: q in [0, nr-2] needs |z - zt + A| <= l_hat tan,
+            // with l_hat <= R - min(t) over the tile and A monotonic in p_hat
+            const float t1 = xa * sc.y + ya * sc.x, t2 = xa * sc.y + yb * sc.x;
+            const float t3 = xb * sc.y + ya * sc.x, t4 = xb * sc.y + yb * sc.x;
+            const float lhi = sqrtf(p.R2) - fminf(fminf(t1, t2), fminf(t3, t4));
+            const float amin = p.zr2pi * asinf(p.rR * pmin), amax = p.zr2pi * asinf(p.rR * pmax);
+            const float eps = 1e-3f * (1.0f + fabsf(zt));
+            const float wlo = zt - amax - lhi * p.tanc - eps, whi = zt - amin + lhi * p.tanc + eps;
+            sel = !(whi < zmn || wlo > zmx);
+            const float idx_min = p.kp - (pmax * p.ps + p.c0);  // p_idx decreases with p_hat
+            c_lo = max(0, min((int)floorf(idx_min) - 1, p.nch - bt.W));
           }
-          const float2 sc = __ldg(view_sc + j);
-          const float p1 = xa * sc.x - ya * sc.y, p2 = xa * sc.x - yb * sc.y;
-          const float p3 = xb * sc.x - ya * sc.y, p4 = xb * sc.x - yb * sc.y;
-          const float pmax = fmaxf(fmaxf(p1, p2), fmaxf(p3, p4));
-          const float pmin = fminf(fminf(p1, p2), fminf(p3, p4));
-          // rows this tile can use: q in [0, nr-2] needs |z - zt + A| <= l_hat tan,
-          // with l_hat <= R - min(t) over the tile and A monotonic in p_hat
-          const float t1 = xa * sc.y + ya * sc.x, t2 = xa * sc.y + yb * sc.x;
-          const float t3 = xb * sc.y + ya * sc.x, t4 = xb * sc.y + yb * sc.x;
-          const float lhi = sqrtf(p.R2) - fminf(fminf(t1, t2), fminf(t3, t4));
-          const float amin = p.zr2pi * asinf(p.rR * pmin), amax = p.zr2pi * asinf(p.rR * pmax);
-          const float eps = 1e-3f * (1.0f + fabsf(zt));
-          const float wlo = zt - amax - lhi * p.tanc - eps, whi = zt - amin + lhi * p.tanc + eps;
-          if (whi < zmn || wlo > zmx) continue;
-          const float idx_min = p.kp - (pmax * p.ps + p.c0);  // p_idx decreases with p_hat
-          int c_lo = (int)floorf(idx_min) - 1;
-          c_lo = max(0, min(c_lo, p.nch - bt.W));
-          vinfo[s * bt.nv_max + nv] = make_int2(j, c_lo);
-          vsv[s * bt.nv_max + nv] = HALF ? __ldg(view_scale + j) : 1.0f;
-          nv++;
         }
+        const unsigned m = __ballot_sync(0xffffffffu, sel);
+        const int pos = nv + __popc(m & below);
+        if (sel) {
+          if (pos < bt.nv_max) {
+            vinfo[s * bt.nv_max + pos] = make_int2(j, c_lo);
+            vsv[s * bt.nv_max + pos] = HALF ? __ldg(view_scale + j) : 1.0f;
+          } else {
+            atomicOr(err, 0x100);  // more views than slots: host sizing violated
+          }
+        }
+        nv = min(nv + __popc(m), bt.nv_max);
+      }
+      __syncwarp();
+      if (lane == 0) {
         nvs[s] = nv;
         mbar_arrive_tx(&full[s], (uint32_t)nv * view_bytes);
-        for (int v = 0; v < nv; v++) {
-          const int2 vi = vinfo[s * bt.nv_max + v];
-          tma_load_3d(slots + ((size_t)s * bt.nv_max + v) * bt.slot_bytes, map, &full[s], 0, vi.y, vi.x);
-        }
-        issued_upto = t + 1;
       }
-      if (*s_fail) {
-        atomicExch(err, WFBP_ERR_TIMEOUT);
-        // let copies already issued land before the CTA's shared memory goes away
-        for (int t = max(0, issued_upto - BT_STAGES); t < issued_upto; t++) {
-          const uint32_t g = ring + (uint32_t)t;
-          mbar_wait(&full[g & 1u], (g >> 1) & 1u);
-        }
+      __syncwarp();
+      for (int v = lane; v < nv; v += 32) {
+        const int2 vi = vinfo[s * bt.nv_max + v];
+        tma_load_3d(slots + ((size_t)s * bt.nv_max + v) * bt.slot_bytes, map, &full[s], 0, vi.y, vi.x);
+      }
+      issued_upto = t + 1;
+    }
+    if (failed && lane == 0) {
+      *s_fail = 1;
+      atomicExch(err, WFBP_ERR_TIMEOUT);
+      // let copies already issued land before the CTA's shared memory goes away
+      for (int t = max(0, issued_upto - BT_STAGES); t < issued_upto; t++) {
+        const uint32_t g = ring + (uint32_t)t;
+        mbar_wait(&full[g & 1u], (g >> 1) & 1u);
       }
     }
     return p.P2;
