@@ -104,9 +104,13 @@ cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, 
 // nch-1 on each side, the data window of that circular convolution equals the
 // linear convolution y[n] = sum_k h[|n-k|] x[k] over the nch channels: a
 // [rows x nch] x [nch x nch] product with a symmetric Toeplitz matrix. This
-// kernel evaluates it in FP32 on the CUDA cores: 128x128 output tiles, 8x8
-// per thread, the Toeplitz operand read from a shared-memory tap line
-// htab[d + NTAB] = h[|d|] so the inner loop needs no index arithmetic.
+// kernel evaluates it in FP32 on the CUDA cores: 128x128 output tiles, 8 rows
+// x 8 consecutive columns per thread. The Toeplitz operand comes from a
+// shared-memory tap line htab[d + nch] = h[|d|] (zero past the ends): for
+// consecutive k a thread's 8 operand values are a window sliding down the
+// line by one, so each k step loads one new tap. Rows are processed in pairs
+// with the packed FP32x2 FMA; every output still accumulates its products in
+// k order, one rounding per FMA.
 constexpr int TF_BM = 128, TF_BN = 128, TF_BK = 16;
 
 // TR = true writes the backprojection layout Y_T[view][channel][row] with
@@ -117,23 +121,27 @@ k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* 
                int nch, int nr, int nrp) {
   extern __shared__ float smem[];
   float* As = smem;                          // [TF_BK][TF_BM + 4]
-  float* htab = smem + TF_BK * (TF_BM + 4);  // [2*nch + 1], htab[d + nch] = h[|d|]
+  // tap line htab[d + nch + TF_BK] = h[|d|] for -nch - TF_BK <= d <= nch + TF_BN, 0 where |d| >= nch:
+  // the last k block runs up to TF_BK - 1 past nch (zero rows of A) and the
+  // last column block up to TF_BN - 1 past nch (columns that are not stored)
+  float* htab = smem + TF_BK * (TF_BM + 4);
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
   const long m0 = (long)blockIdx.x * TF_BM;
   const int n0 = blockIdx.y * TF_BN;
-  for (int d = tid; d < 2 * nch + 1; d += 256) {
-    int a = d - nch;
+  for (int d = tid; d < 2 * nch + TF_BN + TF_BK + 1; d += 256) {
+    int a = d - nch - TF_BK;
     a = a < 0 ? -a : a;
     htab[d] = a < nch ? taps[a] : 0.0f;
   }
-  float acc[8][8];
+  float2 acc[4][8];  // acc[i][j] = (row 2i, row 2i+1) of column j
 #pragma unroll
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+    for (int j = 0; j < 8; j++) acc[i][j] = make_float2(0.0f, 0.0f);
 
-  // column n_j = n0 + tx + 16 j; output columns >= nch are discarded
+  // thread columns n0 + 8 tx + j; operand h[|n - k|] = htab[n - k + nch + TF_BK]
+  const int hb = n0 + 8 * tx + nch + TF_BK;
   for (int k0 = 0; k0 < nch; k0 += TF_BK) {
     __syncthreads();
     // A tile: 128 rows x 16 k, stored k-major
@@ -144,24 +152,25 @@ k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* 
       As[kk * (TF_BM + 4) + mm] = (m < M && k < nch) ? X[m * nch + k] : 0.0f;
     }
     __syncthreads();
+    // operand window for k = k0: b[j] = htab[hb - k0 + j]
+    float b[TF_BK + 8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) b[TF_BK + j] = htab[hb - k0 + j];
 #pragma unroll
     for (int kk = 0; kk < TF_BK; kk++) {
-      float a[8], b[8];
-      float4 a0 = *reinterpret_cast<const float4*>(&As[kk * (TF_BM + 4) + ty * 8]);
-      float4 a1 = *reinterpret_cast<const float4*>(&As[kk * (TF_BM + 4) + ty * 8 + 4]);
-      a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
-      a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
-      const int k = k0 + kk;
+      // window for k0 + kk is b[TF_BK - kk .. TF_BK - kk + 7]
+      if (kk > 0) b[TF_BK - kk] = htab[hb - k0 - kk];
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[kk * (TF_BM + 4) + ty * 8]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[kk * (TF_BM + 4) + ty * 8 + 4]);
+      const float2 ap[4] = {make_float2(a0.x, a0.y), make_float2(a0.z, a0.w), make_float2(a1.x, a1.y),
+                            make_float2(a1.z, a1.w)};
 #pragma unroll
       for (int j = 0; j < 8; j++) {
-        int d = n0 + tx + 16 * j - k;  // in (-nch, nch + 128)
-        d = d > nch ? nch : d;         // columns beyond nch read h=0 slot
-        b[j] = htab[d + nch];
+        const float bj = b[TF_BK - kk + j];
+        const float2 bb = make_float2(bj, bj);
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[i][j] = __ffma2_rn(ap[i], bb, acc[i][j]);
       }
-#pragma unroll
-      for (int i = 0; i < 8; i++)
-#pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
     }
   }
 #pragma unroll
@@ -171,12 +180,13 @@ k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* 
     const long v = m / nr, row = m % nr;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-      int n = n0 + tx + 16 * j;
+      const int n = n0 + 8 * tx + j;
+      const float val = (i & 1) ? acc[i >> 1][j].y : acc[i >> 1][j].x;
       if (n < nch) {
         if (TR)
-          Y[((size_t)v * nch + n) * nrp + row] = acc[i][j];
+          Y[((size_t)v * nch + n) * nrp + row] = val;
         else
-          Y[m * nch + n] = acc[i][j];
+          Y[m * nch + n] = val;
       }
     }
   }
@@ -185,7 +195,7 @@ k_toeplitz_f32(const float* __restrict__ X, float* __restrict__ Y, const float* 
 template <bool TR>
 cudaError_t launch_toeplitz_f32(const float* x, float* y, const float* d_taps, long rows, int nch, int nr, int nrp,
                                 cudaStream_t s) {
-  size_t smem = sizeof(float) * (TF_BK * (TF_BM + 4) + 2 * nch + 1);
+  size_t smem = sizeof(float) * (TF_BK * (TF_BM + 4) + 2 * nch + TF_BN + TF_BK + 1);
   if (smem > 64 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_toeplitz_f32<TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
   if (e != cudaSuccess) return e;

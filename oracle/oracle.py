@@ -56,6 +56,7 @@ def load():
             "orc_voxelize": (None, [C.POINTER(T.Ellipsoid), C.c_int, R, _D, C.c_int, C.c_double, C.c_int, _D]),
             "orc_ffs_effective": (C.c_int, [G, G]),
             "orc_rebin_ffs_f64": (C.c_int, [G, _F, _D]),
+            "orc_rebin_ffs_f64_off": (C.c_int, [G, _F, C.c_long, _D]),
             "orc_thicken_adjoint_f64": (None, [R, _D, _D, C.c_int, _D, C.c_int, _D]),
             "orc_backproject_adjoint_f64": (None, [G, R, _D, _D, _D, _D, C.c_int, _D]),
             "orc_taps_gradient_f64": (None, [C.c_int, C.c_long, _D, _D, C.c_int, _D]),
@@ -270,12 +271,13 @@ def ffs_effective(cg):
     return ce
 
 
-def rebin_ffs_f64(cg, raw):
+def rebin_ffs_f64(cg, raw, offset_views=0):
+    """offset_views: index of raw's first view (focal-state cycle) within the whole scan."""
     ce = ffs_effective(cg)
     out = np.zeros((int(ce.total_number_of_projections), int(ce.num_detector_rows), int(ce.num_detector_cols)),
                    np.float64)
     r = _f(raw)
-    st = load().orc_rebin_ffs_f64(C.byref(cg), fp(r), dp(out))
+    st = load().orc_rebin_ffs_f64_off(C.byref(cg), fp(r), int(offset_views), dp(out))
     if st:
         raise ValueError("orc_rebin_ffs_f64: status %d" % st)
     return out
@@ -301,6 +303,26 @@ def reconstruct_f64(spec, raw, taps_half=None):
     vol = thicken_f64(rp, vn, zn, zr)
     return dict(cg=cg, gp=gp, rp=rp, rebinned=reb, filtered=filt, native=vn, volume=vol, z_native=zn, z_req=zr,
                 updates=n_updates)
+
+
+def reconstruct_window_f64(cg, rp, window, tube_w, table_w, raw_w, offset_readings, z_native, z_req):
+    """FP64 oracle of a slab reconstructed from a window of a scan's readings:
+    cg is the whole scan's geometry with total_number_of_projections set to
+    the window's readings (z_rot kept), offset_readings the window's first
+    reading; the rebin uses the whole scan's index angles, the slices are the
+    given lists. With FFS the window starts on a focal-state cycle."""
+    G = (2 if cg.ffs_phi else 1) * (2 if cg.ffs_z else 1)
+    if G > 1:
+        x = rebin_ffs_f64(cg, raw_w, offset_views=offset_readings // G)
+        ce = ffs_effective(cg)
+    else:
+        x = rebin_f64(cg, raw_w, offset=offset_readings)
+        ce = cg
+    y = filter_f64(x, taps_f64(ce, window))
+    tw = np.asarray(tube_w, np.float64)[::G]
+    zw = np.asarray(table_w, np.float64)[::G]
+    vn, _ = backproject_f64(ce, rp, y, tw, zw, z_native)
+    return thicken_f64(rp, vn, z_native, z_req)
 
 
 def hu_error(a, b, mu_water=0.019):

@@ -977,7 +977,7 @@ ORC_EXPORT int orc_ffs_effective(const CTGeometry* in, CTGeometry* out) {
  * channels around bidx, each from its own focal state's readings (linear in
  * reading angle between that state's neighbouring readings). out:
  * [V/G][nr_eff][nch_eff]. */
-typedef struct { const CTGeometry* cg; const CTGeometry* ce; const float* raw; double* out; } rbf_args;
+typedef struct { const CTGeometry* cg; const CTGeometry* ce; const float* raw; double* out; long off; } rbf_args;
 static void rbf_body(void* a_, long i0, long i1) {
   rbf_args* a = (rbf_args*)a_;
   const CTGeometry* cg = a->cg; const CTGeometry* ce = a->ce;
@@ -996,7 +996,7 @@ static void rbf_body(void* a_, long i0, long i1) {
       double val = 0.0;
       if (!(bidx < 0 || bidx >= (double)nche || isnan(bidx))) {
         double fx = floor(bidx), ax = bidx - fx;
-        double nf = (double)G * v - beta / dth;
+        double nf = (double)G * (v + a->off) - beta / dth;  /* whole-scan reading index */
         for (int t = 0; t < 2; t++) {
           long e = (long)fx + t;
           if (e < 0) e = 0;
@@ -1007,7 +1007,7 @@ static void rbf_body(void* a_, long i0, long i1) {
           int rho = (G == 4) ? sp + 2 * zs : (phi ? sp : zs);
           double mf = (nf - rho) / G, m0 = floor(mf), ay = mf - m0;
           for (int u = 0; u < 2; u++) {
-            long m = (long)m0 + u;
+            long m = (long)m0 + u - a->off;
             if (m < 0) m = 0;
             if (m > Ve - 1) m = Ve - 1;
             double wy = u ? ay : 1.0 - ay;
@@ -1020,13 +1020,17 @@ static void rbf_body(void* a_, long i0, long i1) {
     }
   }
 }
-ORC_EXPORT int orc_rebin_ffs_f64(const CTGeometry* cg, const float* raw, double* out) {
+/* off: index of the first view (focal-state cycle) of raw within the whole scan */
+ORC_EXPORT int orc_rebin_ffs_f64_off(const CTGeometry* cg, const float* raw, long off, double* out) {
   CTGeometry ce;
   int st = orc_ffs_effective(cg, &ce);
   if (st) return st;
-  rbf_args a = {cg, &ce, raw, out};
+  rbf_args a = {cg, &ce, raw, out, off};
   orc_parallel_for((long)ce.total_number_of_projections * (long)ce.num_detector_rows, 16, rbf_body, &a);
   return WFBP_OK;
+}
+ORC_EXPORT int orc_rebin_ffs_f64(const CTGeometry* cg, const float* raw, double* out) {
+  return orc_rebin_ffs_f64_off(cg, raw, 0, out);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -331,3 +331,37 @@ def test_run_timed_matches_run(orc, tiny):
     torch.cuda.synchronize()
     assert set(ms) == {"rebin", "filter", "backproject", "thicken"} and all(v > 0 for v in ms.values())
     assert np.array_equal(a.cpu().numpy(), b.cpu().numpy(), equal_nan=True)
+
+
+@pytest.mark.parametrize("precision", [T.PRECISION_FP32, T.PRECISION_MIXED])
+def test_descending_slices_and_origin_offset(orc, precision):
+    # start_pos > end_pos (slice lists run downwards, ReconstructionMachine.cu:116-132)
+    # and a reconstruction grid centred off the isocentre (x_origin, y_origin)
+    spec = scans.tiny(nch=96, nr=8, P=96, rotations=3, nx=32, n_slices=4)
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    rp.start_pos, rp.end_pos = rp.end_pos - 0.5 * rp.slice_pitch, rp.start_pos - 0.5 * rp.slice_pitch
+    rp.x_origin, rp.y_origin = 7.5, -4.25
+    ext = wfbp.make_ext(precision=precision, filter_window=spec.window,
+                        tex_weights=1 if precision == T.PRECISION_FP32 else 0)
+    ctx = wfbp.Context(cg, rp, ext, device=0)
+    ctx.set_views(tube, table)
+    nat, req = ctx.slices()
+    assert nat[1] < nat[0] and req[1] < req[0]
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    ctx.check_device_status()
+    got = vol.cpu().numpy()
+    # the same reconstruction through the FP64 oracle's stages with these slice lists
+    zn, zr = orc.slice_locations(cg, rp)
+    assert np.array_equal(zn, nat) and np.array_equal(zr, req)
+    x = orc.rebin_f64(cg, raw)
+    y = orc.filter_f64(x, orc.taps_f64(cg, spec.window))
+    vn, _ = orc.backproject_f64(cg, rp, y, tube.astype(np.float64), table.astype(np.float64), zn)
+    ref = orc.thicken_f64(rp, vn, zn, zr)
+    rms, mx, n = orc.hu_error(got, ref)
+    assert n == np.isfinite(ref).sum() and n > 0
+    assert rms <= (0.5 if precision == T.PRECISION_FP32 else 1.0), (rms, mx)

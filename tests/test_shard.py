@@ -67,16 +67,13 @@ def test_plan_covers_and_aligns(name, world):
         assert v1 - 1 - need[-1] >= min(reach, V - 1 - need[-1])
 
 
-def _oracle_slab(orc, cg, rp, tube, table, raw, p):
+def _oracle_slab(orc, cg, rp, tube, table, raw, p, window=T.FILTER_REFERENCE):
     """The slab of plan p through the FP64 oracle, from the window's readings only."""
     a0, a1 = p.readings
-    scg = shard.sub_geometry(cg, p)
-    nat, req = orc.slice_locations(cg, rp)
-    zn, zr = nat[p.native[0]:p.native[1]], req[p.requested[0]:p.requested[1]]
-    x = orc.rebin_f64(scg, raw[a0:a1], offset=a0)
-    y = orc.filter_f64(x, orc.taps_f64(scg))
-    vn, _ = orc.backproject_f64(scg, rp, y, tube[a0:a1].astype(np.float64), table[a0:a1].astype(np.float64), zn)
-    return orc.thicken_f64(rp, vn, zn, zr)
+    ce = orc.ffs_effective(cg) if (cg.ffs_phi or cg.ffs_z) else cg
+    nat, req = orc.slice_locations(ce, rp)
+    return orc.reconstruct_window_f64(shard.sub_geometry(cg, p), rp, window, tube[a0:a1], table[a0:a1], raw[a0:a1],
+                                      a0, nat[p.native[0]:p.native[1]], req[p.requested[0]:p.requested[1]])
 
 
 def _rank_main(rank, world, port, result_path):
@@ -116,3 +113,13 @@ def test_sharded_oracle_two_ranks_matches_whole(orc, tmp_path):
     cg, rp, tube, table = _geometry(spec)
     parts = [_oracle_slab(orc, cg, rp, tube, table, raw, p) for p in shard.plan(cg, rp, table, 3)]
     assert np.array_equal(np.concatenate(parts), ref, equal_nan=True)
+
+
+def test_sharded_oracle_ffs_matches_whole(orc):
+    spec = scans.tiny_ffs(mode=T.FFS_PHIZ, nch=64, nr=4, P=128, rotations=6, nx=32, n_slices=12)
+    cg, rp, tube, table = _geometry(spec)
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    ref = orc.reconstruct_f64(spec, raw)["volume"]
+    for world in (2, 3):
+        parts = [_oracle_slab(orc, cg, rp, tube, table, raw, p) for p in shard.plan(cg, rp, table, world)]
+        assert np.array_equal(np.concatenate(parts), ref, equal_nan=True), world
