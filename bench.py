@@ -449,7 +449,7 @@ def run_batch(args, rank, world, local, dist):
                        "precision": "mixed, one persistent backprojection launch, CUDA graph replay",
                        "parallelism": "independent batch per GPU",
                        "l2": "inputs larger than L2 (%.1f GB raw frames)" % (sum(r.numel() for r in raws) * 4 / 1e9),
-                       "bp_config": "%dx%d/%d" % batch.bp_config().key(),
+                       "bp_config": autotune.config_name(batch.bp_config().key()),
                        "bp_tuning_ms": tuned["times_ms"] if tuned else None},
             "updates_per_step": updates, "fp32_per_scan_launches_ms": fp32_ms,
             "speedup_vs_fp32_per_scan": fp32_ms / ms, "hu_rms_mixed_vs_fp32_per_scan": hu_rms,
@@ -579,7 +579,7 @@ def hu_vs_fp64(spec, cg, rp, tube, table, raw, vol):
 def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, local):
     import torch
     from freect_b200 import abi_types as T
-    from freect_b200 import wfbp
+    from freect_b200 import autotune, wfbp
     prec = T.PRECISION_MIXED if form == "mixed" else T.PRECISION_FP32
     ext = wfbp.make_ext(precision=prec, filter_window=spec.window, tex_weights=1 if prec == T.PRECISION_FP32 else 0,
                         filtered_layout=T.LAYOUT_BACKPROJECTION)
@@ -602,7 +602,6 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
     tuned = None
     if not args.no_tune:
         # backprojection launch configuration from the autotuner (outside the timed region)
-        from freect_b200 import autotune
         ctx.rebin(raw, reb)
         ctx.filter(reb, filt, scales)
         tuned = autotune.tune_backprojection(ctx, filt, vn, row_scales=scales, use_cache=False)
@@ -689,7 +688,7 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
                         "staging per view window; the kernel is issue-bound (ncu summaries under profiles/)"}
     out = {"value": value, "ms": ms, "stage": stage, "updates": updates, "e2e": e2e, "clocks": clk,
            "roofline": roofline, "dims": d, "tuning": tuned["times_ms"] if tuned else None,
-           "bp_config": "%dx%d/%d" % ctx.bp_config().key(),
+           "bp_config": autotune.config_name(ctx.bp_config().key()),
            "dtype": "f32" if prec == T.PRECISION_FP32 else "f16-storage/f32-accumulate"}
     out["volume"] = vol
     ctx.close()

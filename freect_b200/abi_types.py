@@ -137,10 +137,10 @@ class Dims(C.Structure):
 
 class BpConfig(C.Structure):
     """wfbp_bp_config"""
-    _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("cols_per_step", C.c_int), ("reserved", C.c_int)]
+    _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("cols_per_step", C.c_int), ("consumer_warps", C.c_int)]
 
     def key(self):
-        return (self.tile_x, self.tile_y, self.cols_per_step)
+        return (self.tile_x, self.tile_y, self.cols_per_step, self.consumer_warps)
 
 
 class Ellipsoid(C.Structure):

@@ -1,8 +1,9 @@
 """Differentiable WFBP: a torch.autograd.Function over the C ABI.
 
 The forward pass is the FP32 form's four stages (wfbp_rebin, wfbp_filter,
-wfbp_backproject, wfbp_thicken, reference layout, exact texel weights); the
-backward pass runs their hand-written adjoint kernels in reverse
+wfbp_backproject, wfbp_thicken, exact texel weights; the TMA-staged
+backprojection in the backprojection layout where the geometry allows it);
+the backward pass runs their hand-written adjoint kernels in reverse
 (wfbp_thicken_adjoint, wfbp_backproject_adjoint, wfbp_filter_adjoint,
 wfbp_rebin_adjoint) and, for the learnable filter taps,
 wfbp_taps_gradient, which recomputes the rebinned rows from the saved raw
@@ -32,9 +33,16 @@ class Reconstructor:
     def __init__(self, cg, rp, tube_angles, table_positions, n_taps=64, filter_window=T.FILTER_REFERENCE,
                  device=0):
         ext = wfbp.make_ext(precision=T.PRECISION_FP32, filter_window=filter_window, tex_weights=0,
-                            filtered_layout=T.LAYOUT_REFERENCE)
+                            filtered_layout=T.LAYOUT_BACKPROJECTION)
         self.ctx = wfbp.Context(cg, rp, ext, device=device)
         self.ctx.set_views(tube_angles, table_positions)
+        try:
+            self.ctx.bp_config()
+        except wfbp.WfbpError:  # no TMA launch fits: the reference layout and the generic kernel
+            ext = wfbp.make_ext(precision=T.PRECISION_FP32, filter_window=filter_window, tex_weights=0,
+                                filtered_layout=T.LAYOUT_REFERENCE)
+            self.ctx = wfbp.Context(cg, rp, ext, device=device)
+            self.ctx.set_views(tube_angles, table_positions)
         self.device = torch.device("cuda", device)
         self.n_taps = int(n_taps)
         if not 1 <= self.n_taps <= self.ctx.dims.n_channels:
@@ -50,10 +58,14 @@ class Reconstructor:
         return self.base_taps[: self.n_taps].clone()
 
     def buf(self, name):
-        """Per-reconstructor scratch: rebinned / filtered [V][nr][nch], native volume."""
+        """Per-reconstructor scratch: rebinned / gradient rows [V][nr][nch], the
+        forward's filtered rows (context layout), native volume."""
         if name not in self._buf:
             d = self.ctx.dims
-            if name in ("rebinned", "filtered"):
+            if name == "filtered":
+                self._buf[name] = self.ctx.alloc("filtered")
+                return self._buf[name]
+            if name in ("rebinned", "rows"):
                 shape = (d.n_views, d.n_rows, d.n_channels)
             elif name == "native":
                 shape = (d.n_slices_native, d.ny, d.nx)
@@ -107,7 +119,7 @@ class WFBPFunction(torch.autograd.Function):
         g_raw = torch.empty_like(rb) if need_raw else None
         g_taps = torch.zeros_like(taps) if need_taps else None
         t_b = torch.empty_like(taps) if need_taps else None
-        gvn, gf, gr = rec.buf("native"), rec.buf("filtered"), rec.buf("rebinned")
+        gvn, gf, gr = rec.buf("native"), rec.buf("rows"), rec.buf("rebinned")
         for b in range(rb.shape[0]):
             ctx.thicken_adjoint(gb[b], gvn)
             ctx.backproject_adjoint(gvn, gf)

@@ -25,9 +25,14 @@ def signature(ctx):
     """Key of a tuning result: what the backprojection's cost depends on."""
     d = ctx.dims
     cg, gp = ctx.geometry()
-    return "v1|V%d|nr%d|nch%d|P%d|%dx%dx%d|prec%d|fov%.3f|ps%.5f|zrot%.4f" % (
+    return "v2|V%d|nr%d|nch%d|P%d|%dx%dx%d|prec%d|fov%.3f|ps%.5f|zrot%.4f" % (
         d.n_views, d.n_rows, d.n_channels, int(cg.projections_per_rotation), d.nx, d.ny, d.n_slices_native,
         d.precision, ctx.rp.recon_fov, gp.pixel_scale, cg.z_rot)
+
+
+def config_name(key):
+    """'16x16/4w16': column tile, columns per pass, consumer warps."""
+    return "%dx%d/%dw%d" % tuple(key)
 
 
 def _load(path):
@@ -64,7 +69,7 @@ def tune_backprojection(ctx, filtered, volume_native, row_scales=None, reps=2, u
         if hit:
             ctx.set_bp_config(tuple(hit["config"]))
             return {"config": tuple(hit["config"]), "times_ms": hit.get("times_ms", {}), "cached": True}
-    times = {}
+    times, keys = {}, {}
     for cfg in ctx.bp_configs():
         ctx.set_bp_config(cfg)
         ctx.backproject(filtered, volume_native, row_scales=row_scales)  # warm-up
@@ -75,13 +80,11 @@ def tune_backprojection(ctx, filtered, volume_native, row_scales=None, reps=2, u
         t1.record()
         torch.cuda.synchronize()
         ctx.check_device_status()
-        times["%dx%d/%d" % cfg.key()] = t0.elapsed_time(t1) / reps
+        times[config_name(cfg.key())] = t0.elapsed_time(t1) / reps
+        keys[config_name(cfg.key())] = cfg.key()
     if not times:
         raise RuntimeError("no backprojection configuration fits this geometry")
-    best = min(times, key=times.get)
-    tx, rest = best.split("x")
-    ty, cu = rest.split("/")
-    choice = (int(tx), int(ty), int(cu))
+    choice = keys[min(times, key=times.get)]
     ctx.set_bp_config(choice)
     if use_cache:
         table = _load(path)
@@ -109,7 +112,7 @@ def tune_batch(batch, raws, volumes, reps=1, use_cache=True, path=None):
         if hit:
             batch.set_bp_config(tuple(hit["config"]))
             return {"config": tuple(hit["config"]), "times_ms": hit.get("times_ms", {}), "cached": True}
-    times = {}
+    times, keys = {}, {}
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         for cfg in batch.bp_configs():
@@ -122,11 +125,9 @@ def tune_batch(batch, raws, volumes, reps=1, use_cache=True, path=None):
             t1.record(stream)
             stream.synchronize()
             batch.check_device_status()
-            times["%dx%d/%d" % cfg.key()] = t0.elapsed_time(t1) / reps
-    best = min(times, key=times.get)
-    tx, rest = best.split("x")
-    ty, cu = rest.split("/")
-    choice = (int(tx), int(ty), int(cu))
+            times[config_name(cfg.key())] = t0.elapsed_time(t1) / reps
+            keys[config_name(cfg.key())] = cfg.key()
+    choice = keys[min(times, key=times.get)]
     batch.set_bp_config(choice)
     if use_cache:
         table = _load(path)

@@ -37,7 +37,6 @@
 
 namespace {
 
-constexpr int BT_THREADS = (BT_CWARPS + 1) * 32;  // consumer warps + producer warp
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -84,13 +83,13 @@ __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y
 // of bp_smem_layout for the tile's scan.
 constexpr int BT_OFF_NVS = 64;  // int [16]: [0..1] views per stage, [8] failure flag, [9] next item
 
-__device__ __forceinline__ void bp_init_barriers(uint8_t* smem) {
+__device__ __forceinline__ void bp_init_barriers(uint8_t* smem, int nw) {
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   if (threadIdx.x == 0) {
     reinterpret_cast<int*>(smem + BT_OFF_NVS)[8] = 0;
     for (int s = 0; s < BT_STAGES; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&full[BT_STAGES + s], BT_CWARPS);
+      mbar_init(&full[BT_STAGES + s], nw);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -106,7 +105,7 @@ __device__ __forceinline__ void bp_init_barriers(uint8_t* smem) {
 // outside the reconstruction FOV (whose voxels are written as 0, the value
 // the reference leaves there). A bounded wait that gave up sets the failure
 // word (the CTA must stop).
-template <typename T, int CPW, int CU, bool COUNT>
+template <typename T, int CPW, int CU, int NW, bool COUNT>
 __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __restrict__ view_scale,
                                         float* __restrict__ vol, const float2* __restrict__ view_sc,
                                         const float* __restrict__ view_z, const float* __restrict__ zslices,
@@ -152,7 +151,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
     const float ya = ycoord(iy0), yb = ycoord(min(iy0 + bt.ty - 1, p.ny - 1));
     const float xn = fminf(fmaxf(0.0f, xa), xb), yn = fminf(fmaxf(0.0f, ya), yb);
     if (xn * xn + yn * yn > p.fov_half2 * 1.0001f + 1e-3f) {
-      if (warp < BT_CWARPS && my_s < p.nz) {
+      if (warp < NW && my_s < p.nz) {
         const size_t plane = (size_t)p.nx * p.ny;
         for (int c = 0; c < CPW; c++) {
           const int tt = warp * CPW + c;
@@ -164,7 +163,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
     }
   }
 
-  if (warp == BT_CWARPS) {
+  if (warp == NW) {
     // ---------------- producer ----------------
     // The 32 lanes test the half turns k of theta~ in parallel (lane = k
     // mod 32), the selected views are compacted in k order with a ballot, and
@@ -417,28 +416,28 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
 }
 
 // One tile per CTA: grid (tiles x, tiles y, 32-slice slabs).
-template <typename T, int CPW, int CU, bool COUNT>
-__global__ void __launch_bounds__(BT_THREADS, 1)
+template <typename T, int CPW, int CU, int NW, bool COUNT>
+__global__ void __launch_bounds__((NW + 1) * 32, 1)
 k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
          const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
          BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err) {
   // the dynamic shared memory is the only shared memory of this kernel, so
   // it starts at the (128-byte aligned) base of the CTA's window
   extern __shared__ __align__(128) uint8_t smem[];
-  bp_init_barriers(smem);
-  bp_tile<T, CPW, CU, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
-                             blockIdx.z, count, err, smem, 0u);
+  bp_init_barriers(smem, NW);
+  bp_tile<T, CPW, CU, NW, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
+                                 blockIdx.z, count, err, smem, 0u);
 }
 
 // Persistent launch over the column tiles of several scans: each CTA takes
 // the next work item (scan, tile x, tile y, slab) from a global counter until
 // the list is exhausted. Items are listed by decreasing estimated cost.
-template <typename T, int CPW, int CU>
-__global__ void __launch_bounds__(BT_THREADS, 1)
+template <typename T, int CPW, int CU, int NW>
+__global__ void __launch_bounds__((NW + 1) * 32, 1)
 k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items, int n_items,
                unsigned* __restrict__ next, int* __restrict__ err) {
   extern __shared__ __align__(128) uint8_t smem[];
-  bp_init_barriers(smem);
+  bp_init_barriers(smem, NW);
   volatile int* words = reinterpret_cast<volatile int*>(smem + BT_OFF_NVS);
   uint32_t ring = 0;
   for (;;) {
@@ -450,52 +449,57 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
     const BpScan* sd = scans + w.x;
     const BPParams p = sd->p;
     const BPTile bt = sd->bt;
-    ring += (uint32_t)bp_tile<T, CPW, CU, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
+    ring += (uint32_t)bp_tile<T, CPW, CU, NW, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
                                                  sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring);
     __syncthreads();  // the tile's shared memory and words[9] are free again
   }
 }
 
-template <typename T, int CPW, int CU>
+template <typename T, int CPW, int CU, int NW>
 cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                        unsigned long long* count, int* err, cudaStream_t s) {
   dim3 grid((unsigned)((p.nx + bt.tx - 1) / bt.tx), (unsigned)((p.ny + bt.ty - 1) / bt.ty), (unsigned)((p.nz + 31) / 32));
+  constexpr int threads = (NW + 1) * 32;
   cudaError_t e;
   if (count) {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt.smem_bytes);
+    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, true><<<grid, BT_THREADS, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt, count,
-                                                                      err);
+    k_bp_tma<T, CPW, CU, NW, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
+                                                                         count, err);
   } else {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt.smem_bytes);
+    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, false><<<grid, BT_THREADS, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
-                                                                       count, err);
+    k_bp_tma<T, CPW, CU, NW, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
+                                                                          count, err);
   }
   return cudaGetLastError();
 }
 
-template <typename T, int CPW, int CU>
+template <typename T, int CPW, int CU, int NW>
 cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
                              int smem_bytes, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(k_bp_tma_batch<T, CPW, CU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_bp_tma_batch<T, CPW, CU, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        smem_bytes);
   if (e != cudaSuccess) return e;
-  k_bp_tma_batch<T, CPW, CU><<<grid, BT_THREADS, smem_bytes, s>>>(scans, items, n_items, next, err);
+  k_bp_tma_batch<T, CPW, CU, NW><<<grid, (NW + 1) * 32, smem_bytes, s>>>(scans, items, n_items, next, err);
   return cudaGetLastError();
 }
+
+// The instantiated launch shapes: (columns per warp, columns per pass, consumer warps).
+#define WFBP_BP_SHAPES(X) X(16, 4, 16) X(16, 8, 16) X(8, 4, 16) X(8, 8, 16) X(4, 4, 16) X(8, 4, 20) X(8, 8, 20) X(4, 4, 24)
 
 template <typename T>
 cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                         const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                         unsigned long long* count, int* err, cudaStream_t s) {
-  const int cpw = bt.tx * bt.ty / BT_CWARPS;
-  if (cpw == 16 && bt.cu == 4) return launch_one<T, 16, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-  if (cpw == 16 && bt.cu == 8) return launch_one<T, 16, 8>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-  if (cpw == 8 && bt.cu == 4) return launch_one<T, 8, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-  if (cpw == 8 && bt.cu == 8) return launch_one<T, 8, 8>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-  if (cpw == 4 && bt.cu == 4) return launch_one<T, 4, 4>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  const int cpw = bt.tx * bt.ty / bt.nw;
+#define WFBP_ONE(C, U, N) \
+  if (cpw == C && bt.cu == U && bt.nw == N) return launch_one<T, C, U, N>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  WFBP_BP_SHAPES(WFBP_ONE)
+#undef WFBP_ONE
   return cudaErrorInvalidValue;
 }
 
@@ -504,14 +508,18 @@ cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* 
 // Shared-memory bytes of one launch configuration.
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes) {
   (void)elem_bytes;
-  return bp_smem_layout(bt, bt.tx * bt.ty / BT_CWARPS).total;
+  return bp_smem_layout(bt, bt.tx * bt.ty / bt.nw).total;
 }
 
 bool bp_tma_supported(const BPTile& bt) {
-  const int cpw = bt.tx * bt.ty / BT_CWARPS;
-  if (bt.tx * bt.ty != cpw * BT_CWARPS) return false;
-  return (cpw == 16 && (bt.cu == 4 || bt.cu == 8)) || (cpw == 8 && (bt.cu == 4 || bt.cu == 8)) ||
-         (cpw == 4 && bt.cu == 4);
+  if (bt.nw < 1) return false;
+  const int cpw = bt.tx * bt.ty / bt.nw;
+  if (bt.tx * bt.ty != cpw * bt.nw) return false;
+#define WFBP_SUP(C, U, N) \
+  if (cpw == C && bt.cu == U && bt.nw == N) return true;
+  WFBP_BP_SHAPES(WFBP_SUP)
+#undef WFBP_SUP
+  return false;
 }
 
 cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map) {
@@ -539,24 +547,19 @@ cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* v
   return launch_elem<float>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
 }
 
-cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, const BpScan* scans, const int4* items,
-                                         int n_items, unsigned* next, int* err, int smem_bytes, int grid,
-                                         cudaStream_t s) {
-#define WFBP_BATCH_CASE(T, C, U)                                                                         \
-  if (cpw == C && cu == U) return launch_batch_one<T, C, U>(scans, items, n_items, next, err, smem_bytes, grid, s);
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, const BpScan* scans,
+                                         const int4* items, int n_items, unsigned* next, int* err, int smem_bytes,
+                                         int grid, cudaStream_t s) {
+#define WFBP_B32(C, U, N) \
+  if (cpw == C && cu == U && nw == N) return launch_batch_one<uint32_t, C, U, N>(scans, items, n_items, next, err, smem_bytes, grid, s);
+#define WFBP_BF(C, U, N) \
+  if (cpw == C && cu == U && nw == N) return launch_batch_one<float, C, U, N>(scans, items, n_items, next, err, smem_bytes, grid, s);
   if (elem_half2) {
-    WFBP_BATCH_CASE(uint32_t, 16, 4)
-    WFBP_BATCH_CASE(uint32_t, 16, 8)
-    WFBP_BATCH_CASE(uint32_t, 8, 4)
-    WFBP_BATCH_CASE(uint32_t, 8, 8)
-    WFBP_BATCH_CASE(uint32_t, 4, 4)
+    WFBP_BP_SHAPES(WFBP_B32)
   } else {
-    WFBP_BATCH_CASE(float, 16, 4)
-    WFBP_BATCH_CASE(float, 16, 8)
-    WFBP_BATCH_CASE(float, 8, 4)
-    WFBP_BATCH_CASE(float, 8, 8)
-    WFBP_BATCH_CASE(float, 4, 4)
+    WFBP_BP_SHAPES(WFBP_BF)
   }
-#undef WFBP_BATCH_CASE
+#undef WFBP_B32
+#undef WFBP_BF
   return cudaErrorInvalidValue;
 }

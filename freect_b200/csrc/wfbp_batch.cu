@@ -105,7 +105,6 @@ std::vector<double> slab_view_counts(const wfbp_ctx* c, const std::vector<float>
 // sizes, tensor maps and the cost-sorted work list.
 int build_plan(wfbp_batch* b) {
   const int n = (int)b->ctx.size();
-  const int cpw = b->cfg.tile_x * b->cfg.tile_y / BT_CWARPS;
   std::vector<BpScan> hs(n);
   b->tiles.assign(n, BPTile{});
   int smem = 0;
@@ -117,7 +116,8 @@ int build_plan(wfbp_batch* b) {
   for (int i = 0; i < n; i++) {
     wfbp_ctx* c = b->ctx[i];
     BPTile bt;
-    if (!wfbp_detail::size_backprojection(c, b->cfg.tile_x, b->cfg.tile_y, b->cfg.cols_per_step, &bt))
+    if (!wfbp_detail::size_backprojection(c, b->cfg.tile_x, b->cfg.tile_y, b->cfg.cols_per_step,
+                                          b->cfg.consumer_warps, &bt))
       return bfail(b, WFBP_ERR_UNSUPPORTED, "backprojection configuration " + std::to_string(b->cfg.tile_x) + "x" +
                                                 std::to_string(b->cfg.tile_y) + "/" +
                                                 std::to_string(b->cfg.cols_per_step) + " does not fit scan " +
@@ -168,7 +168,6 @@ int build_plan(wfbp_batch* b) {
   int sms = 0;
   BCUDA(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
   b->grid = std::max(1, std::min(sms, b->n_items));
-  (void)cpw;
   return WFBP_OK;
 }
 
@@ -232,11 +231,12 @@ WFBP_API int wfbp_batch_create(wfbp_ctx* const* ctxs, int n, wfbp_batch** out) {
   // default configuration: the first candidate every scan fits
   int st = WFBP_ERR_UNSUPPORTED;
   for (int k = 0; k < wfbp_detail::n_bp_candidates() && st; k++) {
-    wfbp_detail::bp_candidate(k, &b->cfg.tile_x, &b->cfg.tile_y, &b->cfg.cols_per_step);
+    wfbp_detail::bp_candidate(k, &b->cfg.tile_x, &b->cfg.tile_y, &b->cfg.cols_per_step, &b->cfg.consumer_warps);
     bool fits = true;
     for (int i = 0; i < n && fits; i++) {
       BPTile bt;
-      fits = wfbp_detail::size_backprojection(b->ctx[i], b->cfg.tile_x, b->cfg.tile_y, b->cfg.cols_per_step, &bt);
+      fits = wfbp_detail::size_backprojection(b->ctx[i], b->cfg.tile_x, b->cfg.tile_y, b->cfg.cols_per_step,
+                                              b->cfg.consumer_warps, &bt);
     }
     if (fits) st = build_plan(b);
   }
@@ -259,11 +259,12 @@ WFBP_API int wfbp_batch_bp_configs(const wfbp_batch* b, wfbp_bp_config* out, int
   int k = 0;
   for (int c = 0; c < wfbp_detail::n_bp_candidates(); c++) {
     wfbp_bp_config cfg{};
-    wfbp_detail::bp_candidate(c, &cfg.tile_x, &cfg.tile_y, &cfg.cols_per_step);
+    wfbp_detail::bp_candidate(c, &cfg.tile_x, &cfg.tile_y, &cfg.cols_per_step, &cfg.consumer_warps);
     bool fits = true;
     for (size_t i = 0; i < b->ctx.size() && fits; i++) {
       BPTile bt;
-      fits = wfbp_detail::size_backprojection(b->ctx[i], cfg.tile_x, cfg.tile_y, cfg.cols_per_step, &bt);
+      fits = wfbp_detail::size_backprojection(b->ctx[i], cfg.tile_x, cfg.tile_y, cfg.cols_per_step, cfg.consumer_warps,
+                                              &bt);
     }
     if (!fits) continue;
     if (k < cap) out[k] = cfg;
@@ -284,7 +285,7 @@ WFBP_API int wfbp_batch_set_bp_config(wfbp_batch* b, const wfbp_bp_config* cfg) 
   DevGuard g(b->device);
   const wfbp_bp_config old = b->cfg;
   b->cfg = *cfg;
-  b->cfg.reserved = 0;
+  if (b->cfg.consumer_warps == 0) b->cfg.consumer_warps = BT_CWARPS;
   int st = build_plan(b);
   if (st) {
     const std::string msg = b->err;
@@ -328,8 +329,9 @@ WFBP_API int wfbp_batch_run(wfbp_batch* b, const float* const* raws, float* cons
     cudaError_t e = cudaSuccess;
     if (!st) e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned), s);
     if (!st && !e) {
-      const int cpw = b->cfg.tile_x * b->cfg.tile_y / BT_CWARPS;
+      const int cpw = b->cfg.tile_x * b->cfg.tile_y / b->cfg.consumer_warps;
       e = launch_backproject_tma_batch(b->precision == WFBP_PRECISION_MIXED ? 1 : 0, cpw, b->cfg.cols_per_step,
+                                       b->cfg.consumer_warps,
                                        b->d_scans, b->d_items, b->n_items, b->d_next, b->d_err, b->smem, b->grid, s);
     }
     for (int i = 0; i < n && !st && !e; i++) {

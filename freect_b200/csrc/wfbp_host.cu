@@ -294,12 +294,13 @@ void bp_reach(wfbp_ctx* ctx, const std::vector<float>& table) {
 }
 
 // Sizes one TMA backprojection configuration; false if it does not fit.
-bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out) {
+bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* out) {
   const double vx = ctx->rp.recon_fov / ctx->nx, vy = ctx->rp.recon_fov / ctx->ny;
   BPTile b;
   b.tx = tx;
   b.ty = ty;
   b.cu = cu;
+  b.nw = nw;
   const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
   b.W = (int)ceil(ext * ctx->gp.pixel_scale) + 5;
   b.W = std::max(4, std::min(b.W, 256));
@@ -316,13 +317,16 @@ bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out) {
   return true;
 }
 
-const int kBpCandidates[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 8, 4}, {16, 8, 8}, {8, 16, 4}, {8, 16, 8}, {8, 8, 4}};
+// (tile x, tile y, columns per pass, consumer warps)
+const int kBpCandidates[][4] = {{16, 16, 4, 16}, {16, 16, 8, 16}, {16, 8, 4, 16}, {16, 8, 8, 16}, {8, 16, 4, 16},
+                                {8, 16, 8, 16},  {8, 8, 4, 16},   {16, 10, 4, 20}, {16, 10, 8, 20}, {10, 16, 4, 20},
+                                {12, 8, 4, 24}};
 
 bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
   bp_reach(ctx, table);
   for (auto& c : kBpCandidates) {
     BPTile b;
-    if (size_bp_tile(ctx, c[0], c[1], c[2], &b)) {
+    if (size_bp_tile(ctx, c[0], c[1], c[2], c[3], &b)) {
       ctx->bpt = b;
       return true;
     }
@@ -744,12 +748,12 @@ WFBP_API int wfbp_bp_configs(const wfbp_ctx* ctx, wfbp_bp_config* out, int cap, 
   int k = 0;
   for (auto& c : kBpCandidates) {
     BPTile b;
-    if (!size_bp_tile(ctx, c[0], c[1], c[2], &b)) continue;
+    if (!size_bp_tile(ctx, c[0], c[1], c[2], c[3], &b)) continue;
     if (k < cap) {
       out[k].tile_x = c[0];
       out[k].tile_y = c[1];
       out[k].cols_per_step = c[2];
-      out[k].reserved = 0;
+      out[k].consumer_warps = c[3];
     }
     k++;
   }
@@ -764,7 +768,7 @@ WFBP_API int wfbp_get_bp_config(const wfbp_ctx* ctx, wfbp_bp_config* c) {
   c->tile_x = ctx->bpt.tx;
   c->tile_y = ctx->bpt.ty;
   c->cols_per_step = ctx->bpt.cu;
-  c->reserved = 0;
+  c->consumer_warps = ctx->bpt.nw;
   return WFBP_OK;
 }
 
@@ -772,9 +776,11 @@ WFBP_API int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* c) {
   if (!ctx || !c) return WFBP_ERR_INVALID_ARG;
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_set_bp_config: call wfbp_set_views first");
   BPTile b;
-  if (!size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, &b))
+  const int nw = c->consumer_warps ? c->consumer_warps : BT_CWARPS;
+  if (!size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, nw, &b))
     return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_set_bp_config: configuration " + std::to_string(c->tile_x) + "x" +
-                                               std::to_string(c->tile_y) + "/" + std::to_string(c->cols_per_step) +
+                                               std::to_string(c->tile_y) + "/" + std::to_string(c->cols_per_step) + "w" +
+                                               std::to_string(nw) +
                                                " is not supported for this geometry");
   ctx->bpt = b;
   ctx->bp_tma_ok = true;
@@ -1163,16 +1169,17 @@ BPParams backprojection_params(const wfbp_ctx* ctx) { return bp_params(ctx); }
 void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal) {
   stage_bytes(ctx, layout, reb, filt, scal);
 }
-bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out) {
-  return size_bp_tile(ctx, tx, ty, cu, out);
+bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* out) {
+  return size_bp_tile(ctx, tx, ty, cu, nw, out);
 }
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
   return do_filter(ctx, rebinned, filtered, scales, layout, stream);
 }
 int n_bp_candidates() { return (int)(sizeof(kBpCandidates) / sizeof(kBpCandidates[0])); }
-void bp_candidate(int i, int* tx, int* ty, int* cu) {
+void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw) {
   *tx = kBpCandidates[i][0];
   *ty = kBpCandidates[i][1];
   *cu = kBpCandidates[i][2];
+  *nw = kBpCandidates[i][3];
 }
 }  // namespace wfbp_detail

@@ -45,11 +45,12 @@ struct BPTile {
   float reach;       // slab-level half width of the table-position prefilter (mm)
   int smem_bytes;    // dynamic shared memory of the launch
   int cu;            // columns accumulated per step of the view loop (4 or 8)
+  int nw;            // consumer warps per CTA (16, 20 or 24; one more warp produces)
 };
 
 // Byte offsets of the TMA backprojection's shared-memory regions; the same
 // function sizes the launch on the host and carves the buffer on the device.
-constexpr int BT_CWARPS = 16;  // consumer warps of the TMA backprojection
+constexpr int BT_CWARPS = 16;  // default consumer warps of the TMA backprojection
 constexpr int BT_STAGES = 2;   // view-window ring depth
 struct BpSmem {
   unsigned slots, vinfo, vsv, geo, total;
@@ -67,7 +68,7 @@ __host__ __device__ inline BpSmem bp_smem_layout(const BPTile& bt, int cpw) {
   o += (unsigned)(BT_STAGES * bt.nv_max * 4);
   o = (o + 15u) & ~15u;
   L.geo = o;
-  o += (unsigned)(BT_CWARPS * bt.nv_max * (cpw / 2) * 48);  // column-pair geometry records
+  o += (unsigned)(bt.nw * bt.nv_max * (cpw / 2) * 48);  // column-pair geometry records
   L.total = o;
   return L;
 }
@@ -198,9 +199,9 @@ struct alignas(64) BpScan {
   const float* zslices;
 };
 cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map);
-cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, const BpScan* scans, const int4* items,
-                                         int n_items, unsigned* next, int* err, int smem_bytes, int grid,
-                                         cudaStream_t s);
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, const BpScan* scans,
+                                         const int4* items, int n_items, unsigned* next, int* err, int smem_bytes,
+                                         int grid, cudaStream_t s);
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);
 bool bp_tma_supported(const BPTile& bt);
 cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
@@ -229,8 +230,8 @@ namespace wfbp_detail {
 int set_error(wfbp_ctx* ctx, int code, const std::string& msg);
 BPParams backprojection_params(const wfbp_ctx* ctx);
 void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal);
-bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, BPTile* out);
+bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* out);
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream);
 int n_bp_candidates();
-void bp_candidate(int i, int* tx, int* ty, int* cu);
+void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw);
 }  // namespace wfbp_detail

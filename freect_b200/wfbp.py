@@ -286,7 +286,8 @@ class Context:
     def set_bp_config(self, config):
         if isinstance(config, (tuple, list)):
             c = T.BpConfig()
-            c.tile_x, c.tile_y, c.cols_per_step = config
+            c.tile_x, c.tile_y, c.cols_per_step = config[:3]
+            c.consumer_warps = config[3] if len(config) > 3 else 0
             config = c
         _check(self._lib.wfbp_set_bp_config(self._h, C.byref(config)), "wfbp_set_bp_config", self._h)
 
@@ -488,7 +489,8 @@ class Batch:
     def set_bp_config(self, config):
         if isinstance(config, (tuple, list)):
             c = T.BpConfig()
-            c.tile_x, c.tile_y, c.cols_per_step = config
+            c.tile_x, c.tile_y, c.cols_per_step = config[:3]
+            c.consumer_warps = config[3] if len(config) > 3 else 0
             config = c
         self._check(self._lib.wfbp_batch_set_bp_config(self._h, C.byref(config)), "wfbp_batch_set_bp_config")
 
