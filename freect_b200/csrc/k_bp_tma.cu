@@ -426,7 +426,7 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
   extern __shared__ __align__(128) uint8_t smem[];
   bp_init_barriers(smem, NW);
   bp_tile<T, CPW, CU, NW, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
-                                 blockIdx.z, count, err, smem, 0u);
+                                 bt.zb0 + blockIdx.z, count, err, smem, 0u);
 }
 
 // Persistent launch over the column tiles of several scans: each CTA takes
@@ -459,7 +459,10 @@ template <typename T, int CPW, int CU, int NW>
 cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                        unsigned long long* count, int* err, cudaStream_t s) {
-  dim3 grid((unsigned)((p.nx + bt.tx - 1) / bt.tx), (unsigned)((p.ny + bt.ty - 1) / bt.ty), (unsigned)((p.nz + 31) / 32));
+  const int nslab = (p.nz + 31) / 32;
+  if (bt.zb0 < 0 || bt.zb0 >= nslab || bt.nzb < 0 || bt.zb0 + bt.nzb > nslab) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((p.nx + bt.tx - 1) / bt.tx), (unsigned)((p.ny + bt.ty - 1) / bt.ty),
+            (unsigned)(bt.nzb ? bt.nzb : nslab - bt.zb0));
   constexpr int threads = (NW + 1) * 32;
   cudaError_t e;
   if (count) {

@@ -34,7 +34,8 @@ constexpr int TC_THREADS = 128;
 constexpr uint32_t TC_TMEM_COLS = 256;
 
 struct TcParams {
-  int M;          // rows of X (V * nrv)
+  int M;          // rows of one operand plane of X (V * nrv)
+  int mb, me;     // rows [mb, me) computed by this launch (mb a multiple of nrv)
   int nch;        // valid output channels
   int BN;         // N tile
   int kblocks;    // Kp / 64
@@ -117,7 +118,7 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   __shared__ float s_xchg[4][16];  // row 32w of each warp, for the pairs of the warp above
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * p.BN;
+  const int m0 = p.mb + blockIdx.x * TC_BM, n0 = blockIdx.y * p.BN;
 
   if (threadIdx.x == 0) {
     s_fail = 0;
@@ -194,12 +195,12 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     // row m of the tile: view v = m / nrv, row i = m % nrv (rows i >= nr are zero padding)
     const int m = m0 + warp * 32 + lane;
     const int v = m / o.nrv, i = m % o.nrv;
-    const bool row_ok = m < p.M && i < o.nr;
+    const bool row_ok = m < p.me && i < o.nr;
     float inv = 1.0f;
     if (o.mode == TC_OUT_F16_ROWS && row_ok) {
       inv = 1.0f / o.row_scale_in[m];
       if (blockIdx.y == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
-    } else if (o.mode == TC_OUT_PAIRS && m < p.M) {
+    } else if (o.mode == TC_OUT_PAIRS && m < p.me) {
       inv = 1.0f / o.view_scale[v];
     }
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
@@ -307,13 +308,17 @@ int tc_choose_bn(int nch) {
 
 // a_planes: bf16 [2][M][kp] (hi then lo); b_planes: bf16 [2][np][kp].
 cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
-                             const TcOutArgs& out, int* err, cudaStream_t s) {
+                             const TcOutArgs& out, int* err, cudaStream_t s, int mb, int me) {
+  if (me < 0) me = M;
+  if (mb < 0 || mb >= me || me > M || mb % (out.nrv > 0 ? out.nrv : 1)) return cudaErrorInvalidValue;
   if (bn < 16 || bn > 256 || bn % 16 || kp % TC_BK || np % bn) return cudaErrorInvalidValue;
-  CUtensorMap ma, mb;
-  if (!make_map(&ma, a_planes, (uint64_t)kp, 2ull * M, TC_BM)) return cudaErrorInvalidValue;
-  if (!make_map(&mb, b_planes, (uint64_t)kp, 2ull * np, (uint32_t)bn)) return cudaErrorInvalidValue;
+  CUtensorMap map_a, map_b;
+  if (!make_map(&map_a, a_planes, (uint64_t)kp, 2ull * M, TC_BM)) return cudaErrorInvalidValue;
+  if (!make_map(&map_b, b_planes, (uint64_t)kp, 2ull * np, (uint32_t)bn)) return cudaErrorInvalidValue;
   TcParams p;
   p.M = M;
+  p.mb = mb;
+  p.me = me;
   p.nch = nch;
   p.BN = bn;
   p.kblocks = kp / TC_BK;
@@ -322,7 +327,7 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
   size_t smem = tc_smem_bytes(bn);
   cudaError_t e = cudaFuncSetAttribute(k_toeplitz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((M + TC_BM - 1) / TC_BM), (unsigned)(np / bn));
-  k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(ma, mb, p, out, err);
+  dim3 grid((unsigned)((me - mb + TC_BM - 1) / TC_BM), (unsigned)(np / bn));
+  k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(map_a, map_b, p, out, err);
   return cudaGetLastError();
 }

@@ -58,7 +58,7 @@ constexpr int REB_QUADS = 64;
 
 __global__ void __launch_bounds__(REB_ROWS * REB_QUADS)
 k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float* __restrict__ beta_t,
-            const float* __restrict__ bidx_t, RebinParams p) {
+            const float* __restrict__ bidx_t, RebinParams p, int vb, int ve) {
   __shared__ float s_beta[REB_QUADS * 4], s_bidx[REB_QUADS * 4];
   const int tq = threadIdx.x % REB_QUADS, tr = threadIdx.x / REB_QUADS;
   const int c_base = blockIdx.y * REB_QUADS * 4;
@@ -68,8 +68,8 @@ k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float*
     s_bidx[t] = c < p.nch ? bidx_t[c] : __int_as_float(0x7fc00000);
   }
   __syncthreads();
-  const long row = (long)blockIdx.x * REB_ROWS + tr;
-  if (row >= (long)p.V * p.nr) return;
+  const long row = (long)vb * p.nr + (long)blockIdx.x * REB_ROWS + tr;
+  if (row >= (long)ve * p.nr) return;
   const int v = (int)(row / p.nr), i = (int)(row % p.nr);
   const int c = c_base + tq * 4;
   float* o = out + (size_t)row * p.nch;
@@ -87,10 +87,12 @@ k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float*
 }
 
 cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, const float* d_bidx,
-                             const RebinParams& p, cudaStream_t s) {
-  long rows = (long)p.V * p.nr;
+                             const RebinParams& p, cudaStream_t s, int vb, int ve) {
+  if (ve < 0) ve = p.V;
+  if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
+  long rows = (long)(ve - vb) * p.nr;
   dim3 grid((unsigned)((rows + REB_ROWS - 1) / REB_ROWS), (unsigned)((p.nch + REB_QUADS * 4 - 1) / (REB_QUADS * 4)));
-  k_rebin_f32<<<grid, REB_ROWS * REB_QUADS, 0, s>>>(raw, out, d_beta, d_bidx, p);
+  k_rebin_f32<<<grid, REB_ROWS * REB_QUADS, 0, s>>>(raw, out, d_beta, d_bidx, p, vb, ve);
   return cudaGetLastError();
 }
 
@@ -258,9 +260,9 @@ constexpr int RS_THREADS = 256;
 __global__ void __launch_bounds__(RS_THREADS)
 k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
               float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
-              const float* __restrict__ bidx_t, RebinParams p, int kp, int nrv, float taps_l1) {
+              const float* __restrict__ bidx_t, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
   extern __shared__ float s_rowmax[];  // [nrv]
-  const int v = blockIdx.x;
+  const int v = vb + blockIdx.x;
   for (int i = threadIdx.x; i < nrv; i += RS_THREADS) s_rowmax[i] = 0.0f;
   __syncthreads();
   const int quads = kp / 4;
@@ -301,11 +303,13 @@ k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, _
 
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
                                const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
-                               float taps_l1, cudaStream_t s) {
+                               float taps_l1, cudaStream_t s, int vb, int ve) {
+  if (ve < 0) ve = p.V;
+  if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
   const size_t rows = (size_t)p.V * nrv;
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
   __nv_bfloat16* lo = hi + rows * kp;
-  k_rebin_split<<<(unsigned)p.V, RS_THREADS, sizeof(float) * nrv, s>>>(raw, hi, lo, row_scale, view_scale, d_beta,
-                                                                       d_bidx, p, kp, nrv, taps_l1);
+  k_rebin_split<<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(raw, hi, lo, row_scale, view_scale,
+                                                                             d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
   return cudaGetLastError();
 }

@@ -178,6 +178,10 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_radj_idx);
   free_dev(ctx->d_radj_w);
   free_dev(ctx->d_tg_partial);
+  for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
+  ctx->ev_copy.clear();
+  if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
+  ctx->s_copy = nullptr;
   free_dev(ctx->s_rebinned);
   free_dev(ctx->s_filtered);
   free_dev(ctx->s_scales);
@@ -301,6 +305,8 @@ bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* o
   b.ty = ty;
   b.cu = cu;
   b.nw = nw;
+  b.zb0 = 0;
+  b.nzb = 0;
   const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
   b.W = (int)ceil(ext * ctx->gp.pixel_scale) + 5;
   b.W = std::max(4, std::min(b.W, 256));
@@ -843,26 +849,36 @@ RebinParams rebin_params(const wfbp_ctx* ctx) {
 }
 }  // namespace
 
-WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream) {
-  if (!ctx) return WFBP_ERR_INVALID_ARG;
-  if (!raw || !rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin: null buffer");
-  DeviceGuard g(ctx->device);
+namespace {
+// Rebin of views [vb, ve) (all: 0, V).
+int do_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, int vb, int ve, void* stream) {
   const RebinParams p = rebin_params(ctx);
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
     float *row_sc, *view_sc;
     mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
     CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, row_sc, view_sc, ctx->d_chan_beta, ctx->d_chan_bidx, p,
-                                     ctx->tc_kp, ctx->nrv, ctx->taps_l1, (cudaStream_t)stream));
+                                     ctx->tc_kp, ctx->nrv, ctx->taps_l1, (cudaStream_t)stream, vb, ve));
   } else {
-    CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream));
+    CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream,
+                                   vb, ve));
   }
   return WFBP_OK;
+}
+}  // namespace
+
+WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream) {
+  if (!ctx) return WFBP_ERR_INVALID_ARG;
+  if (!raw || !rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin: null buffer");
+  DeviceGuard g(ctx->device);
+  return do_rebin(ctx, raw, rebinned, 0, ctx->V, stream);
 }
 
 namespace {
 
-int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
+int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream, int vb = 0,
+              int ve = -1) {
   const cudaStream_t s = (cudaStream_t)stream;
+  if (ve < 0) ve = ctx->V;
   const bool bpl = layout == WFBP_LAYOUT_BACKPROJECTION;
   if (bpl && !ctx->bp_tma_ok)
     return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_filter: no backprojection-layout launch fits this geometry");
@@ -880,22 +896,24 @@ int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales
     if (bpl) {
       o.mode = TC_OUT_PAIRS;
       o.pairs = static_cast<uint32_t*>(filtered);
-      CUDA_TRY(ctx, cudaMemcpyAsync(scales, view_sc, sizeof(float) * ctx->V, cudaMemcpyDeviceToDevice, s));
+      CUDA_TRY(ctx, cudaMemcpyAsync(scales + vb, view_sc + vb, sizeof(float) * (ve - vb), cudaMemcpyDeviceToDevice, s));
     } else {
       o.mode = TC_OUT_F16_ROWS;
       o.y16 = static_cast<__half*>(filtered);
       o.row_scale_out = scales;
     }
     CUDA_TRY(ctx, launch_filter_tc(rebinned, ctx->d_bplanes, ctx->V * ctx->nrv, ctx->nch, ctx->tc_kp, ctx->tc_np,
-                                   ctx->tc_bn, o, ctx->d_err, s));
+                                   ctx->tc_bn, o, ctx->d_err, s, vb * ctx->nrv, ve * ctx->nrv));
     return WFBP_OK;
   }
+  const float* x = (const float*)rebinned + (size_t)vb * ctx->nr * ctx->nch;
+  const long rows = (long)(ve - vb) * ctx->nr;
   if (bpl)
-    CUDA_TRY(ctx, launch_filter_f32_tr((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
+    CUDA_TRY(ctx, launch_filter_f32_tr(x, (float*)filtered + (size_t)vb * ctx->nch * ctx->bpt.nrp, ctx->d_taps, rows,
                                        ctx->nch, ctx->nr, ctx->bpt.nrp, s));
   else
-    CUDA_TRY(ctx, launch_filter_f32((const float*)rebinned, (float*)filtered, ctx->d_taps, (long)ctx->V * ctx->nr,
-                                    ctx->nch, s));
+    CUDA_TRY(ctx, launch_filter_f32(x, (float*)filtered + (size_t)vb * ctx->nr * ctx->nch, ctx->d_taps, rows, ctx->nch,
+                                    s));
   return WFBP_OK;
 }
 
@@ -1046,6 +1064,10 @@ WFBP_API int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_
   const size_t need = (size_t)taps_grad_blocks(p) * n;
   if (need > ctx->tg_partial_n) {
     free_dev(ctx->d_tg_partial);
+  for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
+  ctx->ev_copy.clear();
+  if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
+  ctx->s_copy = nullptr;
     CUDA_TRY(ctx, cudaMalloc(&ctx->d_tg_partial, sizeof(float) * need));
     ctx->tg_partial_n = need;
   }
@@ -1128,15 +1150,113 @@ WFBP_API int wfbp_run_timed(wfbp_ctx* ctx, const float* raw, float* vol, void* s
   return WFBP_OK;
 }
 
+namespace {
+// Views the rebin reads either side of a view (fan half-angle over the angular
+// step, in views, plus the interpolation).
+int rebin_reach_views(const wfbp_ctx* ctx) {
+  const CTGeometry& cg = ctx->cg_read;
+  const double sdd = cg.distance_source_to_detector, dcol = cg.detector_pixel_size_col, c0 = cg.detector_central_col;
+  double beta = 0.0;
+  for (double c : {0.0, (double)cg.num_detector_cols - 1.0})
+    beta = std::max(beta, fabs(asin(std::max(-1.0, std::min(1.0, (c - c0) * dcol / sdd)))));
+  const int reach_readings = (int)ceil(beta * cg.projections_per_rotation / (2 * M_PI)) + 2;
+  return reach_readings / ctx->G + 2;
+}
+
+// wfbp_run_host as a pipeline over chunks of readings: the host-to-device
+// copy of chunk c+1 (own stream) overlaps the rebin and filter of chunk c and
+// the backprojection of every 32-slice slab whose views are all filtered
+// (the slab's table-position reach, the z cull of cuda_kernels.cuh:232); the
+// last slabs, the thickening and the copy back follow. Same kernels, same
+// per-voxel sums: the volume equals wfbp_run's.
+int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cudaStream_t s) {
+  wfbp_dims d;
+  wfbp_query(ctx, &d);
+  int st = ensure_scratch(ctx);
+  if (st) return st;
+  const int lay = WFBP_LAYOUT_BACKPROJECTION;
+  constexpr int kChunks = 8;
+  if (!ctx->s_copy) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
+  if (ctx->ev_copy.empty()) {
+    ctx->ev_copy.resize(kChunks + 1);
+    for (auto& e : ctx->ev_copy) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const int V = ctx->V, G = ctx->G;
+  const int cv = (V + kChunks - 1) / kChunks;
+  const size_t frame = (size_t)ctx->raw_rows * ctx->raw_ch;
+  const int reach = rebin_reach_views(ctx);
+  // order the copies after the caller's earlier work on its stream
+  CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[kChunks], s));
+  CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_copy, ctx->ev_copy[kChunks], 0));
+  const int nchunk = (V + cv - 1) / cv;
+  for (int c = 0; c < nchunk; c++) {
+    const size_t r0 = (size_t)c * cv * G, r1 = (size_t)std::min(V, (c + 1) * cv) * G;
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->s_raw + r0 * frame, raw_host + r0 * frame, sizeof(float) * (r1 - r0) * frame,
+                                  cudaMemcpyHostToDevice, ctx->s_copy));
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[c], ctx->s_copy));
+  }
+  // last view each slab needs: views j < K P/2 within the slab's reach in z
+  const int nslab = (ctx->nz + 31) / 32;
+  std::vector<int> need(nslab, -1);
+  const int used = ctx->K * ctx->P2;
+  for (int sl = 0; sl < nslab; sl++) {
+    float zmn = 3e38f, zmx = -3e38f;
+    for (int i = sl * 32; i < std::min(ctx->nz, sl * 32 + 32); i++) {
+      zmn = std::min(zmn, ctx->z_native[i]);
+      zmx = std::max(zmx, ctx->z_native[i]);
+    }
+    for (int j = 0; j < used; j++)
+      if (!(ctx->view_table[j] < zmn - ctx->bp_reach || ctx->view_table[j] > zmx + ctx->bp_reach)) need[sl] = j;
+  }
+  std::vector<char> done(nslab, 0);
+  const BPParams p = bp_params(ctx);
+  const bool mixed = ctx->ext.precision == WFBP_PRECISION_MIXED;
+  auto launch_ready = [&](int filtered_upto) -> int {
+    for (int sl = 0; sl < nslab;) {
+      if (done[sl] || need[sl] >= filtered_upto) {
+        sl++;
+        continue;
+      }
+      int e = sl;  // a run of ready slabs in one launch
+      while (e < nslab && !done[e] && need[e] < filtered_upto) e++;
+      BPTile bt = ctx->bpt;
+      bt.zb0 = sl;
+      bt.nzb = e - sl;
+      CUDA_TRY(ctx, launch_backproject_tma(ctx->s_filtered, mixed ? 1 : 0, ctx->s_scales, ctx->s_vol_native,
+                                           ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, bt, nullptr,
+                                           ctx->d_err, s));
+      for (int k = sl; k < e; k++) done[k] = 1;
+      sl = e;
+    }
+    return WFBP_OK;
+  };
+  for (int c = 0; c < nchunk; c++) {
+    const int vb = c * cv, ve = std::min(V, (c + 1) * cv);
+    const int last = std::min(nchunk - 1, (std::min(V, ve + reach) - 1) / cv);
+    CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->ev_copy[last], 0));
+    if ((st = do_rebin(ctx, ctx->s_raw, ctx->s_rebinned, vb, ve, s))) return st;
+    if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, s, vb, ve))) return st;
+    if ((st = launch_ready(ve))) return st;
+  }
+  if ((st = launch_ready(V + 1))) return st;
+  if ((st = wfbp_thicken(ctx, ctx->s_vol_native, ctx->s_vol, s))) return st;
+  CUDA_TRY(ctx, cudaMemcpyAsync(vol_host, ctx->s_vol, d.volume_bytes, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  return wfbp_check_device_status(ctx);
+}
+}  // namespace
+
 WFBP_API int wfbp_run_host(wfbp_ctx* ctx, const float* raw_host, float* vol_host, void* stream) {
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (!raw_host || !vol_host) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_run_host: null buffer");
+  if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_run_host: wfbp_set_views not called");
   DeviceGuard g(ctx->device);
   wfbp_dims d;
   wfbp_query(ctx, &d);
   if (!ctx->s_raw) CUDA_TRY(ctx, cudaMalloc(&ctx->s_raw, d.raw_bytes));
   if (!ctx->s_vol) CUDA_TRY(ctx, cudaMalloc(&ctx->s_vol, d.volume_bytes));
   cudaStream_t s = (cudaStream_t)stream;
+  if (run_layout(ctx) == WFBP_LAYOUT_BACKPROJECTION) return run_host_pipelined(ctx, raw_host, vol_host, s);
   CUDA_TRY(ctx, cudaMemcpyAsync(ctx->s_raw, raw_host, d.raw_bytes, cudaMemcpyHostToDevice, s));
   int st = wfbp_run(ctx, ctx->s_raw, ctx->s_vol, stream);
   if (st) return st;

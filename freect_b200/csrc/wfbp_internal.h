@@ -46,6 +46,7 @@ struct BPTile {
   int smem_bytes;    // dynamic shared memory of the launch
   int cu;            // columns accumulated per step of the view loop (4 or 8)
   int nw;            // consumer warps per CTA (16, 20 or 24; one more warp produces)
+  int zb0, nzb;      // 32-slice slabs [zb0, zb0 + nzb) of this launch (nzb 0: all)
 };
 
 // Byte offsets of the TMA backprojection's shared-memory regions; the same
@@ -149,6 +150,8 @@ struct wfbp_ctx {
   float* s_vol_native = nullptr;
   float* s_raw = nullptr;
   float* s_vol = nullptr;
+  cudaStream_t s_copy = nullptr;    // wfbp_run_host: host-to-device copies of the reading chunks
+  std::vector<cudaEvent_t> ev_copy; // one per chunk, plus the caller-stream fence
 
   bool views_set = false;
   std::string err;
@@ -159,8 +162,10 @@ cudaError_t launch_view_tables(const float* d_tube, const float* d_table, float2
                                cudaStream_t s);
 cudaError_t launch_rebin_tables(float* d_beta, float* d_bidx, int nch, float c0, float dcol, float sdd,
                                 cudaStream_t s);
+// Stage launchers take an optional range: views [vb, ve) for the rebins,
+// rows [mb, me) for the tensor-core filter (-1: all).
 cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, const float* d_bidx,
-                             const RebinParams& p, cudaStream_t s);
+                             const RebinParams& p, cudaStream_t s, int vb = 0, int ve = -1);
 cudaError_t launch_filter_f32(const float* x, float* y, const float* d_taps, long rows, int nch, cudaStream_t s);
 cudaError_t launch_backproject_f32(const float* D, float* vol, const float2* sc, const float* vz,
                                    const float* zs, const BPParams& p, unsigned long long* count,
@@ -170,7 +175,7 @@ cudaError_t launch_backproject_f16(const __half* D, const float* scales, float* 
                                    cudaStream_t s);
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
                                const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
-                               float taps_l1, cudaStream_t s);
+                               float taps_l1, cudaStream_t s, int vb = 0, int ve = -1);
 // Output modes of the tensor-core filter epilogue.
 enum TcOut { TC_OUT_F32 = 0, TC_OUT_F16_ROWS = 1, TC_OUT_PAIRS = 2 };
 struct TcOutArgs {
@@ -184,7 +189,7 @@ struct TcOutArgs {
   const float* view_scale;      // [V]
 };
 cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
-                             const TcOutArgs& out, int* err, cudaStream_t s);
+                             const TcOutArgs& out, int* err, cudaStream_t s, int mb = 0, int me = -1);
 cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps, long rows, int nch, int nr, int nrp,
                                  cudaStream_t s);
 // One scan of a persistent (batched) backprojection launch, in device memory.

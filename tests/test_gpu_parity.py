@@ -178,14 +178,28 @@ def test_synth_gpu_matches_cpu(orc):
     assert np.allclose(out.cpu().numpy(), ref, rtol=1e-6, atol=1e-6)
 
 
-def test_run_host_matches_run(orc, tiny):
-    spec, raw = tiny
-    ctx, cg, gp = make_ctx(spec, tex_weights=1)
+@pytest.mark.parametrize("precision", [T.PRECISION_FP32, T.PRECISION_MIXED])
+@pytest.mark.parametrize("which", ["tiny", "small"])
+def test_run_host_matches_run(orc, tiny, which, precision):
+    # wfbp_run_host pipelines the copies of reading chunks with the rebin,
+    # filter and the backprojection of the slabs whose views are ready; the
+    # volume must equal wfbp_run's bit for bit
+    if which == "tiny":
+        spec, raw = tiny
+    else:
+        spec = scans.small(seed=9)
+        spec.nx = spec.ny = 64
+        spec.n_slices = 40  # several 32-slice slabs
+        raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    ctx, cg, gp = make_ctx(spec, tex_weights=1 if precision == T.PRECISION_FP32 else 0, precision=precision)
+    assert ctx.dims.n_slices_native > 32 or which == "tiny"
     vol = ctx.alloc("volume")
     ctx.run(dev(raw), vol)
     torch.cuda.synchronize()
-    host = ctx.run_host(np.ascontiguousarray(raw))
-    assert np.array_equal(host, vol.cpu().numpy())
+    pinned = torch.from_numpy(np.ascontiguousarray(raw)).pin_memory()
+    for _ in range(2):
+        host = ctx.run_host(pinned)
+        assert np.array_equal(host, vol.cpu().numpy(), equal_nan=True)
 
 
 def test_state_and_argument_errors(tiny):
