@@ -108,7 +108,8 @@ class Ext(C.Structure):
         ("tex_weights", C.c_int),
         ("bp_slab", C.c_int),
         ("filtered_layout", C.c_int),
-        ("reserved", C.c_int * 6),
+        ("adjoint_scale_table", C.c_int),
+        ("reserved", C.c_int * 5),
     ]
 
 
@@ -137,10 +138,11 @@ class Dims(C.Structure):
 
 class BpConfig(C.Structure):
     """wfbp_bp_config"""
-    _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("cols_per_step", C.c_int), ("consumer_warps", C.c_int)]
+    _fields_ = [("tile_x", C.c_int), ("tile_y", C.c_int), ("cols_per_step", C.c_int), ("consumer_warps", C.c_int),
+                ("slab", C.c_int)]
 
     def key(self):
-        return (self.tile_x, self.tile_y, self.cols_per_step, self.consumer_warps)
+        return (self.tile_x, self.tile_y, self.cols_per_step, self.consumer_warps, self.slab)
 
 
 class Ellipsoid(C.Structure):

@@ -25,14 +25,14 @@ def signature(ctx):
     """Key of a tuning result: what the backprojection's cost depends on."""
     d = ctx.dims
     cg, gp = ctx.geometry()
-    return "v2|V%d|nr%d|nch%d|P%d|%dx%dx%d|prec%d|fov%.3f|ps%.5f|zrot%.4f" % (
+    return "v3|V%d|nr%d|nch%d|P%d|%dx%dx%d|prec%d|fov%.3f|ps%.5f|zrot%.4f" % (
         d.n_views, d.n_rows, d.n_channels, int(cg.projections_per_rotation), d.nx, d.ny, d.n_slices_native,
         d.precision, ctx.rp.recon_fov, gp.pixel_scale, cg.z_rot)
 
 
 def config_name(key):
-    """'16x16/4w16': column tile, columns per pass, consumer warps."""
-    return "%dx%d/%dw%d" % tuple(key)
+    """'16x16/4w16s32': column tile, columns per pass, consumer warps, slab slices."""
+    return "%dx%d/%dw%ds%d" % tuple(key)
 
 
 def _load(path):

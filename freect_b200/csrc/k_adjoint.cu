@@ -73,9 +73,60 @@ __device__ __forceinline__ float view_weight(const BPParams& p, const ViewGeo& g
   return ok ? q_weight_fwd(qh) : 0.0f;
 }
 
+// Scaled voxel gradients G[t][s][y][x] = g_vol * dtheta / sum_k W_k for each
+// half-turn angle t (0 where no half turn contributes, as the forward's NaN
+// voxel has no gradient): one thread per (x, y) column and ZS slices, the
+// weights summed in the forward's order. With this table the gather below
+// needs one load instead of the other half turns' geometry.
+constexpr int AN_ZS = 8, AN_TX = 16, AN_TY = 8;
+
+__global__ void __launch_bounds__(AN_TX * AN_TY)
+k_bp_adjoint_scale(const float* __restrict__ gvol, float* __restrict__ G, const float2* __restrict__ view_sc,
+                   const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p) {
+  const int ix = blockIdx.x * AN_TX + (threadIdx.x % AN_TX);
+  const int iy = blockIdx.y * AN_TY + (threadIdx.x / AN_TX);
+  const int s0 = blockIdx.z * AN_ZS;
+  if (ix >= p.nx || iy >= p.ny) return;
+  const float x = xcoord(p, ix), y = ycoord(p, iy);
+  const size_t plane = (size_t)p.nx * p.ny, vox = (size_t)iy * p.nx + ix;
+  const bool active = !(x * x + y * y > p.fov_half2);
+  float z[AN_ZS], gv[AN_ZS];
+#pragma unroll
+  for (int i = 0; i < AN_ZS; i++) {
+    const int sl = s0 + i;
+    z[i] = sl < p.nz ? __ldg(zslices + sl) : 0.0f;
+    gv[i] = sl < p.nz ? __ldg(gvol + (size_t)sl * plane + vox) : 0.0f;
+  }
+  for (int t = 0; t < p.P2; t++) {
+    float aw[AN_ZS];
+#pragma unroll
+    for (int i = 0; i < AN_ZS; i++) aw[i] = 0.0f;
+    if (active) {
+      for (int k = 0; k < p.K; k++) {
+        const int j = t + k * p.P2;
+        const float zt = __ldg(view_z + j);
+        const ViewGeo g = view_geo(p, x, y, __ldg(view_sc + j), zt);
+        if (!g.valid_p) continue;
+#pragma unroll
+        for (int i = 0; i < AN_ZS; i++) {
+          float qi;
+          aw[i] += view_weight(p, g, z[i], &qi);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < AN_ZS; i++) {
+      const int sl = s0 + i;
+      if (sl < p.nz)
+        G[((size_t)t * p.nz + sl) * plane + vox] = aw[i] > 0.0f ? gv[i] * (p.dtheta * (1.0f / aw[i])) : 0.0f;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(AD_CH)
-k_bp_adjoint(const float* __restrict__ gvol, float* __restrict__ gD, const float2* __restrict__ view_sc,
-             const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, float z0, float dzs) {
+k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float* __restrict__ gD,
+             const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
+             BPParams p, float z0, float dzs) {
   extern __shared__ float col[];  // [nr][AD_CH], thread c owns column c
   const int j = blockIdx.y;
   const int cl = threadIdx.x;
@@ -142,23 +193,30 @@ k_bp_adjoint(const float* __restrict__ gvol, float* __restrict__ gD, const float
           float q_idx;
           const float Wj = view_weight(p, g, z, &q_idx);
           if (Wj == 0.0f) continue;
-          const float gv = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix);
-          if (gv == 0.0f) continue;
-          // sum of the weights of all half turns, in the forward's order
-          float aw = 0.0f;
-          for (int k = 0; k < p.K; k++) {
-            const int jj = t + k * p.P2;
-            if (jj == j) {
-              aw += Wj;
-              continue;
+          float scaled;  // g_vol * dtheta / sum_k W_k (cuda_kernels.cuh:283)
+          if (G) {
+            scaled = __ldg(G + (((size_t)t * p.nz + s) * p.ny + iy) * p.nx + ix);
+            if (scaled == 0.0f) continue;
+          } else {
+            const float gv = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix);
+            if (gv == 0.0f) continue;
+            // sum of the weights of all half turns, in the forward's order
+            float aw = 0.0f;
+            for (int k = 0; k < p.K; k++) {
+              const int jj = t + k * p.P2;
+              if (jj == j) {
+                aw += Wj;
+                continue;
+              }
+              const float ztk = __ldg(view_z + jj);
+              if (!(fabsf(z - ztk) <= p.z_rot)) continue;
+              const ViewGeo gk = view_geo(p, x, y, __ldg(view_sc + jj), ztk);
+              float qk;
+              aw += view_weight(p, gk, z, &qk);
             }
-            const float ztk = __ldg(view_z + jj);
-            if (!(fabsf(z - ztk) <= p.z_rot)) continue;
-            const ViewGeo gk = view_geo(p, x, y, __ldg(view_sc + jj), ztk);
-            float qk;
-            aw += view_weight(p, gk, z, &qk);
+            scaled = gv * (p.dtheta * (1.0f / aw));
           }
-          const float cval = gv * (p.dtheta * (1.0f / aw)) * Wj * hp;  // cuda_kernels.cuh:283
+          const float cval = scaled * Wj * hp;
           const float qf = floorf(q_idx), wq = q_idx - qf;
           const int r = min(max((int)qf, 0), p.nr - 2);
           col[r * AD_CH + cl] += cval * (1.0f - wq);
@@ -336,14 +394,21 @@ __global__ void k_taps_reduce(const float* __restrict__ partial, int nblk, int n
 }  // namespace
 
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
-                              const BPParams& p, float z0, float dzs, cudaStream_t s) {
+                              const BPParams& p, float z0, float dzs, float* scale_table, cudaStream_t s) {
+  if (scale_table) {
+    dim3 g((unsigned)((p.nx + AN_TX - 1) / AN_TX), (unsigned)((p.ny + AN_TY - 1) / AN_TY),
+           (unsigned)((p.nz + AN_ZS - 1) / AN_ZS));
+    k_bp_adjoint_scale<<<g, AN_TX * AN_TY, 0, s>>>(gvol, scale_table, sc, vz, zs, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   dim3 grid((unsigned)((p.nch + AD_CH - 1) / AD_CH), (unsigned)p.V);
   const size_t smem = (size_t)p.nr * AD_CH * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_bp_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_bp_adjoint<<<grid, AD_CH, smem, s>>>(gvol, gD, sc, vz, zs, p, z0, dzs);
+  k_bp_adjoint<<<grid, AD_CH, smem, s>>>(gvol, scale_table, gD, sc, vz, zs, p, z0, dzs);
   return cudaGetLastError();
 }
 

@@ -105,7 +105,7 @@ __device__ __forceinline__ void bp_init_barriers(uint8_t* smem, int nw) {
 // outside the reconstruction FOV (whose voxels are written as 0, the value
 // the reference leaves there). A bounded wait that gave up sets the failure
 // word (the CTA must stop).
-template <typename T, int CPW, int CU, int NW, bool COUNT>
+template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
 __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __restrict__ view_scale,
                                         float* __restrict__ vol, const float2* __restrict__ view_sc,
                                         const float* __restrict__ view_z, const float* __restrict__ zslices,
@@ -114,7 +114,12 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
                                         uint32_t ring) {
   constexpr bool HALF = !std::is_same<T, float>::value;
   constexpr int NPW = CPW / 2;  // column pairs per warp
-  static_assert(CU % 2 == 0 && CPW % CU == 0, "columns per step must be even and divide the columns per warp");
+  // SL = 32: the warp's 32 lanes are 32 slices of each of its CPW columns.
+  // SL = 16: lanes 0-15 and 16-31 are 16 slices of two column groups of
+  // CPW / 2 columns each (a 16-slice slab: fewer lanes outside a view's cone).
+  constexpr int NG = 32 / SL, CPG = CPW / NG;  // column groups per warp, columns per group
+  static_assert(SL == 32 || SL == 16, "slab of 32 or 16 slices");
+  static_assert(CU % 2 == 0 && CPG % CU == 0, "columns per step must be even and divide the columns per group");
   const BpSmem L = bp_smem_layout(bt, CPW);
   uint8_t* slots = smem + L.slots;                            // [STAGES][nv_max][slot_bytes]
   int2* vinfo = reinterpret_cast<int2*>(smem + L.vinfo);      // [STAGES][nv_max] (view, first channel)
@@ -127,14 +132,15 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int ix0 = bx * bt.tx, iy0 = by * bt.ty;
-  const int s0 = bz * 32;
+  const int s0 = bz * SL;
+  const int grp = lane / SL;  // column group of this lane
 
-  // slab z range (all warps compute the same values)
-  const int my_s = s0 + lane;
+  // slab z range (all warps and groups compute the same values)
+  const int my_s = s0 + lane % SL;
   const float zl = my_s < p.nz ? zslices[my_s] : __int_as_float(0x7fc00000);
   float zmn = my_s < p.nz ? zl : 3.0e38f, zmx = my_s < p.nz ? zl : -3.0e38f;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
+  for (int o = SL / 2; o > 0; o >>= 1) {
     zmn = fminf(zmn, __shfl_xor_sync(0xffffffffu, zmn, o));
     zmx = fmaxf(zmx, __shfl_xor_sync(0xffffffffu, zmx, o));
   }
@@ -153,8 +159,8 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
     if (xn * xn + yn * yn > p.fov_half2 * 1.0001f + 1e-3f) {
       if (warp < NW && my_s < p.nz) {
         const size_t plane = (size_t)p.nx * p.ny;
-        for (int c = 0; c < CPW; c++) {
-          const int tt = warp * CPW + c;
+        for (int c = 0; c < CPG; c++) {
+          const int tt = warp * CPW + grp * CPG + c;
           const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
           if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = 0.0f;
         }
@@ -249,9 +255,9 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
   }
 
   // ---------------- consumers ----------------
-  float vacc[CPW];
+  float vacc[CPG];
 #pragma unroll
-  for (int c = 0; c < CPW; c++) vacc[c] = 0.0f;
+  for (int c = 0; c < CPG; c++) vacc[c] = 0.0f;
   unsigned long long cnt = 0;
   const float k1 = 2.5f / p.hn;
   GeoP* wgeo = geo + (size_t)warp * bt.nv_max * NPW;
@@ -316,9 +322,13 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       }
     }
     __syncwarp();
+    const unsigned my_cols = (active_mask >> (grp * CPG)) & ((1u << CPG) - 1u);  // this group's columns
 #pragma unroll
-    for (int c0 = 0; c0 < CPW; c0 += CU) {
-      if (!((active_mask >> c0) & ((1u << CU) - 1u))) continue;
+    for (int c0 = 0; c0 < CPG; c0 += CU) {
+      unsigned any = 0u;  // warp-uniform: some group has an active column in this step
+#pragma unroll
+      for (int g2 = 0; g2 < NG; g2++) any |= (active_mask >> (g2 * CPG + c0)) & ((1u << CU) - 1u);
+      if (!any) continue;
       float2 ag[CU / 2], aw[CU / 2];
 #pragma unroll
       for (int u2 = 0; u2 < CU / 2; u2++) {
@@ -331,7 +341,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
           const float sv = vsv[s * bt.nv_max + v];
           sv2 = make_float2(sv, sv);
         }
-        const GeoP* gpv = wgeo + v * NPW + c0 / 2;
+        const GeoP* gpv = wgeo + v * NPW + (grp * CPG + c0) / 2;
 #pragma unroll
         for (int u2 = 0; u2 < CU / 2; u2++) {
           const GeoP g = gpv[u2];
@@ -389,8 +399,8 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       for (int u2 = 0; u2 < CU / 2; u2++) {
         const int c = c0 + 2 * u2;
         // cuda_kernels.cuh:283
-        if ((active_mask >> c) & 1u) vacc[c] += p.dtheta * (1.0f / aw[u2].x) * ag[u2].x;
-        if ((active_mask >> (c + 1)) & 1u) vacc[c + 1] += p.dtheta * (1.0f / aw[u2].y) * ag[u2].y;
+        if ((my_cols >> c) & 1u) vacc[c] += p.dtheta * (1.0f / aw[u2].x) * ag[u2].x;
+        if ((my_cols >> (c + 1)) & 1u) vacc[c + 1] += p.dtheta * (1.0f / aw[u2].y) * ag[u2].y;
       }
     }
     __syncwarp();
@@ -401,8 +411,8 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
   if (my_s < p.nz) {
     const size_t plane = (size_t)p.nx * p.ny;
 #pragma unroll
-    for (int c = 0; c < CPW; c++) {
-      const int tt = warp * CPW + c;
+    for (int c = 0; c < CPG; c++) {
+      const int tt = warp * CPW + grp * CPG + c;
       const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
       if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = vacc[c];
     }
@@ -415,8 +425,8 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
   return p.P2;
 }
 
-// One tile per CTA: grid (tiles x, tiles y, 32-slice slabs).
-template <typename T, int CPW, int CU, int NW, bool COUNT>
+// One tile per CTA: grid (tiles x, tiles y, SL-slice slabs).
+template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
 __global__ void __launch_bounds__((NW + 1) * 32, 1)
 k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
          const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
@@ -425,14 +435,14 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
   // it starts at the (128-byte aligned) base of the CTA's window
   extern __shared__ __align__(128) uint8_t smem[];
   bp_init_barriers(smem, NW);
-  bp_tile<T, CPW, CU, NW, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
+  bp_tile<T, CPW, CU, NW, SL, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
                                  bt.zb0 + blockIdx.z, count, err, smem, 0u);
 }
 
 // Persistent launch over the column tiles of several scans: each CTA takes
 // the next work item (scan, tile x, tile y, slab) from a global counter until
 // the list is exhausted. Items are listed by decreasing estimated cost.
-template <typename T, int CPW, int CU, int NW>
+template <typename T, int CPW, int CU, int NW, int SL>
 __global__ void __launch_bounds__((NW + 1) * 32, 1)
 k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items, int n_items,
                unsigned* __restrict__ next, int* __restrict__ err) {
@@ -449,58 +459,60 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
     const BpScan* sd = scans + w.x;
     const BPParams p = sd->p;
     const BPTile bt = sd->bt;
-    ring += (uint32_t)bp_tile<T, CPW, CU, NW, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
+    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
                                                  sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring);
     __syncthreads();  // the tile's shared memory and words[9] are free again
   }
 }
 
-template <typename T, int CPW, int CU, int NW>
+template <typename T, int CPW, int CU, int NW, int SL>
 cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                        unsigned long long* count, int* err, cudaStream_t s) {
-  const int nslab = (p.nz + 31) / 32;
+  const int nslab = (p.nz + SL - 1) / SL;
   if (bt.zb0 < 0 || bt.zb0 >= nslab || bt.nzb < 0 || bt.zb0 + bt.nzb > nslab) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((p.nx + bt.tx - 1) / bt.tx), (unsigned)((p.ny + bt.ty - 1) / bt.ty),
             (unsigned)(bt.nzb ? bt.nzb : nslab - bt.zb0));
   constexpr int threads = (NW + 1) * 32;
   cudaError_t e;
   if (count) {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, SL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, NW, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
+    k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
                                                                          count, err);
   } else {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, SL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, NW, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
+    k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
                                                                           count, err);
   }
   return cudaGetLastError();
 }
 
-template <typename T, int CPW, int CU, int NW>
+template <typename T, int CPW, int CU, int NW, int SL>
 cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
                              int smem_bytes, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(k_bp_tma_batch<T, CPW, CU, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_bp_tma_batch<T, CPW, CU, NW, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        smem_bytes);
   if (e != cudaSuccess) return e;
-  k_bp_tma_batch<T, CPW, CU, NW><<<grid, (NW + 1) * 32, smem_bytes, s>>>(scans, items, n_items, next, err);
+  k_bp_tma_batch<T, CPW, CU, NW, SL><<<grid, (NW + 1) * 32, smem_bytes, s>>>(scans, items, n_items, next, err);
   return cudaGetLastError();
 }
 
-// The instantiated launch shapes: (columns per warp, columns per pass, consumer warps).
-#define WFBP_BP_SHAPES(X) X(16, 4, 16) X(16, 8, 16) X(8, 4, 16) X(8, 8, 16) X(4, 4, 16) X(8, 4, 20) X(8, 8, 20) X(4, 4, 24)
+// The instantiated launch shapes: (columns per warp, columns per pass, consumer warps, slab slices).
+#define WFBP_BP_SHAPES(X)                                                                                        \
+  X(16, 4, 16, 32) X(16, 8, 16, 32) X(8, 4, 16, 32) X(8, 8, 16, 32) X(4, 4, 16, 32) X(8, 4, 20, 32) X(8, 8, 20, 32) \
+  X(4, 4, 24, 32) X(16, 4, 16, 16) X(16, 8, 16, 16) X(8, 4, 20, 16) X(16, 4, 20, 16) X(16, 8, 20, 16)
 
 template <typename T>
 cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                         const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                         unsigned long long* count, int* err, cudaStream_t s) {
   const int cpw = bt.tx * bt.ty / bt.nw;
-#define WFBP_ONE(C, U, N) \
-  if (cpw == C && bt.cu == U && bt.nw == N) return launch_one<T, C, U, N>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+#define WFBP_ONE(C, U, N, S) \
+  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return launch_one<T, C, U, N, S>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
   WFBP_BP_SHAPES(WFBP_ONE)
 #undef WFBP_ONE
   return cudaErrorInvalidValue;
@@ -518,8 +530,8 @@ bool bp_tma_supported(const BPTile& bt) {
   if (bt.nw < 1) return false;
   const int cpw = bt.tx * bt.ty / bt.nw;
   if (bt.tx * bt.ty != cpw * bt.nw) return false;
-#define WFBP_SUP(C, U, N) \
-  if (cpw == C && bt.cu == U && bt.nw == N) return true;
+#define WFBP_SUP(C, U, N, S) \
+  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return true;
   WFBP_BP_SHAPES(WFBP_SUP)
 #undef WFBP_SUP
   return false;
@@ -550,13 +562,13 @@ cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* v
   return launch_elem<float>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
 }
 
-cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, const BpScan* scans,
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,
                                          const int4* items, int n_items, unsigned* next, int* err, int smem_bytes,
                                          int grid, cudaStream_t s) {
-#define WFBP_B32(C, U, N) \
-  if (cpw == C && cu == U && nw == N) return launch_batch_one<uint32_t, C, U, N>(scans, items, n_items, next, err, smem_bytes, grid, s);
-#define WFBP_BF(C, U, N) \
-  if (cpw == C && cu == U && nw == N) return launch_batch_one<float, C, U, N>(scans, items, n_items, next, err, smem_bytes, grid, s);
+#define WFBP_B32(C, U, N, S) \
+  if (cpw == C && cu == U && nw == N && slab == S) return launch_batch_one<uint32_t, C, U, N, S>(scans, items, n_items, next, err, smem_bytes, grid, s);
+#define WFBP_BF(C, U, N, S) \
+  if (cpw == C && cu == U && nw == N && slab == S) return launch_batch_one<float, C, U, N, S>(scans, items, n_items, next, err, smem_bytes, grid, s);
   if (elem_half2) {
     WFBP_BP_SHAPES(WFBP_B32)
   } else {

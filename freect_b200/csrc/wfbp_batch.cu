@@ -84,12 +84,12 @@ void free_plan(wfbp_batch* b) {
 
 // Views per theta~ reaching each 32-slice slab of a scan, summed over
 // theta~: the backprojection work of one column of that slab.
-std::vector<double> slab_view_counts(const wfbp_ctx* c, const std::vector<float>& view_z) {
-  const int nslab = (c->nz + 31) / 32;
+std::vector<double> slab_view_counts(const wfbp_ctx* c, const std::vector<float>& view_z, int slab) {
+  const int nslab = (c->nz + slab - 1) / slab;
   std::vector<double> out(nslab, 0.0);
   for (int sl = 0; sl < nslab; sl++) {
     float zmn = 3e38f, zmx = -3e38f;
-    for (int i = sl * 32; i < std::min(c->nz, sl * 32 + 32); i++) {
+    for (int i = sl * slab; i < std::min(c->nz, sl * slab + slab); i++) {
       zmn = std::min(zmn, c->z_native[i]);
       zmx = std::max(zmx, c->z_native[i]);
     }
@@ -117,7 +117,7 @@ int build_plan(wfbp_batch* b) {
     wfbp_ctx* c = b->ctx[i];
     BPTile bt;
     if (!wfbp_detail::size_backprojection(c, b->cfg.tile_x, b->cfg.tile_y, b->cfg.cols_per_step,
-                                          b->cfg.consumer_warps, &bt))
+                                          b->cfg.consumer_warps, b->cfg.slab, &bt))
       return bfail(b, WFBP_ERR_UNSUPPORTED, "backprojection configuration " + std::to_string(b->cfg.tile_x) + "x" +
                                                 std::to_string(b->cfg.tile_y) + "/" +
                                                 std::to_string(b->cfg.cols_per_step) + " does not fit scan " +
@@ -138,7 +138,7 @@ int build_plan(wfbp_batch* b) {
     // view table positions for the cost estimate
     std::vector<float> vz(c->V);
     BCUDA(b, cudaMemcpy(vz.data(), c->d_view_z, sizeof(float) * c->V, cudaMemcpyDeviceToHost));
-    const std::vector<double> nv = slab_view_counts(c, vz);
+    const std::vector<double> nv = slab_view_counts(c, vz, bt.slab);
     const int tx = (c->nx + bt.tx - 1) / bt.tx, ty = (c->ny + bt.ty - 1) / bt.ty;
     const double vx = c->rp.recon_fov / c->nx, vy = c->rp.recon_fov / c->ny;
     const double r2 = 0.25 * c->cg.acquisition_field_of_view * c->cg.acquisition_field_of_view;
@@ -231,12 +231,13 @@ WFBP_API int wfbp_batch_create(wfbp_ctx* const* ctxs, int n, wfbp_batch** out) {
   // default configuration: the first candidate every scan fits
   int st = WFBP_ERR_UNSUPPORTED;
   for (int k = 0; k < wfbp_detail::n_bp_candidates() && st; k++) {
-    wfbp_detail::bp_candidate(k, &b->cfg.tile_x, &b->cfg.tile_y, &b->cfg.cols_per_step, &b->cfg.consumer_warps);
+    wfbp_detail::bp_candidate(k, &b->cfg.tile_x, &b->cfg.tile_y, &b->cfg.cols_per_step, &b->cfg.consumer_warps,
+                              &b->cfg.slab);
     bool fits = true;
     for (int i = 0; i < n && fits; i++) {
       BPTile bt;
       fits = wfbp_detail::size_backprojection(b->ctx[i], b->cfg.tile_x, b->cfg.tile_y, b->cfg.cols_per_step,
-                                              b->cfg.consumer_warps, &bt);
+                                              b->cfg.consumer_warps, b->cfg.slab, &bt);
     }
     if (fits) st = build_plan(b);
   }
@@ -259,12 +260,12 @@ WFBP_API int wfbp_batch_bp_configs(const wfbp_batch* b, wfbp_bp_config* out, int
   int k = 0;
   for (int c = 0; c < wfbp_detail::n_bp_candidates(); c++) {
     wfbp_bp_config cfg{};
-    wfbp_detail::bp_candidate(c, &cfg.tile_x, &cfg.tile_y, &cfg.cols_per_step, &cfg.consumer_warps);
+    wfbp_detail::bp_candidate(c, &cfg.tile_x, &cfg.tile_y, &cfg.cols_per_step, &cfg.consumer_warps, &cfg.slab);
     bool fits = true;
     for (size_t i = 0; i < b->ctx.size() && fits; i++) {
       BPTile bt;
       fits = wfbp_detail::size_backprojection(b->ctx[i], cfg.tile_x, cfg.tile_y, cfg.cols_per_step, cfg.consumer_warps,
-                                              &bt);
+                                              cfg.slab, &bt);
     }
     if (!fits) continue;
     if (k < cap) out[k] = cfg;
@@ -286,6 +287,7 @@ WFBP_API int wfbp_batch_set_bp_config(wfbp_batch* b, const wfbp_bp_config* cfg) 
   const wfbp_bp_config old = b->cfg;
   b->cfg = *cfg;
   if (b->cfg.consumer_warps == 0) b->cfg.consumer_warps = BT_CWARPS;
+  if (b->cfg.slab == 0) b->cfg.slab = 32;
   int st = build_plan(b);
   if (st) {
     const std::string msg = b->err;
@@ -331,7 +333,7 @@ WFBP_API int wfbp_batch_run(wfbp_batch* b, const float* const* raws, float* cons
     if (!st && !e) {
       const int cpw = b->cfg.tile_x * b->cfg.tile_y / b->cfg.consumer_warps;
       e = launch_backproject_tma_batch(b->precision == WFBP_PRECISION_MIXED ? 1 : 0, cpw, b->cfg.cols_per_step,
-                                       b->cfg.consumer_warps,
+                                       b->cfg.consumer_warps, b->cfg.slab,
                                        b->d_scans, b->d_items, b->n_items, b->d_next, b->d_err, b->smem, b->grid, s);
     }
     for (int i = 0; i < n && !st && !e; i++) {

@@ -178,6 +178,7 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_radj_idx);
   free_dev(ctx->d_radj_w);
   free_dev(ctx->d_tg_partial);
+  free_dev(ctx->d_adj_scale);
   for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
   ctx->ev_copy.clear();
   if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
@@ -298,13 +299,14 @@ void bp_reach(wfbp_ctx* ctx, const std::vector<float>& table) {
 }
 
 // Sizes one TMA backprojection configuration; false if it does not fit.
-bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* out) {
+bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, int slab, BPTile* out) {
   const double vx = ctx->rp.recon_fov / ctx->nx, vy = ctx->rp.recon_fov / ctx->ny;
   BPTile b;
   b.tx = tx;
   b.ty = ty;
   b.cu = cu;
   b.nw = nw;
+  b.slab = slab;
   b.zb0 = 0;
   b.nzb = 0;
   const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
@@ -323,16 +325,18 @@ bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* o
   return true;
 }
 
-// (tile x, tile y, columns per pass, consumer warps)
-const int kBpCandidates[][4] = {{16, 16, 4, 16}, {16, 16, 8, 16}, {16, 8, 4, 16}, {16, 8, 8, 16}, {8, 16, 4, 16},
-                                {8, 16, 8, 16},  {8, 8, 4, 16},   {16, 10, 4, 20}, {16, 10, 8, 20}, {10, 16, 4, 20},
-                                {12, 8, 4, 24}};
+// (tile x, tile y, columns per pass, consumer warps, slab slices)
+const int kBpCandidates[][5] = {
+    {16, 16, 4, 16, 32}, {16, 16, 8, 16, 32}, {16, 8, 4, 16, 32},  {16, 8, 8, 16, 32},  {8, 16, 4, 16, 32},
+    {8, 16, 8, 16, 32},  {8, 8, 4, 16, 32},   {16, 10, 4, 20, 32}, {16, 10, 8, 20, 32}, {10, 16, 4, 20, 32},
+    {12, 8, 4, 24, 32},  {16, 16, 4, 16, 16}, {16, 16, 8, 16, 16}, {16, 10, 4, 20, 16}, {16, 20, 4, 20, 16},
+    {16, 20, 8, 20, 16}};
 
 bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
   bp_reach(ctx, table);
   for (auto& c : kBpCandidates) {
     BPTile b;
-    if (size_bp_tile(ctx, c[0], c[1], c[2], c[3], &b)) {
+    if (size_bp_tile(ctx, c[0], c[1], c[2], c[3], c[4], &b)) {
       ctx->bpt = b;
       return true;
     }
@@ -754,12 +758,13 @@ WFBP_API int wfbp_bp_configs(const wfbp_ctx* ctx, wfbp_bp_config* out, int cap, 
   int k = 0;
   for (auto& c : kBpCandidates) {
     BPTile b;
-    if (!size_bp_tile(ctx, c[0], c[1], c[2], c[3], &b)) continue;
+    if (!size_bp_tile(ctx, c[0], c[1], c[2], c[3], c[4], &b)) continue;
     if (k < cap) {
       out[k].tile_x = c[0];
       out[k].tile_y = c[1];
       out[k].cols_per_step = c[2];
       out[k].consumer_warps = c[3];
+      out[k].slab = c[4];
     }
     k++;
   }
@@ -775,6 +780,7 @@ WFBP_API int wfbp_get_bp_config(const wfbp_ctx* ctx, wfbp_bp_config* c) {
   c->tile_y = ctx->bpt.ty;
   c->cols_per_step = ctx->bpt.cu;
   c->consumer_warps = ctx->bpt.nw;
+  c->slab = ctx->bpt.slab;
   return WFBP_OK;
 }
 
@@ -783,10 +789,11 @@ WFBP_API int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* c) {
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_set_bp_config: call wfbp_set_views first");
   BPTile b;
   const int nw = c->consumer_warps ? c->consumer_warps : BT_CWARPS;
-  if (!size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, nw, &b))
+  const int slab = c->slab ? c->slab : 32;
+  if (!size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, nw, slab, &b))
     return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_set_bp_config: configuration " + std::to_string(c->tile_x) + "x" +
                                                std::to_string(c->tile_y) + "/" + std::to_string(c->cols_per_step) + "w" +
-                                               std::to_string(nw) +
+                                               std::to_string(nw) + "s" + std::to_string(slab) +
                                                " is not supported for this geometry");
   ctx->bpt = b;
   ctx->bp_tma_ok = true;
@@ -971,6 +978,8 @@ WFBP_API int wfbp_thicken(wfbp_ctx* ctx, const float* vn, float* vol, void* stre
 // ---------------------------------------------------------------------------
 
 namespace {
+constexpr size_t kAdjointTableBytes = size_t(6) << 30;  // backprojection adjoint scale table limit
+
 int require_fp32_views(wfbp_ctx* ctx, const char* what) {
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, std::string(what) + ": wfbp_set_views not called");
   if (ctx->ext.precision != WFBP_PRECISION_FP32)
@@ -1015,8 +1024,23 @@ WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, floa
   const BPParams p = bp_params(ctx);
   const float z0 = ctx->z_native[0];
   const float dzs = ctx->nz > 1 ? (ctx->z_native[ctx->nz - 1] - ctx->z_native[0]) / (float)(ctx->nz - 1) : 0.0f;
+  // the per-(voxel, theta~) scale table when it is small enough (a few GB);
+  // otherwise the gather recomputes the weight sums
+  const size_t n = (size_t)ctx->P2 * ctx->nz * ctx->nx * ctx->ny;
+  const bool want_table = ctx->ext.adjoint_scale_table == 0 && n * sizeof(float) <= kAdjointTableBytes;
+  if (want_table && n > ctx->adj_scale_n) {
+    free_dev(ctx->d_adj_scale);
+    if (cudaMalloc(&ctx->d_adj_scale, n * sizeof(float)) == cudaSuccess) {
+      ctx->adj_scale_n = n;
+    } else {
+      cudaGetLastError();
+      ctx->d_adj_scale = nullptr;
+      ctx->adj_scale_n = 0;
+    }
+  }
+  float* table = want_table && n <= ctx->adj_scale_n ? ctx->d_adj_scale : nullptr;
   CUDA_TRY(ctx, launch_bp_adjoint(g_native, g_filtered, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, z0, dzs,
-                                  (cudaStream_t)stream));
+                                  table, (cudaStream_t)stream));
   return WFBP_OK;
 }
 
@@ -1064,6 +1088,7 @@ WFBP_API int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_
   const size_t need = (size_t)taps_grad_blocks(p) * n;
   if (need > ctx->tg_partial_n) {
     free_dev(ctx->d_tg_partial);
+  free_dev(ctx->d_adj_scale);
   for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
   ctx->ev_copy.clear();
   if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
@@ -1196,12 +1221,13 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[c], ctx->s_copy));
   }
   // last view each slab needs: views j < K P/2 within the slab's reach in z
-  const int nslab = (ctx->nz + 31) / 32;
+  const int SLB = ctx->bpt.slab;
+  const int nslab = (ctx->nz + SLB - 1) / SLB;
   std::vector<int> need(nslab, -1);
   const int used = ctx->K * ctx->P2;
   for (int sl = 0; sl < nslab; sl++) {
     float zmn = 3e38f, zmx = -3e38f;
-    for (int i = sl * 32; i < std::min(ctx->nz, sl * 32 + 32); i++) {
+    for (int i = sl * SLB; i < std::min(ctx->nz, sl * SLB + SLB); i++) {
       zmn = std::min(zmn, ctx->z_native[i]);
       zmx = std::max(zmx, ctx->z_native[i]);
     }
@@ -1289,17 +1315,18 @@ BPParams backprojection_params(const wfbp_ctx* ctx) { return bp_params(ctx); }
 void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal) {
   stage_bytes(ctx, layout, reb, filt, scal);
 }
-bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* out) {
-  return size_bp_tile(ctx, tx, ty, cu, nw, out);
+bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, int slab, BPTile* out) {
+  return size_bp_tile(ctx, tx, ty, cu, nw, slab, out);
 }
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
   return do_filter(ctx, rebinned, filtered, scales, layout, stream);
 }
 int n_bp_candidates() { return (int)(sizeof(kBpCandidates) / sizeof(kBpCandidates[0])); }
-void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw) {
+void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw, int* slab) {
   *tx = kBpCandidates[i][0];
   *ty = kBpCandidates[i][1];
   *cu = kBpCandidates[i][2];
   *nw = kBpCandidates[i][3];
+  *slab = kBpCandidates[i][4];
 }
 }  // namespace wfbp_detail

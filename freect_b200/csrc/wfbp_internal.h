@@ -46,7 +46,8 @@ struct BPTile {
   int smem_bytes;    // dynamic shared memory of the launch
   int cu;            // columns accumulated per step of the view loop (4 or 8)
   int nw;            // consumer warps per CTA (16, 20 or 24; one more warp produces)
-  int zb0, nzb;      // 32-slice slabs [zb0, zb0 + nzb) of this launch (nzb 0: all)
+  int slab;          // native slices per slab (32, or 16 with two column groups per warp)
+  int zb0, nzb;      // slabs [zb0, zb0 + nzb) of this launch (nzb 0: all)
 };
 
 // Byte offsets of the TMA backprojection's shared-memory regions; the same
@@ -129,6 +130,8 @@ struct wfbp_ctx {
   float* d_radj_w = nullptr;
   float* d_tg_partial = nullptr;    // per-CTA partial tap gradients
   size_t tg_partial_n = 0;
+  float* d_adj_scale = nullptr;     // backprojection adjoint: per-(voxel, theta~) gradient scale
+  size_t adj_scale_n = 0;
 
   // mixed precision: Toeplitz operand planes for the tensor-core filter
   int tc_kp = 0, tc_np = 0, tc_bn = 0;
@@ -204,7 +207,7 @@ struct alignas(64) BpScan {
   const float* zslices;
 };
 cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map);
-cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, const BpScan* scans,
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,
                                          const int4* items, int n_items, unsigned* next, int* err, int smem_bytes,
                                          int grid, cudaStream_t s);
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);
@@ -215,8 +218,10 @@ cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* v
 int tc_choose_bn(int nch);
 cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
                            const float* ws, int nxy, int nzr, cudaStream_t s);
+// scale_table: [P/2][nz][ny][nx] scratch for the per-(voxel, theta~) gradient
+// scale, or null (then the gather recomputes the weight sums itself)
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
-                              const BPParams& p, float z0, float dzs, cudaStream_t s);
+                              const BPParams& p, float z0, float dzs, float* scale_table, cudaStream_t s);
 cudaError_t launch_thicken_adjoint(const float* gvol, float* gvn, const int* off, const int* ridx, const float* w,
                                    int nxy, int nz, cudaStream_t s);
 cudaError_t launch_rebin_adj_cols(const float* bidx, int nch, int q8, int* cnt, int* cidx, float* cw, int maxl,
@@ -235,8 +240,8 @@ namespace wfbp_detail {
 int set_error(wfbp_ctx* ctx, int code, const std::string& msg);
 BPParams backprojection_params(const wfbp_ctx* ctx);
 void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal);
-bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, BPTile* out);
+bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, int slab, BPTile* out);
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream);
 int n_bp_candidates();
-void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw);
+void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw, int* slab);
 }  // namespace wfbp_detail

@@ -180,7 +180,7 @@ def filter_taps(cg, window=T.FILTER_REFERENCE, c=1.0, a=1.0, n=None):
 
 
 def make_ext(precision=T.PRECISION_FP32, filter_window=T.FILTER_REFERENCE, filter_c=1.0, filter_a=1.0,
-             user_taps=None, tex_weights=0, bp_slab=0, filtered_layout=T.LAYOUT_REFERENCE):
+             user_taps=None, tex_weights=0, bp_slab=0, filtered_layout=T.LAYOUT_REFERENCE, adjoint_scale_table=0):
     e = T.Ext()
     e.version = T.EXT_VERSION
     e.precision = precision
@@ -190,6 +190,7 @@ def make_ext(precision=T.PRECISION_FP32, filter_window=T.FILTER_REFERENCE, filte
     e.tex_weights = tex_weights
     e.bp_slab = bp_slab
     e.filtered_layout = filtered_layout
+    e.adjoint_scale_table = adjoint_scale_table
     if user_taps is not None:
         arr = np.ascontiguousarray(user_taps, dtype=np.float32)
         e._taps_keepalive = arr
@@ -288,6 +289,7 @@ class Context:
             c = T.BpConfig()
             c.tile_x, c.tile_y, c.cols_per_step = config[:3]
             c.consumer_warps = config[3] if len(config) > 3 else 0
+            c.slab = config[4] if len(config) > 4 else 0
             config = c
         _check(self._lib.wfbp_set_bp_config(self._h, C.byref(config)), "wfbp_set_bp_config", self._h)
 
@@ -491,6 +493,7 @@ class Batch:
             c = T.BpConfig()
             c.tile_x, c.tile_y, c.cols_per_step = config[:3]
             c.consumer_warps = config[3] if len(config) > 3 else 0
+            c.slab = config[4] if len(config) > 4 else 0
             config = c
         self._check(self._lib.wfbp_batch_set_bp_config(self._h, C.byref(config)), "wfbp_batch_set_bp_config")
 

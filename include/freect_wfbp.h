@@ -179,7 +179,9 @@ typedef struct wfbp_ext {
                                  texture unit the reference samples through (cuda_kernels.cuh:36) */
   int bp_slab;                /* 0 = default; native slices per backprojection slab */
   int filtered_layout;        /* wfbp_layout of the stage API (default REFERENCE) */
-  int reserved[6];
+  int adjoint_scale_table;    /* 0: the backprojection adjoint keeps a per-(voxel, half-turn angle)
+                                 gradient scale table when it fits in 6 GB; -1: never (recompute) */
+  int reserved[5];
 } wfbp_ext;
 
 /* Sizes of every stage buffer a context expects (bytes unless noted). */
@@ -280,15 +282,17 @@ int wfbp_set_slices(wfbp_ctx* ctx, const float* native_z, int n_native, const fl
 /* Launch configuration of the backprojection in the backprojection layout
  * (no counterpart in the reference, whose backproject_kernel launch is a
  * fixed 16x16-thread block per voxel tile, ReconstructionMachine.cu:347-351).
- * A CTA covers tile_x * tile_y voxel columns and 32 native slices with
- * consumer_warps warps (0 = 16) plus one TMA producer warp;
- * cols_per_step columns are accumulated per pass over a view window.
+ * A CTA covers tile_x * tile_y voxel columns and `slab` native slices (32,
+ * or 16 with two column groups per warp; 0 = 32) with consumer_warps warps
+ * (0 = 16) plus one TMA producer warp; cols_per_step columns are
+ * accumulated per pass over a view window.
  * wfbp_set_views picks a default; an autotuner lists the configurations that
  * fit this geometry, times them and sets the fastest. All need set_views. */
 typedef struct wfbp_bp_config {
   int tile_x, tile_y;
   int cols_per_step;
   int consumer_warps;
+  int slab;
 } wfbp_bp_config;
 int wfbp_bp_configs(const wfbp_ctx* ctx, wfbp_bp_config* out, int cap, int* n);
 int wfbp_get_bp_config(const wfbp_ctx* ctx, wfbp_bp_config* config);

@@ -28,10 +28,10 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(DEV)
 
 
-def make(spec, tex_weights=0):
+def make(spec, tex_weights=0, adjoint_scale_table=0):
     tube, table = spec.views()
     cg, gp = wfbp.configure_geometry(spec.meta(), table)
-    ext = wfbp.make_ext(filter_window=spec.window, tex_weights=tex_weights)
+    ext = wfbp.make_ext(filter_window=spec.window, tex_weights=tex_weights, adjoint_scale_table=adjoint_scale_table)
     ctx = wfbp.Context(cg, spec.recon_config(), ext, device=0)
     ctx.set_views(tube, table)
     return ctx, cg, tube, table
@@ -82,13 +82,14 @@ def test_filter_adjoint(tiny):
     dot_ok(np.vdot(fx, y), np.vdot(x, gy), np.linalg.norm(fx), np.linalg.norm(y))
 
 
+@pytest.mark.parametrize("table_mode", [0, -1])  # with the scale table, and recomputing the weight sums
 @pytest.mark.parametrize("which", ["tiny", "odd"])
-def test_backproject_adjoint(orc, tiny, which):
+def test_backproject_adjoint(orc, tiny, which, table_mode):
     spec = tiny
     if which == "odd":
         spec = scans.tiny(nch=90, nr=5, P=100, rotations=2.57, nx=33, n_slices=3)
         spec.ny = 17
-    ctx, cg, tube, table = make(spec)
+    ctx, cg, tube, table = make(spec, adjoint_scale_table=table_mode)
     d = ctx.dims
     rng = np.random.default_rng(3)
     f = rng.standard_normal((d.n_views, d.n_rows, d.n_channels)).astype(np.float32)
