@@ -30,12 +30,16 @@ __device__ __forceinline__ float q_weight_fwd(float qh) {
 // The gradient of one filtered sample D[j][r][c] is therefore
 //   sum over voxels of g_vol * dtheta * W_j / sum_k W_k * hat(p_idx_j - c) * hat_row,
 // where hat is the bilinear weight. Ownership: a CTA owns view j and a run of
-// AD_CH channels; thread c owns channel column c of that view and walks the
-// voxels whose p_idx lies within one channel of c (a band around a line
-// through the image, traversed along its longer axis). For each such voxel
-// it visits the slices inside the view's cone, recomputes sum_k W_k from the
-// same expressions as the forward, and adds the two row contributions to its
-// own column in shared memory.
+// AD_CH consecutive channels; thread c walks the voxels whose p_idx lies in
+// [c, c + 1) (a band one channel wide around a line through the image,
+// traversed along its longer axis), so every (voxel, view) pair is visited
+// by exactly one thread. For each such voxel it visits the slices inside the
+// view's cone, takes g_vol * dtheta / sum_k W_k from the scale table (or
+// recomputes sum_k W_k from the same expressions as the forward), and adds
+// the row contributions to two accumulators of its own in shared memory: one
+// for channel c (weight 1 - frac(p_idx)) and one for channel c + 1 (weight
+// frac(p_idx)). At the end channel c = own(c) + next(c - 1), in that order;
+// the CTA's first thread only supplies next(c0 - 1) for its neighbour.
 constexpr int AD_CH = 128;
 
 __device__ __forceinline__ float xcoord(const BPParams& p, int ix) {
@@ -73,16 +77,18 @@ __device__ __forceinline__ float view_weight(const BPParams& p, const ViewGeo& g
   return ok ? q_weight_fwd(qh) : 0.0f;
 }
 
-// Scaled voxel gradients G[t][s][y][x] = g_vol * dtheta / sum_k W_k for each
+// Scaled voxel gradients G[t][y][x][s] = g_vol * dtheta / sum_k W_k for each
 // half-turn angle t (0 where no half turn contributes, as the forward's NaN
-// voxel has no gradient): one thread per (x, y) column and ZS slices, the
-// weights summed in the forward's order. With this table the gather below
-// needs one load instead of the other half turns' geometry.
+// voxel has no gradient), slices innermost with a stride of nzp = nz rounded
+// up to 4: one thread per (x, y) column and ZS slices, the weights summed in
+// the forward's order. With this table the gather below needs one load
+// instead of the other half turns' geometry, and a voxel's slice run is one
+// contiguous span.
 constexpr int AN_ZS = 8, AN_TX = 16, AN_TY = 8;
 
 __global__ void __launch_bounds__(AN_TX * AN_TY)
 k_bp_adjoint_scale(const float* __restrict__ gvol, float* __restrict__ G, const float2* __restrict__ view_sc,
-                   const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p) {
+                   const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, int nzp) {
   const int ix = blockIdx.x * AN_TX + (threadIdx.x % AN_TX);
   const int iy = blockIdx.y * AN_TY + (threadIdx.x / AN_TX);
   const int s0 = blockIdx.z * AN_ZS;
@@ -114,33 +120,37 @@ k_bp_adjoint_scale(const float* __restrict__ gvol, float* __restrict__ G, const 
         }
       }
     }
+    float* out = G + ((size_t)t * plane + vox) * nzp + s0;
 #pragma unroll
-    for (int i = 0; i < AN_ZS; i++) {
-      const int sl = s0 + i;
-      if (sl < p.nz)
-        G[((size_t)t * p.nz + sl) * plane + vox] = aw[i] > 0.0f ? gv[i] * (p.dtheta * (1.0f / aw[i])) : 0.0f;
-    }
+    for (int i = 0; i < AN_ZS; i++)
+      if (s0 + i < nzp) out[i] = aw[i] > 0.0f ? gv[i] * (p.dtheta * (1.0f / aw[i])) : 0.0f;
   }
 }
 
-__global__ void __launch_bounds__(AD_CH)
+template <bool TABLE>
+__global__ void __launch_bounds__(AD_CH, 8)
 k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float* __restrict__ gD,
              const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
-             BPParams p, float z0, float dzs) {
-  extern __shared__ float col[];  // [nr][AD_CH], thread c owns column c
-  const int j = blockIdx.y;
+             BPParams p, float z0, float dzs, int nzp) {
+  extern __shared__ float2 acc2[];  // [nr][AD_CH]: (own channel, next channel) of thread cl
+  // views of one half-turn angle run in consecutive blocks, so that they
+  // share its slice of the scale table in L2: block row b < K P/2 is view
+  // t + k P/2 with t = b / K, k = b % K; the views the forward never reads
+  // (j >= K P/2) follow in order
+  const int b = blockIdx.y, used = p.K * p.P2;
+  const int j = b < used ? (b / p.K) + (b % p.K) * p.P2 : b;
   const int cl = threadIdx.x;
-  const int c = blockIdx.x * AD_CH + cl;
-  for (int r = 0; r < p.nr; r++) col[r * AD_CH + cl] = 0.0f;
+  const int c = blockIdx.x * (AD_CH - 1) - 1 + cl;  // channels c0 - 1 .. c0 + AD_CH - 2
+  for (int r = 0; r < p.nr; r++) acc2[r * AD_CH + cl] = make_float2(0.0f, 0.0f);
 
   const int t = j % p.P2, kj = j / p.P2;
-  if (kj < p.K && c < p.nch) {
+  if (kj < p.K && c >= 0 && c < p.nch) {
     const float2 sc = __ldg(view_sc + j);
     const float zt = __ldg(view_z + j);
-    // p_idx within (c - 1, c + 1) <=> p_hat in this interval (widened; the
-    // exact forward test below decides)
-    const float ph_a = (p.kp - p.c0 - ((float)c + 1.0f)) / p.ps, ph_b = (p.kp - p.c0 - ((float)c - 1.0f)) / p.ps;
-    const float marg = 0.5f / p.ps + 1e-3f * p.fov / (float)p.nx;
+    // p_idx in [c, c + 1) <=> p_hat in this interval (widened by a rounding
+    // margin; the exact forward test below decides)
+    const float ph_a = (p.kp - p.c0 - ((float)c + 1.0f)) / p.ps, ph_b = (p.kp - p.c0 - (float)c) / p.ps;
+    const float marg = 0.02f / p.ps + 1e-3f * p.fov / (float)p.nx;
     const float plo = fminf(ph_a, ph_b) - marg, phi = fmaxf(ph_a, ph_b) + marg;
     const float sx = p.fov / (float)p.nx, sy = p.fov / (float)p.ny;
     const float nxm = 0.5f * ((float)p.nx - 1.0f), nym = 0.5f * ((float)p.ny - 1.0f);
@@ -152,14 +162,14 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
         const float y = ycoord(p, o);
         float xa = (plo + y * sc.y) / sc.x, xb = (phi + y * sc.y) / sc.x;
         if (xa > xb) { const float tt = xa; xa = xb; xb = tt; }
-        i_lo = max(0, (int)floorf((xa - p.x0) / sx + nxm) - 1);
-        i_hi = min(p.nx - 1, (int)ceilf((xb - p.x0) / sx + nxm) + 1);
+        i_lo = max(0, (int)floorf((xa - p.x0) / sx + nxm));
+        i_hi = min(p.nx - 1, (int)ceilf((xb - p.x0) / sx + nxm));
       } else {
         const float x = xcoord(p, o);
         float ya = (x * sc.x - phi) / sc.y, yb = (x * sc.x - plo) / sc.y;
         if (ya > yb) { const float tt = ya; ya = yb; yb = tt; }
-        i_lo = max(0, (int)floorf((ya - p.y0) / sy + nym) - 1);
-        i_hi = min(p.ny - 1, (int)ceilf((yb - p.y0) / sy + nym) + 1);
+        i_lo = max(0, (int)floorf((ya - p.y0) / sy + nym));
+        i_hi = min(p.ny - 1, (int)ceilf((yb - p.y0) / sy + nym));
       }
       for (int in = i_lo; in <= i_hi; in++) {
         const int ix = along_y ? in : o, iy = along_y ? o : in;
@@ -168,11 +178,8 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
         const ViewGeo g = view_geo(p, x, y, sc, zt);
         if (!g.valid_p) continue;
         const float pf = floorf(g.p_idx), wp = g.p_idx - pf;
-        float hp;
-        if ((int)pf == c) hp = 1.0f - wp;
-        else if ((int)pf + 1 == c) hp = wp;
-        else continue;
-        if (hp == 0.0f) continue;
+        if ((int)pf != c) continue;
+        const float h0 = 1.0f - wp;  // channel c; channel c + 1 gets wp
         // slices that can pass this view's tests: |z - zt| <= z_rot and
         // q_idx in [0, nr-2], a z interval around zt - A
         const float za = zt - g.A - 1.0f / g.inv, zb = zt - g.A + (p.nrm2 / p.hn - 1.0f) / g.inv;
@@ -185,17 +192,18 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
         } else {
           float fa = (zlo - z0) / dzs, fb = (zhi - z0) / dzs;
           if (fa > fb) { const float tt = fa; fa = fb; fb = tt; }
-          s_lo = max(0, (int)floorf(fa) - 2);
-          s_hi = min(p.nz - 1, (int)ceilf(fb) + 2);
+          s_lo = max(0, (int)floorf(fa) - 1);
+          s_hi = min(p.nz - 1, (int)ceilf(fb) + 1);
         }
+        const float* gcol = TABLE ? G + (((size_t)t * p.ny + iy) * p.nx + ix) * nzp : nullptr;
         for (int s = s_lo; s <= s_hi; s++) {
           const float z = __ldg(zslices + s);
           float q_idx;
           const float Wj = view_weight(p, g, z, &q_idx);
           if (Wj == 0.0f) continue;
           float scaled;  // g_vol * dtheta / sum_k W_k (cuda_kernels.cuh:283)
-          if (G) {
-            scaled = __ldg(G + (((size_t)t * p.nz + s) * p.ny + iy) * p.nx + ix);
+          if constexpr (TABLE) {
+            scaled = __ldg(gcol + s);
             if (scaled == 0.0f) continue;
           } else {
             const float gv = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix);
@@ -216,18 +224,26 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
             }
             scaled = gv * (p.dtheta * (1.0f / aw));
           }
-          const float cval = scaled * Wj * hp;
+          const float sw = scaled * Wj;
+          const float c0v = sw * h0, c1v = sw * wp;
           const float qf = floorf(q_idx), wq = q_idx - qf;
           const int r = min(max((int)qf, 0), p.nr - 2);
-          col[r * AD_CH + cl] += cval * (1.0f - wq);
-          col[(r + 1) * AD_CH + cl] += cval * wq;
+          float2* a0 = acc2 + r * AD_CH + cl;
+          float2 v0 = a0[0], v1 = a0[AD_CH];
+          v0.x += c0v * (1.0f - wq);
+          v0.y += c1v * (1.0f - wq);
+          v1.x += c0v * wq;
+          v1.y += c1v * wq;
+          a0[0] = v0;
+          a0[AD_CH] = v1;
         }
       }
     }
   }
-  if (c < p.nch) {
+  __syncthreads();
+  if (cl >= 1 && c < p.nch) {
     float* out = gD + (size_t)j * p.nr * p.nch + c;
-    for (int r = 0; r < p.nr; r++) out[(size_t)r * p.nch] = col[r * AD_CH + cl];
+    for (int r = 0; r < p.nr; r++) out[(size_t)r * p.nch] = acc2[r * AD_CH + cl].x + acc2[r * AD_CH + cl - 1].y;
   }
 }
 
@@ -398,17 +414,18 @@ cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, co
   if (scale_table) {
     dim3 g((unsigned)((p.nx + AN_TX - 1) / AN_TX), (unsigned)((p.ny + AN_TY - 1) / AN_TY),
            (unsigned)((p.nz + AN_ZS - 1) / AN_ZS));
-    k_bp_adjoint_scale<<<g, AN_TX * AN_TY, 0, s>>>(gvol, scale_table, sc, vz, zs, p);
+    k_bp_adjoint_scale<<<g, AN_TX * AN_TY, 0, s>>>(gvol, scale_table, sc, vz, zs, p, bp_adjoint_nzp(p.nz));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  dim3 grid((unsigned)((p.nch + AD_CH - 1) / AD_CH), (unsigned)p.V);
-  const size_t smem = (size_t)p.nr * AD_CH * sizeof(float);
+  dim3 grid((unsigned)((p.nch + AD_CH - 2) / (AD_CH - 1)), (unsigned)p.V);
+  const size_t smem = (size_t)p.nr * AD_CH * sizeof(float2);
+  auto kern = scale_table ? k_bp_adjoint<true> : k_bp_adjoint<false>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_bp_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_bp_adjoint<<<grid, AD_CH, smem, s>>>(gvol, scale_table, gD, sc, vz, zs, p, z0, dzs);
+  kern<<<grid, AD_CH, smem, s>>>(gvol, scale_table, gD, sc, vz, zs, p, z0, dzs, bp_adjoint_nzp(p.nz));
   return cudaGetLastError();
 }
 

@@ -1023,10 +1023,15 @@ WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, floa
   DeviceGuard g(ctx->device);
   const BPParams p = bp_params(ctx);
   const float z0 = ctx->z_native[0];
-  const float dzs = ctx->nz > 1 ? (ctx->z_native[ctx->nz - 1] - ctx->z_native[0]) / (float)(ctx->nz - 1) : 0.0f;
+  // the gather finds a voxel's slice range from the spacing when the native
+  // slices are evenly spaced (to a thousandth of a slice); otherwise (0) it
+  // tests every slice
+  float dzs = ctx->nz > 1 ? (ctx->z_native[ctx->nz - 1] - ctx->z_native[0]) / (float)(ctx->nz - 1) : 0.0f;
+  for (int i = 0; i < ctx->nz && dzs != 0.0f; i++)
+    if (fabsf(ctx->z_native[i] - (z0 + (float)i * dzs)) > 1e-3f * fabsf(dzs)) dzs = 0.0f;
   // the per-(voxel, theta~) scale table when it is small enough (a few GB);
   // otherwise the gather recomputes the weight sums
-  const size_t n = (size_t)ctx->P2 * ctx->nz * ctx->nx * ctx->ny;
+  const size_t n = (size_t)ctx->P2 * bp_adjoint_nzp(ctx->nz) * ctx->nx * ctx->ny;
   const bool want_table = ctx->ext.adjoint_scale_table == 0 && n * sizeof(float) <= kAdjointTableBytes;
   if (want_table && n > ctx->adj_scale_n) {
     free_dev(ctx->d_adj_scale);
@@ -1038,7 +1043,7 @@ WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, floa
       ctx->adj_scale_n = 0;
     }
   }
-  float* table = want_table && n <= ctx->adj_scale_n ? ctx->d_adj_scale : nullptr;
+  float* table = want_table && ctx->d_adj_scale && n <= ctx->adj_scale_n ? ctx->d_adj_scale : nullptr;
   CUDA_TRY(ctx, launch_bp_adjoint(g_native, g_filtered, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, z0, dzs,
                                   table, (cudaStream_t)stream));
   return WFBP_OK;
@@ -1088,11 +1093,6 @@ WFBP_API int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_
   const size_t need = (size_t)taps_grad_blocks(p) * n;
   if (need > ctx->tg_partial_n) {
     free_dev(ctx->d_tg_partial);
-  free_dev(ctx->d_adj_scale);
-  for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
-  ctx->ev_copy.clear();
-  if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
-  ctx->s_copy = nullptr;
     CUDA_TRY(ctx, cudaMalloc(&ctx->d_tg_partial, sizeof(float) * need));
     ctx->tg_partial_n = need;
   }

@@ -220,6 +220,8 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
                            const float* ws, int nxy, int nzr, cudaStream_t s);
 // scale_table: [P/2][nz][ny][nx] scratch for the per-(voxel, theta~) gradient
 // scale, or null (then the gather recomputes the weight sums itself)
+// slice stride of the backprojection adjoint's scale table [P/2][ny][nx][nzp]
+inline int bp_adjoint_nzp(int nz) { return (nz + 3) / 4 * 4; }
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
                               const BPParams& p, float z0, float dzs, float* scale_table, cudaStream_t s);
 cudaError_t launch_thicken_adjoint(const float* gvol, float* gvn, const int* off, const int* ridx, const float* w,
