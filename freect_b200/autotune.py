@@ -94,7 +94,7 @@ def tune_backprojection(ctx, filtered, volume_native, row_scales=None, reps=2, u
 
 
 def batch_signature(batch):
-    parts = ["v1-batch"]
+    parts = ["v2-batch"]
     for c in batch.contexts:
         parts.append(signature(c))
     return "||".join(parts)

@@ -77,17 +77,18 @@ __device__ __forceinline__ float view_weight(const BPParams& p, const ViewGeo& g
   return ok ? q_weight_fwd(qh) : 0.0f;
 }
 
-// Scaled voxel gradients G[t][y][x][s] = g_vol * dtheta / sum_k W_k for each
-// half-turn angle t (0 where no half turn contributes, as the forward's NaN
-// voxel has no gradient), slices innermost with a stride of nzp = nz rounded
-// up to 4: one thread per (x, y) column and ZS slices, the weights summed in
-// the forward's order. With this table the gather below needs one load
-// instead of the other half turns' geometry, and a voxel's slice run is one
-// contiguous span.
+// Weights G[t][y][x][s] = dtheta / sum_k W_k for each half-turn angle t
+// (0 where no half turn contributes, as the forward's NaN voxel has no
+// gradient), slices innermost with a stride of nzp = nz rounded up to 4: one
+// thread per (x, y) column and ZS slices, the weights summed in the
+// forward's order. They depend on the geometry alone (views, slices, grid),
+// so the context computes them once and every later gradient reuses them;
+// with the table the gather below needs one load instead of the other half
+// turns' geometry, and a voxel's slice run is one contiguous span.
 constexpr int AN_ZS = 8, AN_TX = 16, AN_TY = 8;
 
 __global__ void __launch_bounds__(AN_TX * AN_TY)
-k_bp_adjoint_scale(const float* __restrict__ gvol, float* __restrict__ G, const float2* __restrict__ view_sc,
+k_bp_adjoint_scale(float* __restrict__ G, const float2* __restrict__ view_sc,
                    const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, int nzp) {
   const int ix = blockIdx.x * AN_TX + (threadIdx.x % AN_TX);
   const int iy = blockIdx.y * AN_TY + (threadIdx.x / AN_TX);
@@ -96,13 +97,9 @@ k_bp_adjoint_scale(const float* __restrict__ gvol, float* __restrict__ G, const 
   const float x = xcoord(p, ix), y = ycoord(p, iy);
   const size_t plane = (size_t)p.nx * p.ny, vox = (size_t)iy * p.nx + ix;
   const bool active = !(x * x + y * y > p.fov_half2);
-  float z[AN_ZS], gv[AN_ZS];
+  float z[AN_ZS];
 #pragma unroll
-  for (int i = 0; i < AN_ZS; i++) {
-    const int sl = s0 + i;
-    z[i] = sl < p.nz ? __ldg(zslices + sl) : 0.0f;
-    gv[i] = sl < p.nz ? __ldg(gvol + (size_t)sl * plane + vox) : 0.0f;
-  }
+  for (int i = 0; i < AN_ZS; i++) z[i] = s0 + i < p.nz ? __ldg(zslices + s0 + i) : 0.0f;
   for (int t = 0; t < p.P2; t++) {
     float aw[AN_ZS];
 #pragma unroll
@@ -123,7 +120,7 @@ k_bp_adjoint_scale(const float* __restrict__ gvol, float* __restrict__ G, const 
     float* out = G + ((size_t)t * plane + vox) * nzp + s0;
 #pragma unroll
     for (int i = 0; i < AN_ZS; i++)
-      if (s0 + i < nzp) out[i] = aw[i] > 0.0f ? gv[i] * (p.dtheta * (1.0f / aw[i])) : 0.0f;
+      if (s0 + i < nzp) out[i] = s0 + i < p.nz && aw[i] > 0.0f ? p.dtheta * (1.0f / aw[i]) : 0.0f;
   }
 }
 
@@ -203,8 +200,9 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
           if (Wj == 0.0f) continue;
           float scaled;  // g_vol * dtheta / sum_k W_k (cuda_kernels.cuh:283)
           if constexpr (TABLE) {
-            scaled = __ldg(gcol + s);
-            if (scaled == 0.0f) continue;
+            const float w = __ldg(gcol + s);
+            if (w == 0.0f) continue;
+            scaled = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix) * w;
           } else {
             const float gv = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix);
             if (gv == 0.0f) continue;
@@ -410,11 +408,12 @@ __global__ void k_taps_reduce(const float* __restrict__ partial, int nblk, int n
 }  // namespace
 
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
-                              const BPParams& p, float z0, float dzs, float* scale_table, cudaStream_t s) {
-  if (scale_table) {
+                              const BPParams& p, float z0, float dzs, float* scale_table, bool fill_table,
+                              cudaStream_t s) {
+  if (scale_table && fill_table) {
     dim3 g((unsigned)((p.nx + AN_TX - 1) / AN_TX), (unsigned)((p.ny + AN_TY - 1) / AN_TY),
            (unsigned)((p.nz + AN_ZS - 1) / AN_ZS));
-    k_bp_adjoint_scale<<<g, AN_TX * AN_TY, 0, s>>>(gvol, scale_table, sc, vz, zs, p, bp_adjoint_nzp(p.nz));
+    k_bp_adjoint_scale<<<g, AN_TX * AN_TY, 0, s>>>(scale_table, sc, vz, zs, p, bp_adjoint_nzp(p.nz));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

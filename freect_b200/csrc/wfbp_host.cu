@@ -332,9 +332,13 @@ const int kBpCandidates[][5] = {
     {12, 8, 4, 24, 32},  {16, 16, 4, 16, 16}, {16, 16, 8, 16, 16}, {16, 10, 4, 20, 16}, {16, 20, 4, 20, 16},
     {16, 20, 8, 20, 16}};
 
+// ext.bp_slab, when set, admits only configurations with slabs of that height
+bool slab_allowed(const wfbp_ctx* ctx, int slab) { return ctx->ext.bp_slab == 0 || ctx->ext.bp_slab == slab; }
+
 bool choose_bp_tile(wfbp_ctx* ctx, const std::vector<float>& table) {
   bp_reach(ctx, table);
   for (auto& c : kBpCandidates) {
+    if (!slab_allowed(ctx, c[4])) continue;
     BPTile b;
     if (size_bp_tile(ctx, c[0], c[1], c[2], c[3], c[4], &b)) {
       ctx->bpt = b;
@@ -450,6 +454,7 @@ namespace {
 // 303-317, float arithmetic), their transpose for the adjoint, and the device
 // tables; re-sizes the backprojection launch when the views are known.
 int setup_slices(wfbp_ctx* ctx) {
+  ctx->adj_scale_valid = false;
   ctx->nz = (int)ctx->z_native.size();
   ctx->nzr = (int)ctx->z_req.size();
   ctx->gp.n_slices_native = ctx->nz;
@@ -539,6 +544,8 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     e = *ext;
   }
   if (e.precision != WFBP_PRECISION_FP32 && e.precision != WFBP_PRECISION_MIXED) return WFBP_ERR_INVALID_ARG;
+  if (e.bp_slab != 0 && e.bp_slab != 16 && e.bp_slab != 32) return WFBP_ERR_INVALID_ARG;
+  if (e.adjoint_scale_table != 0 && e.adjoint_scale_table != -1) return WFBP_ERR_INVALID_ARG;
   if (e.filtered_layout != WFBP_LAYOUT_REFERENCE && e.filtered_layout != WFBP_LAYOUT_BACKPROJECTION)
     return WFBP_ERR_INVALID_ARG;
   if (e.precision == WFBP_PRECISION_MIXED && cg->num_detector_rows > 128) return WFBP_ERR_UNSUPPORTED;
@@ -717,6 +724,7 @@ WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table
   cudaFree(d_z);
   CUDA_TRY(ctx, e);
   ctx->view_table.assign(table, table + ctx->V);
+  ctx->adj_scale_valid = false;
   const int nrp = ctx->bpt.nrp;
   ctx->bp_tma_ok = choose_bp_tile(ctx, ctx->view_table);
   ctx->bpt.nrp = nrp;
@@ -758,7 +766,7 @@ WFBP_API int wfbp_bp_configs(const wfbp_ctx* ctx, wfbp_bp_config* out, int cap, 
   int k = 0;
   for (auto& c : kBpCandidates) {
     BPTile b;
-    if (!size_bp_tile(ctx, c[0], c[1], c[2], c[3], c[4], &b)) continue;
+    if (!slab_allowed(ctx, c[4]) || !size_bp_tile(ctx, c[0], c[1], c[2], c[3], c[4], &b)) continue;
     if (k < cap) {
       out[k].tile_x = c[0];
       out[k].tile_y = c[1];
@@ -789,8 +797,8 @@ WFBP_API int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* c) {
   if (!ctx->views_set) return fail(ctx, WFBP_ERR_STATE, "wfbp_set_bp_config: call wfbp_set_views first");
   BPTile b;
   const int nw = c->consumer_warps ? c->consumer_warps : BT_CWARPS;
-  const int slab = c->slab ? c->slab : 32;
-  if (!size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, nw, slab, &b))
+  const int slab = c->slab ? c->slab : (ctx->ext.bp_slab ? ctx->ext.bp_slab : 32);
+  if (!slab_allowed(ctx, slab) || !size_bp_tile(ctx, c->tile_x, c->tile_y, c->cols_per_step, nw, slab, &b))
     return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_set_bp_config: configuration " + std::to_string(c->tile_x) + "x" +
                                                std::to_string(c->tile_y) + "/" + std::to_string(c->cols_per_step) + "w" +
                                                std::to_string(nw) + "s" + std::to_string(slab) +
@@ -1035,6 +1043,7 @@ WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, floa
   const bool want_table = ctx->ext.adjoint_scale_table == 0 && n * sizeof(float) <= kAdjointTableBytes;
   if (want_table && n > ctx->adj_scale_n) {
     free_dev(ctx->d_adj_scale);
+    ctx->adj_scale_valid = false;
     if (cudaMalloc(&ctx->d_adj_scale, n * sizeof(float)) == cudaSuccess) {
       ctx->adj_scale_n = n;
     } else {
@@ -1045,7 +1054,8 @@ WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, floa
   }
   float* table = want_table && ctx->d_adj_scale && n <= ctx->adj_scale_n ? ctx->d_adj_scale : nullptr;
   CUDA_TRY(ctx, launch_bp_adjoint(g_native, g_filtered, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, z0, dzs,
-                                  table, (cudaStream_t)stream));
+                                  table, table && !ctx->adj_scale_valid, (cudaStream_t)stream));
+  if (table) ctx->adj_scale_valid = true;
   return WFBP_OK;
 }
 

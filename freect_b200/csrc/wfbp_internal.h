@@ -130,8 +130,9 @@ struct wfbp_ctx {
   float* d_radj_w = nullptr;
   float* d_tg_partial = nullptr;    // per-CTA partial tap gradients
   size_t tg_partial_n = 0;
-  float* d_adj_scale = nullptr;     // backprojection adjoint: per-(voxel, theta~) gradient scale
+  float* d_adj_scale = nullptr;     // backprojection adjoint: per-(voxel, theta~) weight dtheta / sum_k W_k
   size_t adj_scale_n = 0;
+  bool adj_scale_valid = false;     // the table matches the current views and slices
 
   // mixed precision: Toeplitz operand planes for the tensor-core filter
   int tc_kp = 0, tc_np = 0, tc_bn = 0;
@@ -222,8 +223,11 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // scale, or null (then the gather recomputes the weight sums itself)
 // slice stride of the backprojection adjoint's scale table [P/2][ny][nx][nzp]
 inline int bp_adjoint_nzp(int nz) { return (nz + 3) / 4 * 4; }
+// scale_table: [P/2][ny][nx][nzp] weights dtheta / sum_k W_k, filled first
+// when fill_table is set; nullptr: the gather recomputes the weight sums
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
-                              const BPParams& p, float z0, float dzs, float* scale_table, cudaStream_t s);
+                              const BPParams& p, float z0, float dzs, float* scale_table, bool fill_table,
+                              cudaStream_t s);
 cudaError_t launch_thicken_adjoint(const float* gvol, float* gvn, const int* off, const int* ridx, const float* w,
                                    int nxy, int nz, cudaStream_t s);
 cudaError_t launch_rebin_adj_cols(const float* bidx, int nch, int q8, int* cnt, int* cidx, float* cw, int maxl,

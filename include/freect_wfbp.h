@@ -177,10 +177,13 @@ typedef struct wfbp_ext {
   int n_user_taps;
   int tex_weights;            /* 1: rebin uses 8-bit fractional bilinear weights like the
                                  texture unit the reference samples through (cuda_kernels.cuh:36) */
-  int bp_slab;                /* 0 = default; native slices per backprojection slab */
+  int bp_slab;                /* 0 = any; 16 or 32: only backprojection configurations whose
+                                 slabs hold that many native slices (wfbp_bp_config.slab) */
   int filtered_layout;        /* wfbp_layout of the stage API (default REFERENCE) */
   int adjoint_scale_table;    /* 0: the backprojection adjoint keeps a per-(voxel, half-turn angle)
-                                 gradient scale table when it fits in 6 GB; -1: never (recompute) */
+                                 weight table dtheta / sum_k W_k when it fits in 6 GB, computed on
+                                 the first adjoint call after the views or slices change;
+                                 -1: never (the adjoint recomputes the weight sums) */
   int reserved[5];
 } wfbp_ext;
 

@@ -114,6 +114,41 @@ def test_backproject_adjoint(orc, tiny, which, table_mode):
     assert np.linalg.norm(gf - ref) < 1e-3 * np.linalg.norm(ref)
 
 
+def test_backproject_adjoint_table_reuse(tiny):
+    # the weight table depends on the geometry alone: one context computes it
+    # once and reuses it for every gradient, and again after its views or
+    # slices change; each result must match a context that recomputes the
+    # weight sums
+    ctx_t, cg, tube, table = make(tiny, adjoint_scale_table=0)
+    ctx_r, _, _, _ = make(tiny, adjoint_scale_table=-1)
+    d = ctx_t.dims
+    rng = np.random.default_rng(6)
+
+    def check():
+        y = dev(rng.standard_normal((d.n_slices_native, d.ny, d.nx)))
+        a = torch.empty((d.n_views, d.n_rows, d.n_channels), dtype=torch.float32, device=DEV)
+        b = torch.empty_like(a)
+        ctx_t.backproject_adjoint(y, a)
+        ctx_r.backproject_adjoint(y, b)
+        torch.cuda.synchronize()
+        a, b = a.cpu().numpy(), b.cpu().numpy()
+        assert np.abs(a).max() > 0
+        assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max()
+
+    check()
+    check()
+    table2 = (table + 0.37).astype(np.float32)  # views moved by a fraction of a slice
+    ctx_t.set_views(tube, table2)
+    ctx_r.set_views(tube, table2)
+    check()
+    nat, req = ctx_t.slices()
+    for c in (ctx_t, ctx_r):
+        c.set_slices(nat + 0.21, req + 0.21)
+    check()
+    with pytest.raises(wfbp.WfbpError):
+        wfbp.Context(cg, tiny.recon_config(), wfbp.make_ext(adjoint_scale_table=2), device=0)
+
+
 def test_thicken_adjoint(orc, tiny):
     ctx, cg, _, _ = make(tiny)
     d = ctx.dims

@@ -325,8 +325,19 @@ def test_bp_configs_identical_and_tuner(orc, tmp_path, precision):
     assert np.isfinite(vols[0]).any()
     for c, v in zip(cfgs[1:], vols[1:]):
         assert np.array_equal(v, vols[0], equal_nan=True), c.key()
+    assert {c.slab for c in cfgs} == {16, 32}
     with pytest.raises(wfbp.WfbpError):
         ctx.set_bp_config((16, 16, 16))
+    # ext.bp_slab admits only the configurations with that slab height
+    c16 = wfbp.Context(cg, spec.recon_config(), wfbp.make_ext(precision=precision, filter_window=spec.window,
+                                                             filtered_layout=T.LAYOUT_BACKPROJECTION, bp_slab=16),
+                       device=0)
+    c16.set_views(tube, table)
+    assert c16.bp_config().slab == 16 and {c.slab for c in c16.bp_configs()} == {16}
+    with pytest.raises(wfbp.WfbpError):
+        c16.set_bp_config((16, 16, 4, 16, 32))
+    with pytest.raises(wfbp.WfbpError):
+        wfbp.Context(cg, spec.recon_config(), wfbp.make_ext(bp_slab=8), device=0)
     path = str(tmp_path / "tune.json")
     vn = ctx.alloc("native")
     r1 = autotune.tune_backprojection(ctx, filt, vn, row_scales=sc, path=path)
