@@ -33,6 +33,8 @@
 
 #include <cuda.h>
 
+#include <algorithm>
+
 #include <type_traits>
 
 namespace {
@@ -427,7 +429,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
 
 // One tile per CTA: grid (tiles x, tiles y, SL-slice slabs).
 template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
-__global__ void __launch_bounds__((NW + 1) * 32, 1)
+__global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
 k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
          const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
          BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err) {
@@ -443,7 +445,7 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
 // the next work item (scan, tile x, tile y, slab) from a global counter until
 // the list is exhausted. Items are listed by decreasing estimated cost.
 template <typename T, int CPW, int CU, int NW, int SL>
-__global__ void __launch_bounds__((NW + 1) * 32, 1)
+__global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
 k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items, int n_items,
                unsigned* __restrict__ next, int* __restrict__ err) {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -465,6 +467,17 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
   }
 }
 
+// Dynamic shared memory of `smem` bytes and the whole unified L1 / shared
+// memory as shared memory, so that as many CTAs fit on an SM as the
+// registers allow.
+template <typename K>
+cudaError_t prepare_kernel(K* kern, int smem) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+  return e;
+}
+
 template <typename T, int CPW, int CU, int NW, int SL>
 cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
@@ -476,14 +489,12 @@ cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* v
   constexpr int threads = (NW + 1) * 32;
   cudaError_t e;
   if (count) {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, SL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bt.smem_bytes);
+    e = prepare_kernel(k_bp_tma<T, CPW, CU, NW, SL, true>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
     k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
                                                                          count, err);
   } else {
-    e = cudaFuncSetAttribute(k_bp_tma<T, CPW, CU, NW, SL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bt.smem_bytes);
+    e = prepare_kernel(k_bp_tma<T, CPW, CU, NW, SL, false>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
     k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
                                                                           count, err);
@@ -494,17 +505,26 @@ cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* v
 template <typename T, int CPW, int CU, int NW, int SL>
 cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
                              int smem_bytes, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(k_bp_tma_batch<T, CPW, CU, NW, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       smem_bytes);
+  auto kern = k_bp_tma_batch<T, CPW, CU, NW, SL>;
+  cudaError_t e = prepare_kernel(kern, smem_bytes);
   if (e != cudaSuccess) return e;
-  k_bp_tma_batch<T, CPW, CU, NW, SL><<<grid, (NW + 1) * 32, smem_bytes, s>>>(scans, items, n_items, next, err);
+  // grid = SMs; persistent CTAs: as many per SM as fit
+  int per_sm = 1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NW + 1) * 32, smem_bytes);
+  if (e != cudaSuccess) return e;
+  grid = std::max(1, std::min(grid * std::max(per_sm, 1), n_items));
+  kern<<<grid, (NW + 1) * 32, smem_bytes, s>>>(scans, items, n_items, next, err);
   return cudaGetLastError();
 }
 
 // The instantiated launch shapes: (columns per warp, columns per pass, consumer warps, slab slices).
+// With 8 consumer warps two CTAs share an SM (registers and shared memory
+// permitting), so one CTA's ring refills and tile tails overlap the other's
+// updates.
 #define WFBP_BP_SHAPES(X)                                                                                        \
   X(16, 4, 16, 32) X(16, 8, 16, 32) X(8, 4, 16, 32) X(8, 8, 16, 32) X(4, 4, 16, 32) X(8, 4, 20, 32) X(8, 8, 20, 32) \
-  X(4, 4, 24, 32) X(16, 4, 16, 16) X(16, 8, 16, 16) X(8, 4, 20, 16) X(16, 4, 20, 16) X(16, 8, 20, 16)
+  X(4, 4, 24, 32) X(16, 4, 16, 16) X(16, 8, 16, 16) X(8, 4, 20, 16) X(16, 4, 20, 16) X(16, 8, 20, 16)           \
+  X(16, 4, 8, 32) X(16, 8, 8, 32) X(16, 4, 8, 16) X(16, 8, 8, 16)
 
 template <typename T>
 cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,

@@ -330,7 +330,8 @@ const int kBpCandidates[][5] = {
     {16, 16, 4, 16, 32}, {16, 16, 8, 16, 32}, {16, 8, 4, 16, 32},  {16, 8, 8, 16, 32},  {8, 16, 4, 16, 32},
     {8, 16, 8, 16, 32},  {8, 8, 4, 16, 32},   {16, 10, 4, 20, 32}, {16, 10, 8, 20, 32}, {10, 16, 4, 20, 32},
     {12, 8, 4, 24, 32},  {16, 16, 4, 16, 16}, {16, 16, 8, 16, 16}, {16, 10, 4, 20, 16}, {16, 20, 4, 20, 16},
-    {16, 20, 8, 20, 16}};
+    {16, 20, 8, 20, 16}, {16, 8, 4, 8, 32},   {8, 16, 4, 8, 32},   {16, 8, 8, 8, 32},   {8, 16, 8, 8, 32},
+    {16, 8, 4, 8, 16},   {16, 8, 8, 8, 16},   {8, 16, 8, 8, 16}};
 
 // ext.bp_slab, when set, admits only configurations with slabs of that height
 bool slab_allowed(const wfbp_ctx* ctx, int slab) { return ctx->ext.bp_slab == 0 || ctx->ext.bp_slab == slab; }
