@@ -34,6 +34,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include <type_traits>
 
@@ -99,6 +100,45 @@ __device__ __forceinline__ void bp_init_barriers(uint8_t* smem, int nw) {
   __syncthreads();
 }
 
+// Fused thickening of one slab (ThickFuse): for every requested slice r whose
+// native slices all lie in slab bz, each group of SL lanes (lane = slice
+// s0 + lane % SL) gathers its native values with shuffles, in the CSR order
+// and with the same FMA chain and division as k_thicken, so the result is
+// bit-identical to thickening the written native volume. Lane c of a group
+// writes column c of the group. All 32 lanes of the warp take part.
+template <int CPW, int SL, int CPG>
+__device__ __forceinline__ void bp_fused_thicken(const ThickFuse& tf, const float (&vals)[CPG], bool zero, int bz,
+                                                 int s0, int warp, int lane, int ix0, int iy0, const BPTile& bt,
+                                                 const BPParams& p) {
+  const int2 rr = tf.slab_req[bz];
+  const int grp = lane / SL, ll = lane % SL;
+  const int tt = warp * CPW + grp * CPG + min(ll, CPG - 1);
+  const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
+  const bool wr = ll < CPG && ix < p.nx && iy < p.ny;
+  const size_t plane = (size_t)p.nx * p.ny, vox = (size_t)iy * p.nx + ix;
+  for (int k = rr.x; k < rr.y; k++) {
+    const int r = __ldg(tf.req + k);
+    float v = 0.0f;
+    if (!zero) {
+      float acc[CPG];
+#pragma unroll
+      for (int c = 0; c < CPG; c++) acc[c] = 0.0f;
+      const int a = __ldg(tf.off + r), b = __ldg(tf.off + r + 1);
+      for (int t = a; t < b; t++) {
+        const int src = grp * SL + (__ldg(tf.idx + t) - s0);
+        const float wt = __ldg(tf.w + t);
+#pragma unroll
+        for (int c = 0; c < CPG; c++) acc[c] = fmaf(wt, __shfl_sync(0xffffffffu, vals[c], src), acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < CPG; c++)
+        if (c == ll) v = acc[c];
+    }
+    // a tile outside the FOV has native values +0, and k_thicken gives +0 / ws = +0
+    if (wr) tf.out[(size_t)r * plane + vox] = zero ? 0.0f : v / __ldg(tf.ws + r);
+  }
+}
+
 // One column tile (bt.tx x bt.ty columns, 32 slices from slab bz) of one scan.
 // `ring` counts the theta~ steps this CTA has run through its two-stage
 // ring before this tile (stage = ring & 1, phase = (ring >> 1) & 1), so a
@@ -113,7 +153,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
                                         const float* __restrict__ view_z, const float* __restrict__ zslices,
                                         const BPParams& p, const BPTile& bt, int bx, int by, int bz,
                                         unsigned long long* __restrict__ count, int* __restrict__ err, uint8_t* smem,
-                                        uint32_t ring) {
+                                        uint32_t ring, const ThickFuse& tf) {
   constexpr bool HALF = !std::is_same<T, float>::value;
   constexpr int NPW = CPW / 2;  // column pairs per warp
   // SL = 32: the warp's 32 lanes are 32 slices of each of its CPW columns.
@@ -166,6 +206,10 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
           const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
           if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = 0.0f;
         }
+      }
+      if (tf.out && warp < NW) {
+        const float none[CPG] = {};
+        bp_fused_thicken<CPW, SL, CPG>(tf, none, true, bz, s0, warp, lane, ix0, iy0, bt, p);
       }
       return 0;
     }
@@ -419,6 +463,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = vacc[c];
     }
   }
+  if (tf.out) bp_fused_thicken<CPW, SL, CPG>(tf, vacc, false, bz, s0, warp, lane, ix0, iy0, bt, p);
   if (COUNT) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
@@ -432,13 +477,13 @@ template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
 __global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
 k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
          const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
-         BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err) {
+         BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {
   // the dynamic shared memory is the only shared memory of this kernel, so
   // it starts at the (128-byte aligned) base of the CTA's window
   extern __shared__ __align__(128) uint8_t smem[];
   bp_init_barriers(smem, NW);
   bp_tile<T, CPW, CU, NW, SL, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
-                                 bt.zb0 + blockIdx.z, count, err, smem, 0u);
+                                 bt.zb0 + blockIdx.z, count, err, smem, 0u, tf);
 }
 
 // Persistent launch over the column tiles of several scans: each CTA takes
@@ -462,7 +507,8 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
     const BPParams p = sd->p;
     const BPTile bt = sd->bt;
     ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
-                                                 sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring);
+                                                 sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring,
+                                                 sd->tf);
     __syncthreads();  // the tile's shared memory and words[9] are free again
   }
 }
@@ -481,7 +527,7 @@ cudaError_t prepare_kernel(K* kern, int smem) {
 template <typename T, int CPW, int CU, int NW, int SL>
 cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
-                       unsigned long long* count, int* err, cudaStream_t s) {
+                       unsigned long long* count, int* err, cudaStream_t s, const ThickFuse& tf) {
   const int nslab = (p.nz + SL - 1) / SL;
   if (bt.zb0 < 0 || bt.zb0 >= nslab || bt.nzb < 0 || bt.zb0 + bt.nzb > nslab) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((p.nx + bt.tx - 1) / bt.tx), (unsigned)((p.ny + bt.ty - 1) / bt.ty),
@@ -492,12 +538,12 @@ cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* v
     e = prepare_kernel(k_bp_tma<T, CPW, CU, NW, SL, true>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
     k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
-                                                                         count, err);
+                                                                         count, err, tf);
   } else {
     e = prepare_kernel(k_bp_tma<T, CPW, CU, NW, SL, false>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
     k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
-                                                                          count, err);
+                                                                          count, err, tf);
   }
   return cudaGetLastError();
 }
@@ -529,10 +575,10 @@ cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items
 template <typename T>
 cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
                         const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
-                        unsigned long long* count, int* err, cudaStream_t s) {
+                        unsigned long long* count, int* err, cudaStream_t s, const ThickFuse& tf) {
   const int cpw = bt.tx * bt.ty / bt.nw;
 #define WFBP_ONE(C, U, N, S) \
-  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return launch_one<T, C, U, N, S>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return launch_one<T, C, U, N, S>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s, tf);
   WFBP_BP_SHAPES(WFBP_ONE)
 #undef WFBP_ONE
   return cudaErrorInvalidValue;
@@ -573,13 +619,17 @@ cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, 
 
 cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
                                    const float2* sc, const float* vz, const float* zs, const BPParams& p,
-                                   const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s) {
+                                   const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s,
+                                   const ThickFuse* tf) {
   if (!bp_tma_supported(bt)) return cudaErrorInvalidValue;
   CUtensorMap map;
   cudaError_t e = bp_tma_encode_map(D, elem_half2, p, bt, &map);
   if (e != cudaSuccess) return e;
-  if (elem_half2) return launch_elem<uint32_t>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
-  return launch_elem<float>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s);
+  ThickFuse none;
+  memset(&none, 0, sizeof(none));
+  const ThickFuse& f = tf ? *tf : none;
+  if (elem_half2) return launch_elem<uint32_t>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s, f);
+  return launch_elem<float>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s, f);
 }
 
 cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,

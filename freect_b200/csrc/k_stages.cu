@@ -226,8 +226,8 @@ cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps,
 // the per-voxel sums run in the same slice order.
 __global__ void k_thicken(const float* __restrict__ vn, float* __restrict__ out, const int* __restrict__ off,
                           const int* __restrict__ idx, const float* __restrict__ w, const float* __restrict__ ws,
-                          int nxy) {
-  const int r = blockIdx.y;
+                          int nxy, const int* __restrict__ list) {
+  const int r = list ? __ldg(list + blockIdx.y) : (int)blockIdx.y;
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
   if (px >= nxy) return;
   const int a = off[r], b = off[r + 1];
@@ -237,9 +237,10 @@ __global__ void k_thicken(const float* __restrict__ vn, float* __restrict__ out,
 }
 
 cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
-                           const float* ws, int nxy, int nzr, cudaStream_t s) {
+                           const float* ws, int nxy, int nzr, cudaStream_t s, const int* list) {
+  if (nzr < 1) return cudaSuccess;
   dim3 grid((unsigned)((nxy + 255) / 256), (unsigned)nzr);
-  k_thicken<<<grid, 256, 0, s>>>(vn, out, off, idx, w, ws, nxy);
+  k_thicken<<<grid, 256, 0, s>>>(vn, out, off, idx, w, ws, nxy, list);
   return cudaGetLastError();
 }
 

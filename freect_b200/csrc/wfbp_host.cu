@@ -169,6 +169,9 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_thick_idx);
   free_dev(ctx->d_thick_w);
   free_dev(ctx->d_thick_ws);
+  free_dev(ctx->d_fuse_slab);
+  free_dev(ctx->d_fuse_req);
+  free_dev(ctx->d_fuse_bnd);
   free_dev(ctx->d_bplanes);
   free_dev(ctx->d_err);
   free_dev(ctx->d_thickT_off);
@@ -456,6 +459,7 @@ namespace {
 // tables; re-sizes the backprojection launch when the views are known.
 int setup_slices(wfbp_ctx* ctx) {
   ctx->adj_scale_valid = false;
+  ctx->fuse_slab = 0;
   ctx->nz = (int)ctx->z_native.size();
   ctx->nzr = (int)ctx->z_req.size();
   ctx->gp.n_slices_native = ctx->nz;
@@ -934,7 +938,7 @@ int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales
 }
 
 int do_backproject(wfbp_ctx* ctx, const void* filtered, const float* scales, float* vol,
-                   unsigned long long* update_count, int layout, void* stream) {
+                   unsigned long long* update_count, int layout, void* stream, const ThickFuse* tf = nullptr) {
   const cudaStream_t s = (cudaStream_t)stream;
   BPParams p = bp_params(ctx);
   const bool mixed = ctx->ext.precision == WFBP_PRECISION_MIXED;
@@ -943,7 +947,7 @@ int do_backproject(wfbp_ctx* ctx, const void* filtered, const float* scales, flo
     if (!ctx->bp_tma_ok)
       return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_backproject: no backprojection-layout launch fits this geometry");
     CUDA_TRY(ctx, launch_backproject_tma(filtered, mixed ? 1 : 0, scales, vol, ctx->d_view_sc, ctx->d_view_z,
-                                         ctx->d_z_native, p, ctx->bpt, update_count, ctx->d_err, s));
+                                         ctx->d_z_native, p, ctx->bpt, update_count, ctx->d_err, s, tf));
     return WFBP_OK;
   }
   if (mixed)
@@ -1128,6 +1132,62 @@ int ensure_scratch(wfbp_ctx* ctx) {
   if (!ctx->s_scales && scal) CUDA_TRY(ctx, cudaMalloc(&ctx->s_scales, scal));
   return WFBP_OK;
 }
+
+// Lists of the fused thickening for the current slab height: requested slices
+// whose thickening CSR row lies in one slab (by slab), and the others.
+int prepare_fuse(wfbp_ctx* ctx) {
+  const int SL = ctx->bpt.slab;
+  if (ctx->fuse_slab == SL) return WFBP_OK;
+  const int nslab = (ctx->nz + SL - 1) / SL;
+  std::vector<std::vector<int>> by(nslab);
+  ctx->fuse_bnd_h.clear();
+  for (int r = 0; r < ctx->nzr; r++) {
+    const int a = ctx->thick_off[r], b = ctx->thick_off[r + 1];
+    if (a < b && ctx->thick_idx[a] / SL == ctx->thick_idx[b - 1] / SL) by[ctx->thick_idx[a] / SL].push_back(r);
+    else ctx->fuse_bnd_h.push_back(r);
+  }
+  ctx->fuse_slab_h.assign(nslab, make_int2(0, 0));
+  ctx->fuse_req_h.clear();
+  for (int b = 0; b < nslab; b++) {
+    ctx->fuse_slab_h[b].x = (int)ctx->fuse_req_h.size();
+    ctx->fuse_req_h.insert(ctx->fuse_req_h.end(), by[b].begin(), by[b].end());
+    ctx->fuse_slab_h[b].y = (int)ctx->fuse_req_h.size();
+  }
+  free_dev(ctx->d_fuse_slab);
+  free_dev(ctx->d_fuse_req);
+  free_dev(ctx->d_fuse_bnd);
+  auto put = [&](auto** dst, const auto& v) -> cudaError_t {
+    const size_t bytes = sizeof(v[0]) * std::max<size_t>(v.size(), 1);
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+  };
+  CUDA_TRY(ctx, put(&ctx->d_fuse_slab, ctx->fuse_slab_h));
+  CUDA_TRY(ctx, put(&ctx->d_fuse_req, ctx->fuse_req_h));
+  CUDA_TRY(ctx, put(&ctx->d_fuse_bnd, ctx->fuse_bnd_h));
+  ctx->n_fuse_bnd = (int)ctx->fuse_bnd_h.size();
+  ctx->fuse_slab = SL;
+  return WFBP_OK;
+}
+
+ThickFuse make_fuse(const wfbp_ctx* ctx, float* out) {
+  ThickFuse f;
+  f.out = out;
+  f.slab_req = ctx->d_fuse_slab;
+  f.req = ctx->d_fuse_req;
+  f.off = ctx->d_thick_off;
+  f.idx = ctx->d_thick_idx;
+  f.w = ctx->d_thick_w;
+  f.ws = ctx->d_thick_ws;
+  return f;
+}
+
+// The requested slices the fused write-back leaves out (they straddle slabs).
+int thicken_boundary(wfbp_ctx* ctx, const float* vn, float* vol, cudaStream_t s) {
+  CUDA_TRY(ctx, launch_thicken(vn, vol, ctx->d_thick_off, ctx->d_thick_idx, ctx->d_thick_w, ctx->d_thick_ws,
+                               ctx->nx * ctx->ny, ctx->n_fuse_bnd, s, ctx->d_fuse_bnd));
+  return WFBP_OK;
+}
 }  // namespace
 
 namespace {
@@ -1149,12 +1209,19 @@ int run_stages(wfbp_ctx* ctx, const float* raw, float* vol, void* stream, cudaEv
   if (!st) st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, stream);
   nvtxRangePop();
   if (ev) cudaEventRecord(ev[2], s);
+  // with the backprojection layout the thickening of the slices inside one
+  // slab runs in the backprojection's write-back; the rest follow
+  const bool fuse = lay == WFBP_LAYOUT_BACKPROJECTION;
+  if (!st && fuse) st = prepare_fuse(ctx);
+  const ThickFuse tf = make_fuse(ctx, vol);
   nvtxRangePushA("backproject");
-  if (!st) st = do_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, lay, stream);
+  if (!st)
+    st = do_backproject(ctx, ctx->s_filtered, ctx->s_scales, ctx->s_vol_native, nullptr, lay, stream,
+                        fuse ? &tf : nullptr);
   nvtxRangePop();
   if (ev) cudaEventRecord(ev[3], s);
   nvtxRangePushA("thicken");
-  if (!st) st = wfbp_thicken(ctx, ctx->s_vol_native, vol, stream);
+  if (!st) st = fuse ? thicken_boundary(ctx, ctx->s_vol_native, vol, s) : wfbp_thicken(ctx, ctx->s_vol_native, vol, stream);
   nvtxRangePop();
   if (ev) cudaEventRecord(ev[4], s);
   nvtxRangePop();
@@ -1201,20 +1268,20 @@ int rebin_reach_views(const wfbp_ctx* ctx) {
 
 // wfbp_run_host as a pipeline over chunks of readings: the host-to-device
 // copy of chunk c+1 (own stream) overlaps the rebin and filter of chunk c and
-// the backprojection of every 32-slice slab whose views are all filtered
-// (the slab's table-position reach, the z cull of cuda_kernels.cuh:232); the
-// last slabs, the thickening and the copy back follow. Same kernels, same
-// per-voxel sums: the volume equals wfbp_run's.
+// the backprojection of every slab whose views are all filtered (the slab's
+// table-position reach, the z cull of cuda_kernels.cuh:232). The
+// backprojection thickens the requested slices inside its slabs as it writes
+// them, and with a pinned destination those are copied back while later
+// slabs run; the slices that straddle slabs are thickened and copied last.
+// Same kernels, same per-voxel sums: the volume equals wfbp_run's.
 int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cudaStream_t s) {
-  wfbp_dims d;
-  wfbp_query(ctx, &d);
   int st = ensure_scratch(ctx);
   if (st) return st;
   const int lay = WFBP_LAYOUT_BACKPROJECTION;
   constexpr int kChunks = 8;
   if (!ctx->s_copy) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
   if (ctx->ev_copy.empty()) {
-    ctx->ev_copy.resize(kChunks + 1);
+    ctx->ev_copy.resize(kChunks + 2);  // chunk copies, caller order, fused slices ready
     for (auto& e : ctx->ev_copy) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   const int V = ctx->V, G = ctx->G;
@@ -1248,6 +1315,27 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   std::vector<char> done(nslab, 0);
   const BPParams p = bp_params(ctx);
   const bool mixed = ctx->ext.precision == WFBP_PRECISION_MIXED;
+  // fused thickening: the requested slices inside a slab are final when its
+  // launch ends; with a pinned destination they are copied back right away
+  // (on the copy stream, behind the launch's event) while later slabs run
+  if ((st = prepare_fuse(ctx))) return st;
+  const ThickFuse tf = make_fuse(ctx, ctx->s_vol);
+  cudaPointerAttributes pa;
+  const bool pinned = cudaPointerGetAttributes(&pa, vol_host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  const size_t plane = (size_t)ctx->nx * ctx->ny;
+  auto copy_back = [&](const std::vector<int>& rs, cudaStream_t cs) -> int {
+    // one copy per run of consecutive requested slices
+    for (size_t a = 0; a < rs.size();) {
+      size_t b = a + 1;
+      while (b < rs.size() && rs[b] == rs[b - 1] + 1) b++;
+      CUDA_TRY(ctx, cudaMemcpyAsync(vol_host + (size_t)rs[a] * plane, ctx->s_vol + (size_t)rs[a] * plane,
+                                    sizeof(float) * plane * (b - a), cudaMemcpyDeviceToHost, cs));
+      a = b;
+    }
+    return WFBP_OK;
+  };
+  std::vector<char> copied(ctx->nzr, 0);
   auto launch_ready = [&](int filtered_upto) -> int {
     for (int sl = 0; sl < nslab;) {
       if (done[sl] || need[sl] >= filtered_upto) {
@@ -1261,8 +1349,20 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
       bt.nzb = e - sl;
       CUDA_TRY(ctx, launch_backproject_tma(ctx->s_filtered, mixed ? 1 : 0, ctx->s_scales, ctx->s_vol_native,
                                            ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, bt, nullptr,
-                                           ctx->d_err, s));
+                                           ctx->d_err, s, &tf));
       for (int k = sl; k < e; k++) done[k] = 1;
+      if (pinned) {
+        std::vector<int> rs;
+        for (int k = sl; k < e; k++)
+          for (int i = ctx->fuse_slab_h[k].x; i < ctx->fuse_slab_h[k].y; i++) rs.push_back(ctx->fuse_req_h[i]);
+        if (!rs.empty()) {
+          CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[kChunks + 1], s));
+          CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_copy, ctx->ev_copy[kChunks + 1], 0));
+          const int cst = copy_back(rs, ctx->s_copy);
+          if (cst) return cst;
+          for (int r : rs) copied[r] = 1;
+        }
+      }
       sl = e;
     }
     return WFBP_OK;
@@ -1276,8 +1376,12 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     if ((st = launch_ready(ve))) return st;
   }
   if ((st = launch_ready(V + 1))) return st;
-  if ((st = wfbp_thicken(ctx, ctx->s_vol_native, ctx->s_vol, s))) return st;
-  CUDA_TRY(ctx, cudaMemcpyAsync(vol_host, ctx->s_vol, d.volume_bytes, cudaMemcpyDeviceToHost, s));
+  if ((st = thicken_boundary(ctx, ctx->s_vol_native, ctx->s_vol, s))) return st;
+  std::vector<int> rest;
+  for (int r = 0; r < ctx->nzr; r++)
+    if (!copied[r]) rest.push_back(r);
+  if ((st = copy_back(rest, s))) return st;
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->s_copy));
   CUDA_TRY(ctx, cudaStreamSynchronize(s));
   return wfbp_check_device_status(ctx);
 }

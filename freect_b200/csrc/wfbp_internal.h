@@ -120,6 +120,14 @@ struct wfbp_ctx {
   int* d_thick_idx = nullptr;
   float* d_thick_w = nullptr;
   float* d_thick_ws = nullptr;      // [nzr] sum of weights
+  // fused thickening lists for slabs of fuse_slab native slices (0: not built)
+  int fuse_slab = 0;
+  int2* d_fuse_slab = nullptr;      // [slabs] range into d_fuse_req
+  int* d_fuse_req = nullptr;        // interior requested slices by slab
+  int* d_fuse_bnd = nullptr;        // boundary requested slices
+  int n_fuse_bnd = 0;
+  std::vector<int2> fuse_slab_h;    // host copies
+  std::vector<int> fuse_req_h, fuse_bnd_h;
   int* d_thickT_off = nullptr;      // transposed CSR over native slices: (requested slice, w / sum w)
   int* d_thickT_idx = nullptr;
   float* d_thickT_w = nullptr;
@@ -196,6 +204,21 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
                              const TcOutArgs& out, int* err, cudaStream_t s, int mb = 0, int me = -1);
 cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps, long rows, int nch, int nr, int nrp,
                                  cudaStream_t s);
+// Thickening fused into the TMA backprojection's write-back: a requested
+// slice whose native slices (the thickening CSR row) all lie in one slab is
+// formed from that slab's registers and written to `out`; the other
+// ("boundary") requested slices are thickened afterwards from the native
+// volume. out == nullptr: no fusion.
+struct ThickFuse {
+  float* out;            // requested volume [nzr][ny][nx]
+  const int2* slab_req;  // per slab: [begin, end) into req
+  const int* req;        // requested slice indices, grouped by slab, ascending
+  const int* off;        // thickening CSR (the same arrays k_thicken reads)
+  const int* idx;
+  const float* w;
+  const float* ws;
+};
+
 // One scan of a persistent (batched) backprojection launch, in device memory.
 struct alignas(64) BpScan {
   CUtensorMap map;              // filtered rows [V][nch][nrp], box {nrp, W, 1}
@@ -206,6 +229,7 @@ struct alignas(64) BpScan {
   const float2* view_sc;
   const float* view_z;
   const float* zslices;
+  ThickFuse tf;                 // fused thickening (tf.out == nullptr: none)
 };
 cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map);
 cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,
@@ -215,12 +239,12 @@ size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);
 bool bp_tma_supported(const BPTile& bt);
 cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
                                    const float2* sc, const float* vz, const float* zs, const BPParams& p,
-                                   const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s);
+                                   const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s,
+                                   const ThickFuse* tf = nullptr);
 int tc_choose_bn(int nch);
+// requested slices list[0..nzr) (list == nullptr: 0..nzr-1)
 cudaError_t launch_thicken(const float* vn, float* out, const int* off, const int* idx, const float* w,
-                           const float* ws, int nxy, int nzr, cudaStream_t s);
-// scale_table: [P/2][nz][ny][nx] scratch for the per-(voxel, theta~) gradient
-// scale, or null (then the gather recomputes the weight sums itself)
+                           const float* ws, int nxy, int nzr, cudaStream_t s, const int* list = nullptr);
 // slice stride of the backprojection adjoint's scale table [P/2][ny][nx][nzp]
 inline int bp_adjoint_nzp(int nz) { return (nz + 3) / 4 * 4; }
 // scale_table: [P/2][ny][nx][nzp] weights dtheta / sum_k W_k, filled first

@@ -200,6 +200,50 @@ def test_run_host_matches_run(orc, tiny, which, precision):
     for _ in range(2):
         host = ctx.run_host(pinned)
         assert np.array_equal(host, vol.cpu().numpy(), equal_nan=True)
+    # a pinned destination: the slices thickened inside a slab are copied
+    # back while later slabs run
+    out = torch.full(tuple(vol.shape), -7.0, dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        ctx.run_host(pinned, out)
+        assert np.array_equal(out.numpy(), vol.cpu().numpy(), equal_nan=True)
+
+
+@pytest.mark.parametrize("precision", [T.PRECISION_FP32, T.PRECISION_MIXED])
+def test_run_fused_thickening_matches_stages(orc, precision):
+    # wfbp_run thickens the requested slices that lie inside one slab in the
+    # backprojection's write-back and the slices that straddle slabs
+    # afterwards; the volume must equal the stage chain's (backproject, then
+    # wfbp_thicken) bit for bit, for both slab heights
+    spec = scans.small(seed=11)
+    spec.nx = spec.ny = 64
+    spec.n_slices = 50
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    ctx = wfbp.Context(cg, spec.recon_config(), wfbp.make_ext(precision=precision, filter_window=spec.window,
+                                                             filtered_layout=T.LAYOUT_BACKPROJECTION), device=0)
+    ctx.set_views(tube, table)
+    assert ctx.dims.n_slices_native > 64
+    reb, filt, sc, vn = ctx.alloc("rebinned"), ctx.alloc("filtered"), ctx.alloc("row_scales"), ctx.alloc("native")
+    staged, fused = ctx.alloc("volume"), ctx.alloc("volume")
+    seen = set()
+    for c in ctx.bp_configs():
+        if c.slab in seen:
+            continue
+        seen.add(c.slab)
+        ctx.set_bp_config(c)
+        ctx.rebin(dev(raw), reb)
+        ctx.filter(reb, filt, sc)
+        ctx.backproject(filt, vn, sc)
+        ctx.thicken(vn, staged)
+        fused.fill_(-7.0)
+        ctx.run(dev(raw), fused)
+        torch.cuda.synchronize()
+        ctx.check_device_status()
+        a, b = staged.cpu().numpy(), fused.cpu().numpy()
+        assert np.isfinite(a).any()
+        assert np.array_equal(a, b, equal_nan=True), c.key()
+    assert seen == {16, 32}
 
 
 def test_state_and_argument_errors(tiny):
