@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-slices", type=int, default=1)
     ap.add_argument("--no-tune", action="store_true", help="keep the default backprojection configuration")
     ap.add_argument("--no-hu", action="store_true", help="skip the HU check against the FP64 oracle")
+    ap.add_argument("--bp-config", default=None,
+                    help="fixed backprojection configuration, e.g. 16x20/8w20s16 (no tuning)")
     return ap.parse_args()
 
 
@@ -604,20 +606,20 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
         ctx.thicken(vn, vol)
 
     tuned = None
-    if not args.no_tune:
+    if not args.no_tune and not args.bp_config:
         # backprojection launch configuration from the autotuner (outside the timed region)
         ctx.rebin(raw, reb)
         ctx.filter(reb, filt, scales)
         tuned = autotune.tune_backprojection(ctx, filt, vn, row_scales=scales, use_cache=False)
+    if args.bp_config:
+        ctx.set_bp_config(autotune.parse_config_name(args.bp_config))
     step(cnt)  # counts the contributing updates once, outside the timed region
     torch.cuda.synchronize()
     updates = int(cnt.item())
     for _ in range(args.warmup):
-        step()
+        ctx.run(raw, vol)
     torch.cuda.synchronize()
 
-    ev = {k: [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)] for k in
-          ("s", "reb", "flt", "bp", "th")}
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
     clocks.start()
@@ -625,29 +627,20 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    # one step = wfbp_run (rebin, filter, backprojection with the thickening of
+    # the slices inside a slab fused into its write-back, the remaining
+    # slices' thickening), with the library's own stage events
+    stage = {"rebin": 0.0, "filter": 0.0, "backproject": 0.0, "thicken": 0.0}
     start.record(stream)
     for i in range(args.steps):
-        ev["s"][i].record(stream)
-        ctx.rebin(raw, reb)
-        ev["reb"][i].record(stream)
-        ctx.filter(reb, filt, scales)
-        ev["flt"][i].record(stream)
-        ctx.backproject(filt, vn, scales)
-        ev["bp"][i].record(stream)
-        ctx.thicken(vn, vol)
-        ev["th"][i].record(stream)
+        for k, v in ctx.run_timed(raw, vol).items():
+            stage[k] += v
     stop.record(stream)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     clk = clocks.stop()
     total_ms = start.elapsed_time(stop)
-    stage = {"rebin": 0.0, "filter": 0.0, "backproject": 0.0, "thicken": 0.0}
-    for i in range(args.steps):
-        stage["rebin"] += ev["s"][i].elapsed_time(ev["reb"][i])
-        stage["filter"] += ev["reb"][i].elapsed_time(ev["flt"][i])
-        stage["backproject"] += ev["flt"][i].elapsed_time(ev["bp"][i])
-        stage["thicken"] += ev["bp"][i].elapsed_time(ev["th"][i])
     stage = {k: v / args.steps for k, v in stage.items()}
     ms = total_ms / args.steps
     t_max = torch.tensor([ms], dtype=torch.float64, device=dev)

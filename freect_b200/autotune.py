@@ -35,6 +35,15 @@ def config_name(key):
     return "%dx%d/%dw%ds%d" % tuple(key)
 
 
+def parse_config_name(name):
+    """Inverse of config_name: '16x20/8w20s16' -> (16, 20, 8, 20, 16)."""
+    import re
+    m = re.fullmatch(r"(\d+)x(\d+)/(\d+)w(\d+)s(\d+)", name.strip())
+    if not m:
+        raise ValueError("backprojection configuration %r is not of the form TXxTY/CwNsS" % name)
+    return tuple(int(g) for g in m.groups())
+
+
 def _load(path):
     try:
         with open(path) as f:

@@ -84,12 +84,14 @@ __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y
 // Shared memory of a CTA: the mbarriers and small words at fixed offsets
 // (they persist across the tiles of a persistent launch), then the regions
 // of bp_smem_layout for the tile's scan.
-constexpr int BT_OFF_NVS = 64;  // int [16]: [0..1] views per stage, [8] failure flag, [9] next item
+// int [16]: [0..1] views per stage, [8] failure flag, [9] next item, [10] fused-thickening words
+constexpr int BT_OFF_NVS = 64;
 
 __device__ __forceinline__ void bp_init_barriers(uint8_t* smem, int nw) {
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   if (threadIdx.x == 0) {
     reinterpret_cast<int*>(smem + BT_OFF_NVS)[8] = 0;
+    reinterpret_cast<int*>(smem + BT_OFF_NVS)[10] = 0;
     for (int s = 0; s < BT_STAGES; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&full[BT_STAGES + s], nw);
@@ -100,42 +102,63 @@ __device__ __forceinline__ void bp_init_barriers(uint8_t* smem, int nw) {
   __syncthreads();
 }
 
-// Fused thickening of one slab (ThickFuse): for every requested slice r whose
-// native slices all lie in slab bz, each group of SL lanes (lane = slice
+// Fused thickening of one slab (ThickFuse). The producer warp has copied the
+// slab's records into shared memory (fz, nfz words) while the ring filled.
+// For every interior requested slice r each group of SL lanes (lane = slice
 // s0 + lane % SL) gathers its native values with shuffles, in the CSR order
 // and with the same FMA chain and division as k_thicken, so the result is
 // bit-identical to thickening the written native volume. Lane c of a group
 // writes column c of the group. All 32 lanes of the warp take part.
 template <int CPW, int SL, int CPG>
-__device__ __forceinline__ void bp_fused_thicken(const ThickFuse& tf, const float (&vals)[CPG], bool zero, int bz,
-                                                 int s0, int warp, int lane, int ix0, int iy0, const BPTile& bt,
+__device__ __forceinline__ void bp_fused_thicken(const ThickFuse& tf, const float (&vals)[CPG], const int* fz,
+                                                 int nfz, int warp, int lane, int ix0, int iy0, const BPTile& bt,
                                                  const BPParams& p) {
+  const int grp = lane / SL, ll = lane % SL;
+  const int tt = warp * CPW + grp * CPG + min(ll, CPG - 1);
+  const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
+  const bool wr = ll < CPG && ix < p.nx && iy < p.ny;
+  const size_t plane = (size_t)p.nx * p.ny, vox = (size_t)iy * p.nx + ix;
+  nfz = min(nfz, BT_FUSE_WORDS);
+  for (int pos = 0; pos + 3 <= nfz;) {
+    const int r = fz[pos], n = fz[pos + 1];
+    const float ws = __int_as_float(fz[pos + 2]);
+    if (n < 0 || pos + 3 + 2 * n > nfz) break;  // malformed records (host sizing guarantees otherwise)
+    float acc[CPG];
+#pragma unroll
+    for (int c = 0; c < CPG; c++) acc[c] = 0.0f;
+    for (int e = 0; e < n; e++) {
+      const int src = grp * SL + (fz[pos + 3 + 2 * e] & (SL - 1));
+      const float wt = __int_as_float(fz[pos + 4 + 2 * e]);
+#pragma unroll
+      for (int c = 0; c < CPG; c++) acc[c] = fmaf(wt, __shfl_sync(0xffffffffu, vals[c], src), acc[c]);
+    }
+    float v = 0.0f;
+#pragma unroll
+    for (int c = 0; c < CPG; c++)
+      if (c == ll) v = acc[c];
+    if (wr && r >= 0 && r < tf.nzr) tf.out[(size_t)r * plane + vox] = v / ws;
+    pos += 3 + 2 * n;
+  }
+}
+
+// The same for a tile outside the FOV, whose native values are all +0:
+// k_thicken gives +0 / sum of weights = +0 for every interior slice.
+template <int CPW, int SL, int CPG>
+__device__ __forceinline__ void bp_fused_zero(const ThickFuse& tf, int bz, int warp, int lane, int ix0, int iy0,
+                                              const BPTile& bt, const BPParams& p) {
   const int2 rr = tf.slab_req[bz];
   const int grp = lane / SL, ll = lane % SL;
   const int tt = warp * CPW + grp * CPG + min(ll, CPG - 1);
   const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
   const bool wr = ll < CPG && ix < p.nx && iy < p.ny;
   const size_t plane = (size_t)p.nx * p.ny, vox = (size_t)iy * p.nx + ix;
-  for (int k = rr.x; k < rr.y; k++) {
-    const int r = __ldg(tf.req + k);
-    float v = 0.0f;
-    if (!zero) {
-      float acc[CPG];
-#pragma unroll
-      for (int c = 0; c < CPG; c++) acc[c] = 0.0f;
-      const int a = __ldg(tf.off + r), b = __ldg(tf.off + r + 1);
-      for (int t = a; t < b; t++) {
-        const int src = grp * SL + (__ldg(tf.idx + t) - s0);
-        const float wt = __ldg(tf.w + t);
-#pragma unroll
-        for (int c = 0; c < CPG; c++) acc[c] = fmaf(wt, __shfl_sync(0xffffffffu, vals[c], src), acc[c]);
-      }
-#pragma unroll
-      for (int c = 0; c < CPG; c++)
-        if (c == ll) v = acc[c];
+  for (int k0 = rr.x; k0 < rr.y; k0 += 32) {
+    const int mine = k0 + lane < rr.y ? __ldg(tf.req + k0 + lane) : -1;  // one load per lane
+    const int cnt = min(32, rr.y - k0);
+    for (int k = 0; k < cnt; k++) {
+      const int r = __shfl_sync(0xffffffffu, mine, k);
+      if (wr && r >= 0 && r < tf.nzr) tf.out[(size_t)r * plane + vox] = 0.0f;
     }
-    // a tile outside the FOV has native values +0, and k_thicken gives +0 / ws = +0
-    if (wr) tf.out[(size_t)r * plane + vox] = zero ? 0.0f : v / __ldg(tf.ws + r);
   }
 }
 
@@ -147,7 +170,7 @@ __device__ __forceinline__ void bp_fused_thicken(const ThickFuse& tf, const floa
 // outside the reconstruction FOV (whose voxels are written as 0, the value
 // the reference leaves there). A bounded wait that gave up sets the failure
 // word (the CTA must stop).
-template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
+template <typename T, int CPW, int CU, int NW, int SL, bool COUNT, bool FUSE>
 __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __restrict__ view_scale,
                                         float* __restrict__ vol, const float2* __restrict__ view_sc,
                                         const float* __restrict__ view_z, const float* __restrict__ zslices,
@@ -207,10 +230,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
           if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = 0.0f;
         }
       }
-      if (tf.out && warp < NW) {
-        const float none[CPG] = {};
-        bp_fused_thicken<CPW, SL, CPG>(tf, none, true, bz, s0, warp, lane, ix0, iy0, bt, p);
-      }
+      if (FUSE && tf.out && warp < NW) bp_fused_zero<CPW, SL, CPG>(tf, bz, warp, lane, ix0, iy0, bt, p);
       return 0;
     }
   }
@@ -236,6 +256,16 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       if (!__shfl_sync(0xffffffffu, ok, 0)) {
         failed = true;
         break;
+      }
+      if (FUSE && tf.out && t == min(1, p.P2 - 1)) {
+        // the slab's fused-thickening records, copied while the consumers work
+        // on the first stage and published by this stage's full-barrier arrive
+        const int2 fr = tf.slab_tab[bz];
+        const int nw = max(0, min(fr.y - fr.x, BT_FUSE_WORDS));
+        int* fz = reinterpret_cast<int*>(smem + L.fuse);
+        for (int j = lane; j < nw; j += 32) fz[j] = __ldg(tf.tab + fr.x + j);
+        if (lane == 0) nvs[10] = nw;
+        __syncwarp();
       }
       int nv = 0;
       for (int kb = 0; kb < p.K; kb += 32) {
@@ -463,7 +493,9 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = vacc[c];
     }
   }
-  if (tf.out) bp_fused_thicken<CPW, SL, CPG>(tf, vacc, false, bz, s0, warp, lane, ix0, iy0, bt, p);
+  if (FUSE && tf.out)
+    bp_fused_thicken<CPW, SL, CPG>(tf, vacc, reinterpret_cast<const int*>(smem + L.fuse),
+                                   reinterpret_cast<volatile int*>(nvs)[10], warp, lane, ix0, iy0, bt, p);
   if (COUNT) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
@@ -482,7 +514,7 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view
   // it starts at the (128-byte aligned) base of the CTA's window
   extern __shared__ __align__(128) uint8_t smem[];
   bp_init_barriers(smem, NW);
-  bp_tile<T, CPW, CU, NW, SL, COUNT>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
+  bp_tile<T, CPW, CU, NW, SL, COUNT, true>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
                                  bt.zb0 + blockIdx.z, count, err, smem, 0u, tf);
 }
 
@@ -506,20 +538,21 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
     const BpScan* sd = scans + w.x;
     const BPParams p = sd->p;
     const BPTile bt = sd->bt;
-    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
+    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
                                                  sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring,
                                                  sd->tf);
     __syncthreads();  // the tile's shared memory and words[9] are free again
   }
 }
 
-// Dynamic shared memory of `smem` bytes and the whole unified L1 / shared
-// memory as shared memory, so that as many CTAs fit on an SM as the
-// registers allow.
-template <typename K>
+// Dynamic shared memory of `smem` bytes. Shapes meant to run two CTAs per SM
+// (8 consumer warps) also ask for the whole unified L1 / shared memory as
+// shared memory; the others leave the split to the driver, which keeps more
+// L1 for the geometry and view-table loads.
+template <int NW, typename K>
 cudaError_t prepare_kernel(K* kern, int smem) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && NW <= 8)
     e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   return e;
 }
@@ -535,12 +568,12 @@ cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* v
   constexpr int threads = (NW + 1) * 32;
   cudaError_t e;
   if (count) {
-    e = prepare_kernel(k_bp_tma<T, CPW, CU, NW, SL, true>, bt.smem_bytes);
+    e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, true>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
     k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
                                                                          count, err, tf);
   } else {
-    e = prepare_kernel(k_bp_tma<T, CPW, CU, NW, SL, false>, bt.smem_bytes);
+    e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, false>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
     k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
                                                                           count, err, tf);
@@ -552,7 +585,7 @@ template <typename T, int CPW, int CU, int NW, int SL>
 cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
                              int smem_bytes, int grid, cudaStream_t s) {
   auto kern = k_bp_tma_batch<T, CPW, CU, NW, SL>;
-  cudaError_t e = prepare_kernel(kern, smem_bytes);
+  cudaError_t e = prepare_kernel<NW>(kern, smem_bytes);
   if (e != cudaSuccess) return e;
   // grid = SMs; persistent CTAs: as many per SM as fit
   int per_sm = 1;

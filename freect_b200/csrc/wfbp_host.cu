@@ -172,6 +172,8 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_fuse_slab);
   free_dev(ctx->d_fuse_req);
   free_dev(ctx->d_fuse_bnd);
+  free_dev(ctx->d_fuse_slab_tab);
+  free_dev(ctx->d_fuse_tab);
   free_dev(ctx->d_bplanes);
   free_dev(ctx->d_err);
   free_dev(ctx->d_thickT_off);
@@ -1148,14 +1150,37 @@ int prepare_fuse(wfbp_ctx* ctx) {
   }
   ctx->fuse_slab_h.assign(nslab, make_int2(0, 0));
   ctx->fuse_req_h.clear();
+  std::vector<int2> slab_tab(nslab, make_int2(0, 0));
+  std::vector<int> tab;
+  ctx->fuse_ok = true;
   for (int b = 0; b < nslab; b++) {
     ctx->fuse_slab_h[b].x = (int)ctx->fuse_req_h.size();
     ctx->fuse_req_h.insert(ctx->fuse_req_h.end(), by[b].begin(), by[b].end());
     ctx->fuse_slab_h[b].y = (int)ctx->fuse_req_h.size();
+    slab_tab[b].x = (int)tab.size();
+    for (int r : by[b]) {
+      const int a = ctx->thick_off[r], e = ctx->thick_off[r + 1];
+      float wsum = 0.0f;  // the sum k_thicken divides by, in the same order as setup_slices
+      for (int t = a; t < e; t++) wsum += ctx->thick_w[t];
+      int bits;
+      tab.push_back(r);
+      tab.push_back(e - a);
+      memcpy(&bits, &wsum, 4);
+      tab.push_back(bits);
+      for (int t = a; t < e; t++) {
+        tab.push_back(ctx->thick_idx[t] - b * SL);
+        memcpy(&bits, &ctx->thick_w[t], 4);
+        tab.push_back(bits);
+      }
+    }
+    slab_tab[b].y = (int)tab.size();
+    if (slab_tab[b].y - slab_tab[b].x > BT_FUSE_WORDS) ctx->fuse_ok = false;
   }
   free_dev(ctx->d_fuse_slab);
   free_dev(ctx->d_fuse_req);
   free_dev(ctx->d_fuse_bnd);
+  free_dev(ctx->d_fuse_slab_tab);
+  free_dev(ctx->d_fuse_tab);
   auto put = [&](auto** dst, const auto& v) -> cudaError_t {
     const size_t bytes = sizeof(v[0]) * std::max<size_t>(v.size(), 1);
     cudaError_t e = cudaMalloc(dst, bytes);
@@ -1165,6 +1190,8 @@ int prepare_fuse(wfbp_ctx* ctx) {
   CUDA_TRY(ctx, put(&ctx->d_fuse_slab, ctx->fuse_slab_h));
   CUDA_TRY(ctx, put(&ctx->d_fuse_req, ctx->fuse_req_h));
   CUDA_TRY(ctx, put(&ctx->d_fuse_bnd, ctx->fuse_bnd_h));
+  CUDA_TRY(ctx, put(&ctx->d_fuse_slab_tab, slab_tab));
+  CUDA_TRY(ctx, put(&ctx->d_fuse_tab, tab));
   ctx->n_fuse_bnd = (int)ctx->fuse_bnd_h.size();
   ctx->fuse_slab = SL;
   return WFBP_OK;
@@ -1173,12 +1200,11 @@ int prepare_fuse(wfbp_ctx* ctx) {
 ThickFuse make_fuse(const wfbp_ctx* ctx, float* out) {
   ThickFuse f;
   f.out = out;
+  f.nzr = ctx->nzr;
   f.slab_req = ctx->d_fuse_slab;
   f.req = ctx->d_fuse_req;
-  f.off = ctx->d_thick_off;
-  f.idx = ctx->d_thick_idx;
-  f.w = ctx->d_thick_w;
-  f.ws = ctx->d_thick_ws;
+  f.slab_tab = ctx->d_fuse_slab_tab;
+  f.tab = ctx->d_fuse_tab;
   return f;
 }
 
@@ -1211,8 +1237,8 @@ int run_stages(wfbp_ctx* ctx, const float* raw, float* vol, void* stream, cudaEv
   if (ev) cudaEventRecord(ev[2], s);
   // with the backprojection layout the thickening of the slices inside one
   // slab runs in the backprojection's write-back; the rest follow
-  const bool fuse = lay == WFBP_LAYOUT_BACKPROJECTION;
-  if (!st && fuse) st = prepare_fuse(ctx);
+  if (!st && lay == WFBP_LAYOUT_BACKPROJECTION) st = prepare_fuse(ctx);
+  const bool fuse = !st && lay == WFBP_LAYOUT_BACKPROJECTION && ctx->fuse_ok;
   const ThickFuse tf = make_fuse(ctx, vol);
   nvtxRangePushA("backproject");
   if (!st)
@@ -1319,9 +1345,10 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   // launch ends; with a pinned destination they are copied back right away
   // (on the copy stream, behind the launch's event) while later slabs run
   if ((st = prepare_fuse(ctx))) return st;
+  const bool fuse = ctx->fuse_ok;
   const ThickFuse tf = make_fuse(ctx, ctx->s_vol);
   cudaPointerAttributes pa;
-  const bool pinned = cudaPointerGetAttributes(&pa, vol_host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  const bool pinned = fuse && cudaPointerGetAttributes(&pa, vol_host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
   cudaGetLastError();
   const size_t plane = (size_t)ctx->nx * ctx->ny;
   auto copy_back = [&](const std::vector<int>& rs, cudaStream_t cs) -> int {
@@ -1349,7 +1376,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
       bt.nzb = e - sl;
       CUDA_TRY(ctx, launch_backproject_tma(ctx->s_filtered, mixed ? 1 : 0, ctx->s_scales, ctx->s_vol_native,
                                            ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, bt, nullptr,
-                                           ctx->d_err, s, &tf));
+                                           ctx->d_err, s, fuse ? &tf : nullptr));
       for (int k = sl; k < e; k++) done[k] = 1;
       if (pinned) {
         std::vector<int> rs;
@@ -1376,7 +1403,9 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     if ((st = launch_ready(ve))) return st;
   }
   if ((st = launch_ready(V + 1))) return st;
-  if ((st = thicken_boundary(ctx, ctx->s_vol_native, ctx->s_vol, s))) return st;
+  if ((st = fuse ? thicken_boundary(ctx, ctx->s_vol_native, ctx->s_vol, s)
+                 : wfbp_thicken(ctx, ctx->s_vol_native, ctx->s_vol, s)))
+    return st;
   std::vector<int> rest;
   for (int r = 0; r < ctx->nzr; r++)
     if (!copied[r]) rest.push_back(r);

@@ -54,8 +54,9 @@ struct BPTile {
 // function sizes the launch on the host and carves the buffer on the device.
 constexpr int BT_CWARPS = 16;  // default consumer warps of the TMA backprojection
 constexpr int BT_STAGES = 2;   // view-window ring depth
+constexpr int BT_FUSE_WORDS = 384;  // shared-memory words for one slab's fused-thickening records
 struct BpSmem {
-  unsigned slots, vinfo, vsv, geo, total;
+  unsigned slots, vinfo, vsv, geo, fuse, total;
 };
 // Bytes 0..127 hold the ring's mbarriers and a few words (fixed across the
 // tiles of a persistent launch); the per-scan regions follow.
@@ -71,6 +72,8 @@ __host__ __device__ inline BpSmem bp_smem_layout(const BPTile& bt, int cpw) {
   o = (o + 15u) & ~15u;
   L.geo = o;
   o += (unsigned)(bt.nw * bt.nv_max * (cpw / 2) * 48);  // column-pair geometry records
+  L.fuse = o;
+  o += (unsigned)(BT_FUSE_WORDS * 4);  // the slab's fused-thickening records (ThickFuse)
   L.total = o;
   return L;
 }
@@ -125,7 +128,10 @@ struct wfbp_ctx {
   int2* d_fuse_slab = nullptr;      // [slabs] range into d_fuse_req
   int* d_fuse_req = nullptr;        // interior requested slices by slab
   int* d_fuse_bnd = nullptr;        // boundary requested slices
+  int2* d_fuse_slab_tab = nullptr;  // [slabs] range into d_fuse_tab
+  int* d_fuse_tab = nullptr;        // records (ThickFuse)
   int n_fuse_bnd = 0;
+  bool fuse_ok = false;             // every slab's records fit in BT_FUSE_WORDS
   std::vector<int2> fuse_slab_h;    // host copies
   std::vector<int> fuse_req_h, fuse_bnd_h;
   int* d_thickT_off = nullptr;      // transposed CSR over native slices: (requested slice, w / sum w)
@@ -209,14 +215,17 @@ cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps,
 // formed from that slab's registers and written to `out`; the other
 // ("boundary") requested slices are thickened afterwards from the native
 // volume. out == nullptr: no fusion.
+// Records of slab b, words tab[slab_tab[b].x .. slab_tab[b].y) (at most
+// BT_FUSE_WORDS), one per interior requested slice r:
+//   r, n, bits(sum of weights), then n pairs (native slice - slab start, bits(w))
+// in the thickening CSR's order.
 struct ThickFuse {
   float* out;            // requested volume [nzr][ny][nx]
+  int nzr;
   const int2* slab_req;  // per slab: [begin, end) into req
-  const int* req;        // requested slice indices, grouped by slab, ascending
-  const int* off;        // thickening CSR (the same arrays k_thicken reads)
-  const int* idx;
-  const float* w;
-  const float* ws;
+  const int* req;        // interior requested slices, grouped by slab, ascending
+  const int2* slab_tab;  // per slab: [begin, end) into tab
+  const int* tab;
 };
 
 // One scan of a persistent (batched) backprojection launch, in device memory.

@@ -124,3 +124,11 @@ def test_ffs_geometry_and_validation(lib, orc):
     bad.total_number_of_projections -= 1
     h = C.c_void_p()
     assert lib.wfbp_ctx_create(C.byref(bad), C.byref(spec.recon_config()), None, 0, C.byref(h)) == 1
+
+
+def test_bp_config_names_round_trip():
+    from freect_b200 import autotune
+    for key in [(16, 16, 4, 16, 32), (16, 20, 8, 20, 16), (8, 16, 8, 8, 32)]:
+        assert autotune.parse_config_name(autotune.config_name(key)) == key
+    with pytest.raises(ValueError):
+        autotune.parse_config_name("16x16/4w16")
