@@ -29,10 +29,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed vs FP32"
-# dram__bytes_read.sum + dram__bytes_write.sum / contributing updates of one k_bp_tma launch,
-# ncu capture of rows64_short (profiles/k_bp_tma_rows64_short.md)
-DRAM_BYTES_PER_UPDATE = {"fp32": (5.157631e9 + 0.103164e9) / 2.3819501378e10,
-                         "mixed": (5.689086e9 + 0.103863e9) / 2.3819501378e10}
+# DRAM read + write bytes per contributing update of one backprojection launch, from the
+# ncu captures of rows64_short (2.3819501378e10 updates), by precision form and slab height
+# (16-slice slabs stage each view window in twice as many CTAs)
+DRAM_BYTES_PER_UPDATE = {("fp32", 32): (5.157631e9 + 0.103164e9) / 2.3819501378e10,
+                         ("mixed", 32): (5.689086e9 + 0.103863e9) / 2.3819501378e10,
+                         ("fp32", 16): (13.673464e9 + 0.162628e9) / 2.3819501378e10,
+                         ("mixed", 16): (14.311128e9 + 0.162348e9) / 2.3819501378e10}
 UNIT = "voxel-view updates/s"
 
 
@@ -679,9 +682,8 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
     elem = 4 if prec == T.PRECISION_FP32 else 2
     achieved = updates * 4 * elem / (stage["backproject"] / 1000.0) / 1e9
     # DRAM bytes per contributing update of the backprojection from the ncu capture of the
-    # same kernel on the rows64 scanner's short scan (profiles/k_bp_tma_rows64_short.md),
-    # scaled to this launch by its updates
-    dram_per_update = DRAM_BYTES_PER_UPDATE[form]
+    # same kernel on the rows64 scanner's short scan, scaled to this launch by its updates
+    dram_per_update = DRAM_BYTES_PER_UPDATE[(form, ctx.bp_config().slab)]
     roofline = {"bound": "hbm", "kernel": "backproject", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": dram_per_update * updates,
                 "traffic_note": "dram read+write bytes per launch: %.4f B/update from the rows64_short ncu capture "
