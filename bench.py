@@ -218,13 +218,22 @@ def run_diff(args, rank, world, local, dist):
     the four FP32 stages, MSE to a target volume, backward through the
     adjoint kernels to the raw readings and 64 learnable filter taps. The
     target is each scan's noiseless reconstruction (computed once on the GPU).
-    Updates are counted for the forward and the adjoint backprojection."""
+    Updates are counted for the forward and the adjoint backprojection.
+    --workload diff1: the same step on one scan of the small scanner reduced
+    to 2 rotations and 192^2 x 12 slices, a profiling-size case of the same
+    kernels (about 2 GB on the device)."""
     import torch
     from freect_b200 import scans, wfbp
     from freect_b200.autograd import Reconstructor
 
     dev = torch.device("cuda", local)
-    specs = [scans.small(seed=4 * rank + i) for i in range(4)]
+    n_scans = 4 if args.workload == "diff4" else 1
+    specs = [scans.small(seed=4 * rank + i) for i in range(n_scans)]
+    if args.workload == "diff1":
+        for sp in specs:
+            sp.rotations = 2
+            sp.nx = sp.ny = 192
+            sp.n_slices = 12
     tube, table = specs[0].views()
     cg, gp = wfbp.configure_geometry(specs[0].meta(), table)
     rp = specs[0].recon_config()
@@ -306,16 +315,17 @@ def run_diff(args, rank, world, local, dist):
     line = {"metric": METRIC, "value": updates * world / (ms / 1000.0), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (4 seeded head-like ellipsoid phantoms per rank, Poisson noise)",
-            "config": {"workload": "diff4", "scans": 4, "channels": specs[0].nch, "rows": specs[0].nr,
+            "data": "synthetic (%d seeded head-like ellipsoid phantoms per rank, Poisson noise)" % n_scans,
+            "config": {"workload": args.workload, "scans": n_scans, "channels": specs[0].nch, "rows": specs[0].nr,
                        "views": specs[0].V, "volume": [specs[0].n_slices, specs[0].ny, specs[0].nx],
                        "learnable_taps": 64, "step": "forward + MSE + backward to raw readings and taps",
                        "updates_counted": "forward and adjoint backprojection",
-                       "parallelism": "independent batch per GPU", "l2": "inputs larger than L2 (0.6 GB raw)"},
+                       "parallelism": "independent batch per GPU",
+                       "l2": "inputs larger than L2 (%.2f GB raw)" % (raw.numel() * 4 / 1e9)},
             "updates_per_step": updates, "loss": float(loss.item()),
-            # per step: 4 scans x (rebin, filter, backprojection, thickening) forward and
+            # per step and scan: (rebin, filter, backprojection, thickening) forward and
             # (thickening, backprojection, filter, rebin adjoints + 2 tap-gradient kernels) backward
-            "gpu_launches": 4 * (4 + 6) * args.steps,
+            "gpu_launches": n_scans * (4 + 6) * args.steps,
             "e2e": {"value": updates * world / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
                     "h2d_bytes_per_step": int(raw.numel() * 4), "d2h_bytes_per_step": 4 + 64 * 4},
             "clocks": clk}
@@ -491,7 +501,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    if args.workload in ("batch24", "diff4"):
+    if args.workload in ("batch24", "diff4", "diff1"):
         (run_batch if args.workload == "batch24" else run_diff)(args, rank, world, local, dist)
         if dist:
             dist.destroy_process_group()

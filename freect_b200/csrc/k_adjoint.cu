@@ -192,18 +192,49 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
           s_lo = max(0, (int)floorf(fa) - 1);
           s_hi = min(p.nz - 1, (int)ceilf(fb) + 1);
         }
-        const float* gcol = TABLE ? G + (((size_t)t * p.ny + iy) * p.nx + ix) * nzp : nullptr;
-        for (int s = s_lo; s <= s_hi; s++) {
-          const float z = __ldg(zslices + s);
-          float q_idx;
-          const float Wj = view_weight(p, g, z, &q_idx);
-          if (Wj == 0.0f) continue;
-          float scaled;  // g_vol * dtheta / sum_k W_k (cuda_kernels.cuh:283)
-          if constexpr (TABLE) {
-            const float w = __ldg(gcol + s);
-            if (w == 0.0f) continue;
-            scaled = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix) * w;
-          } else {
+        if constexpr (TABLE) {
+          // the voxel's weights and gradients are contiguous runs over the
+          // slices (both [.][y][x][nzp]): aligned float4 blocks, the next
+          // block's loads issued before this block's arithmetic
+          const float4* wrow = reinterpret_cast<const float4*>(G + (((size_t)t * p.ny + iy) * p.nx + ix) * nzp);
+          const float4* grow = reinterpret_cast<const float4*>(gvol + ((size_t)iy * p.nx + ix) * nzp);
+          const int e4 = s_hi >> 2;
+          int b4 = s_lo >> 2;
+          float4 wn = __ldg(wrow + b4), gn = __ldg(grow + b4);
+          for (; b4 <= e4; b4++) {
+            const float wa[4] = {wn.x, wn.y, wn.z, wn.w}, ga[4] = {gn.x, gn.y, gn.z, gn.w};
+            if (b4 < e4) {
+              wn = __ldg(wrow + b4 + 1);
+              gn = __ldg(grow + b4 + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              const int s = 4 * b4 + u;
+              if (s < s_lo || s > s_hi || wa[u] == 0.0f) continue;
+              float q_idx;
+              const float Wj = view_weight(p, g, __ldg(zslices + s), &q_idx);
+              if (Wj == 0.0f) continue;
+              const float scaled = ga[u] * wa[u];  // g_vol * dtheta / sum_k W_k (cuda_kernels.cuh:283)
+            const float sw = scaled * Wj;
+            const float c0v = sw * h0, c1v = sw * wp;
+            const float qf = floorf(q_idx), wq = q_idx - qf;
+            const int r = min(max((int)qf, 0), p.nr - 2);
+            float2* a0 = acc2 + r * AD_CH + cl;
+            float2 v0 = a0[0], v1 = a0[AD_CH];
+            v0.x += c0v * (1.0f - wq);
+            v0.y += c1v * (1.0f - wq);
+            v1.x += c0v * wq;
+            v1.y += c1v * wq;
+            a0[0] = v0;
+            a0[AD_CH] = v1;
+            }
+          }
+        } else {
+          for (int s = s_lo; s <= s_hi; s++) {
+            const float z = __ldg(zslices + s);
+            float q_idx;
+            const float Wj = view_weight(p, g, z, &q_idx);
+            if (Wj == 0.0f) continue;
             const float gv = __ldg(gvol + ((size_t)s * p.ny + iy) * p.nx + ix);
             if (gv == 0.0f) continue;
             // sum of the weights of all half turns, in the forward's order
@@ -220,20 +251,20 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
               float qk;
               aw += view_weight(p, gk, z, &qk);
             }
-            scaled = gv * (p.dtheta * (1.0f / aw));
+            const float scaled = gv * (p.dtheta * (1.0f / aw));  // cuda_kernels.cuh:283
+            const float sw = scaled * Wj;
+            const float c0v = sw * h0, c1v = sw * wp;
+            const float qf = floorf(q_idx), wq = q_idx - qf;
+            const int r = min(max((int)qf, 0), p.nr - 2);
+            float2* a0 = acc2 + r * AD_CH + cl;
+            float2 v0 = a0[0], v1 = a0[AD_CH];
+            v0.x += c0v * (1.0f - wq);
+            v0.y += c1v * (1.0f - wq);
+            v1.x += c0v * wq;
+            v1.y += c1v * wq;
+            a0[0] = v0;
+            a0[AD_CH] = v1;
           }
-          const float sw = scaled * Wj;
-          const float c0v = sw * h0, c1v = sw * wp;
-          const float qf = floorf(q_idx), wq = q_idx - qf;
-          const int r = min(max((int)qf, 0), p.nr - 2);
-          float2* a0 = acc2 + r * AD_CH + cl;
-          float2 v0 = a0[0], v1 = a0[AD_CH];
-          v0.x += c0v * (1.0f - wq);
-          v0.y += c1v * (1.0f - wq);
-          v1.x += c0v * wq;
-          v1.y += c1v * wq;
-          a0[0] = v0;
-          a0[AD_CH] = v1;
         }
       }
     }
@@ -243,6 +274,15 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
     float* out = gD + (size_t)j * p.nr * p.nch + c;
     for (int r = 0; r < p.nr; r++) out[(size_t)r * p.nch] = acc2[r * AD_CH + cl].x + acc2[r * AD_CH + cl - 1].y;
   }
+}
+
+// gvt[vox][s] = gvol[s][vox] (s < nz), 0 for the padding up to nzp.
+__global__ void k_adj_gvol_t(const float* __restrict__ gvol, float* __restrict__ gvt, int nxy, int nz, int nzp) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)nxy * nzp) return;
+  const long vox = i / nzp;
+  const int sl = (int)(i % nzp);
+  gvt[i] = sl < nz ? __ldg(gvol + (size_t)sl * nxy + vox) : 0.0f;
 }
 
 // ---------------------------------------------------------------------------
@@ -409,7 +449,7 @@ __global__ void k_taps_reduce(const float* __restrict__ partial, int nblk, int n
 
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
                               const BPParams& p, float z0, float dzs, float* scale_table, bool fill_table,
-                              cudaStream_t s) {
+                              float* gvol_t, cudaStream_t s) {
   if (scale_table && fill_table) {
     dim3 g((unsigned)((p.nx + AN_TX - 1) / AN_TX), (unsigned)((p.ny + AN_TY - 1) / AN_TY),
            (unsigned)((p.nz + AN_ZS - 1) / AN_ZS));
@@ -423,6 +463,15 @@ cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, co
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+  }
+  if (scale_table) {
+    // the gradient volume with the table's layout [y][x][nzp]
+    const int nzp = bp_adjoint_nzp(p.nz);
+    const long n = (long)p.nx * p.ny * nzp;
+    k_adj_gvol_t<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gvol, gvol_t, p.nx * p.ny, p.nz, nzp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    gvol = gvol_t;
   }
   kern<<<grid, AD_CH, smem, s>>>(gvol, scale_table, gD, sc, vz, zs, p, z0, dzs, bp_adjoint_nzp(p.nz));
   return cudaGetLastError();

@@ -184,6 +184,7 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_radj_w);
   free_dev(ctx->d_tg_partial);
   free_dev(ctx->d_adj_scale);
+  free_dev(ctx->d_adj_gvt);
   for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
   ctx->ev_copy.clear();
   if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
@@ -1050,18 +1051,23 @@ WFBP_API int wfbp_backproject_adjoint(wfbp_ctx* ctx, const float* g_native, floa
   const bool want_table = ctx->ext.adjoint_scale_table == 0 && n * sizeof(float) <= kAdjointTableBytes;
   if (want_table && n > ctx->adj_scale_n) {
     free_dev(ctx->d_adj_scale);
+    free_dev(ctx->d_adj_gvt);
     ctx->adj_scale_valid = false;
-    if (cudaMalloc(&ctx->d_adj_scale, n * sizeof(float)) == cudaSuccess) {
+    const size_t ngt = (size_t)bp_adjoint_nzp(ctx->nz) * ctx->nx * ctx->ny;
+    if (cudaMalloc(&ctx->d_adj_scale, n * sizeof(float)) == cudaSuccess &&
+        cudaMalloc(&ctx->d_adj_gvt, ngt * sizeof(float)) == cudaSuccess) {
       ctx->adj_scale_n = n;
     } else {
-      cudaGetLastError();
-      ctx->d_adj_scale = nullptr;
+      cudaGetLastError();  // too large for the free memory: recompute the sums instead
+      free_dev(ctx->d_adj_scale);
+      free_dev(ctx->d_adj_gvt);
       ctx->adj_scale_n = 0;
     }
   }
-  float* table = want_table && ctx->d_adj_scale && n <= ctx->adj_scale_n ? ctx->d_adj_scale : nullptr;
+  float* table = want_table && ctx->d_adj_scale && ctx->d_adj_gvt && n <= ctx->adj_scale_n ? ctx->d_adj_scale
+                                                                                              : nullptr;
   CUDA_TRY(ctx, launch_bp_adjoint(g_native, g_filtered, ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, z0, dzs,
-                                  table, table && !ctx->adj_scale_valid, (cudaStream_t)stream));
+                                  table, table && !ctx->adj_scale_valid, ctx->d_adj_gvt, (cudaStream_t)stream));
   if (table) ctx->adj_scale_valid = true;
   return WFBP_OK;
 }

@@ -146,6 +146,7 @@ struct wfbp_ctx {
   size_t tg_partial_n = 0;
   float* d_adj_scale = nullptr;     // backprojection adjoint: per-(voxel, theta~) weight dtheta / sum_k W_k
   size_t adj_scale_n = 0;
+  float* d_adj_gvt = nullptr;       // backprojection adjoint: gradient as [ny][nx][nzp]
   bool adj_scale_valid = false;     // the table matches the current views and slices
 
   // mixed precision: Toeplitz operand planes for the tensor-core filter
@@ -257,10 +258,11 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // slice stride of the backprojection adjoint's scale table [P/2][ny][nx][nzp]
 inline int bp_adjoint_nzp(int nz) { return (nz + 3) / 4 * 4; }
 // scale_table: [P/2][ny][nx][nzp] weights dtheta / sum_k W_k, filled first
-// when fill_table is set; nullptr: the gather recomputes the weight sums
+// when fill_table is set; nullptr: the gather recomputes the weight sums.
+// gvol_t: [ny][nx][nzp] scratch for the transposed gradient (table path).
 cudaError_t launch_bp_adjoint(const float* gvol, float* gD, const float2* sc, const float* vz, const float* zs,
                               const BPParams& p, float z0, float dzs, float* scale_table, bool fill_table,
-                              cudaStream_t s);
+                              float* gvol_t, cudaStream_t s);
 cudaError_t launch_thicken_adjoint(const float* gvol, float* gvn, const int* off, const int* ridx, const float* w,
                                    int nxy, int nz, cudaStream_t s);
 cudaError_t launch_rebin_adj_cols(const float* bidx, int nch, int q8, int* cnt, int* cidx, float* cw, int maxl,
