@@ -397,43 +397,83 @@ __global__ void k_rebin_adjoint(const float* __restrict__ gR, float* __restrict_
 // ---------------------------------------------------------------------------
 // Forward: y[n] = sum_m h[|n - m|] x[m] over the nch channels of each row.
 // dL/dh[0] = sum_rows sum_n g[n] x[n]; dL/dh[d] = sum_rows sum_n g[n] (x[n-d] + x[n+d]).
-// A CTA takes TG_ROWS rows, recomputes their rebinned samples x from the raw
-// readings into shared memory (nothing of the rebinned array is stored), and
-// each thread correlates them with the incoming gradient rows for its taps.
-// Per-CTA partial sums are reduced in a fixed order by k_taps_reduce.
+// A CTA takes TG_ROWS rows and recomputes their rebinned samples x from the
+// raw readings into shared memory (nothing of the rebinned array is stored).
+// Thread (tap group, row) correlates its row for TG_TAPS consecutive taps d0..
+// d0+3: one gradient load and two sliding-window loads of x feed 8 FMAs per
+// channel. The rows of a CTA (8 consecutive lanes) are summed with shuffles
+// in a fixed order, and the per-CTA partial sums by k_taps_reduce, so the
+// result does not depend on scheduling.
 constexpr int TG_ROWS = 8;
-constexpr int TG_THREADS = 128;
+constexpr int TG_TAPS = 4;
+constexpr int TG_THREADS = 128;  // 16 tap groups x 8 rows
 
 __global__ void __launch_bounds__(TG_THREADS)
 k_taps_grad(const float* __restrict__ raw, const float* __restrict__ gY, const float* __restrict__ beta_t,
             const float* __restrict__ bidx_t, RebinParams p, int ntaps, float* __restrict__ partial) {
   extern __shared__ float sm[];
-  float* xs = sm;                        // [TG_ROWS][nch]
-  float* gs = sm + TG_ROWS * p.nch;      // [TG_ROWS][nch]
+  const int ns = p.nch | 1;               // odd row stride: the 8 rows of a warp fall in different banks
+  float* xs = sm;                         // [TG_ROWS][ns]
+  float* gs = sm + TG_ROWS * ns;          // [TG_ROWS][ns]
   const long m0 = (long)blockIdx.x * TG_ROWS;
   const long M = (long)p.V * p.nr;
   const int rows = (int)min((long)TG_ROWS, M - m0);
-  for (int e = threadIdx.x; e < rows * p.nch; e += TG_THREADS) {
+  for (int e = threadIdx.x; e < TG_ROWS * p.nch; e += TG_THREADS) {
     const int rr = e / p.nch, c = e % p.nch;
     const long m = m0 + rr;
-    const int v = (int)(m / p.nr), i = (int)(m % p.nr);
-    xs[e] = wfbp_rebin_sample(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v, i);
-    gs[e] = __ldg(gY + m * p.nch + c);
+    float xv = 0.0f, gv = 0.0f;  // rows past the end contribute nothing
+    if (rr < rows) {
+      const int v = (int)(m / p.nr), i = (int)(m % p.nr);
+      xv = wfbp_rebin_sample(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v, i);
+      gv = __ldg(gY + m * p.nch + c);
+    }
+    xs[rr * ns + c] = xv;
+    gs[rr * ns + c] = gv;
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < ntaps; d += TG_THREADS) {
-    float acc = 0.0f;
-    for (int rr = 0; rr < rows; rr++) {
-      const float* xr = xs + rr * p.nch;
-      const float* gr = gs + rr * p.nch;
-      if (d == 0) {
-        for (int n = 0; n < p.nch; n++) acc = fmaf(gr[n], xr[n], acc);
-      } else {
-        for (int n = d; n < p.nch; n++) acc = fmaf(gr[n], xr[n - d], acc);
-        for (int n = 0; n + d < p.nch; n++) acc = fmaf(gr[n], xr[n + d], acc);
+  const int rr = threadIdx.x % TG_ROWS;
+  const float* xr = xs + rr * ns;
+  const float* gr = gs + rr * ns;
+  const int ngroups = (ntaps + TG_TAPS - 1) / TG_TAPS;
+  // every lane of a warp runs the same number of group iterations (the shuffles below)
+  for (int g0 = 0; g0 < ngroups; g0 += TG_THREADS / TG_ROWS) {
+    const int gi = g0 + threadIdx.x / TG_ROWS;
+    const int d0 = gi * TG_TAPS;
+    float af[TG_TAPS], ab[TG_TAPS], wf[TG_TAPS], wb[TG_TAPS];
+#pragma unroll
+    for (int k = 0; k < TG_TAPS; k++) {
+      af[k] = ab[k] = 0.0f;
+      wf[k] = 0.0f;  // wf[k] = x[n - d0 - k]
+      const int jb = d0 + k;
+      wb[k] = jb < p.nch ? xr[jb] : 0.0f;  // wb[k] = x[n + d0 + k]
+    }
+    if (gi < ngroups) {
+      for (int n = 0; n < p.nch; n++) {
+        const float g = gr[n];
+        // slide the forward window: wf[k] = x[n - d0 - k]
+#pragma unroll
+        for (int k = TG_TAPS - 1; k > 0; k--) wf[k] = wf[k - 1];
+        wf[0] = n - d0 >= 0 ? xr[n - d0] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < TG_TAPS; k++) {
+          af[k] = fmaf(g, wf[k], af[k]);
+          ab[k] = fmaf(g, wb[k], ab[k]);
+        }
+        // slide the backward window to n + 1: wb[k] = x[n + 1 + d0 + k]
+#pragma unroll
+        for (int k = 0; k < TG_TAPS - 1; k++) wb[k] = wb[k + 1];
+        const int jb = n + 1 + d0 + TG_TAPS - 1;
+        wb[TG_TAPS - 1] = jb < p.nch ? xr[jb] : 0.0f;
       }
     }
-    partial[(size_t)blockIdx.x * ntaps + d] = acc;
+#pragma unroll
+    for (int k = 0; k < TG_TAPS; k++) {
+      // dL/dh[0] counts the product once, dL/dh[d > 0] both neighbours
+      float v = d0 + k == 0 ? af[k] : af[k] + ab[k];
+#pragma unroll
+      for (int o = TG_ROWS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (rr == 0 && gi < ngroups && d0 + k < ntaps) partial[(size_t)blockIdx.x * ntaps + d0 + k] = v;
+    }
   }
 }
 
@@ -502,7 +542,7 @@ int taps_grad_blocks(const RebinParams& p) { return (int)(((long)p.V * p.nr + TG
 cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float* beta, const float* bidx,
                                  const RebinParams& p, int ntaps, float* partial, float* out, cudaStream_t s) {
   const int nblk = taps_grad_blocks(p);
-  const size_t smem = (size_t)2 * TG_ROWS * p.nch * sizeof(float);
+  const size_t smem = (size_t)2 * TG_ROWS * (p.nch | 1) * sizeof(float);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_taps_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
