@@ -211,6 +211,11 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def autotune_name(key):
+    from freect_b200 import autotune
+    return autotune.config_name(key)
+
+
 def run_diff(args, rank, world, local, dist):
     """--workload diff4: one training step of the differentiable WFBP on a
     batch of 4 scans of the small scanner (672 x 16, 1160 views/rotation, 3
@@ -260,7 +265,16 @@ def run_diff(args, rank, world, local, dist):
     rec.ctx.filter(reb, flt)
     rec.ctx.backproject(flt, vn, update_count=cnt)
     torch.cuda.synchronize()
-    updates = 2 * 4 * int(cnt.item())
+    updates = 2 * n_scans * int(cnt.item())
+    tuned = None
+    if not args.no_tune:
+        # forward backprojection launch shape from the autotuner (outside the timed region)
+        from freect_b200 import autotune
+        tuned = autotune.tune_backprojection(rec.ctx, flt, vn, use_cache=False)["config"]
+    try:
+        bp_name = autotune_name(rec.ctx.bp_config().key())
+    except wfbp.WfbpError:  # the reference-layout kernel (no TMA launch fits)
+        bp_name = "reference layout"
     taps = torch.nn.Parameter(rec.initial_taps())
     raw.requires_grad_(True)
 
@@ -321,7 +335,8 @@ def run_diff(args, rank, world, local, dist):
                        "learnable_taps": 64, "step": "forward + MSE + backward to raw readings and taps",
                        "updates_counted": "forward and adjoint backprojection",
                        "parallelism": "independent batch per GPU",
-                       "l2": "inputs larger than L2 (%.2f GB raw)" % (raw.numel() * 4 / 1e9)},
+                       "l2": "inputs larger than L2 (%.2f GB raw)" % (raw.numel() * 4 / 1e9),
+                       "bp_config": bp_name},
             "updates_per_step": updates, "loss": float(loss.item()),
             # per step and scan: (rebin, filter, backprojection, thickening) forward and
             # (thickening, backprojection, filter, rebin adjoints + 2 tap-gradient kernels) backward
