@@ -189,6 +189,10 @@ void release(wfbp_ctx* ctx) {
   ctx->ev_copy.clear();
   if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
   ctx->s_copy = nullptr;
+  for (auto& b : ctx->s_bp) {
+    if (b) cudaStreamDestroy(b);
+    b = nullptr;
+  }
   free_dev(ctx->s_rebinned);
   free_dev(ctx->s_filtered);
   free_dev(ctx->s_scales);
@@ -1312,8 +1316,11 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   const int lay = WFBP_LAYOUT_BACKPROJECTION;
   constexpr int kChunks = 8;
   if (!ctx->s_copy) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
+  for (auto& b : ctx->s_bp)
+    if (!b) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
   if (ctx->ev_copy.empty()) {
-    ctx->ev_copy.resize(kChunks + 2);  // chunk copies, caller order, fused slices ready
+    // chunk copies, caller order, a launch's slices final, views filtered, streams joined
+    ctx->ev_copy.resize(kChunks + 4);
     for (auto& e : ctx->ev_copy) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   const int V = ctx->V, G = ctx->G;
@@ -1369,6 +1376,11 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     return WFBP_OK;
   };
   std::vector<char> copied(ctx->nzr, 0);
+  // Range launches alternate between two streams, so that one launch's last
+  // partial wave of CTAs overlaps the next launch instead of idling the SMs;
+  // each waits only for the views it reads (filtered on s).
+  cudaEvent_t ev_done = ctx->ev_copy[kChunks + 1], ev_filt = ctx->ev_copy[kChunks + 2];
+  int nlaunch = 0;
   auto launch_ready = [&](int filtered_upto) -> int {
     for (int sl = 0; sl < nslab;) {
       if (done[sl] || need[sl] >= filtered_upto) {
@@ -1380,17 +1392,20 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
       BPTile bt = ctx->bpt;
       bt.zb0 = sl;
       bt.nzb = e - sl;
+      const cudaStream_t sb = ctx->s_bp[nlaunch++ % 2];
+      CUDA_TRY(ctx, cudaEventRecord(ev_filt, s));
+      CUDA_TRY(ctx, cudaStreamWaitEvent(sb, ev_filt, 0));
       CUDA_TRY(ctx, launch_backproject_tma(ctx->s_filtered, mixed ? 1 : 0, ctx->s_scales, ctx->s_vol_native,
                                            ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, bt, nullptr,
-                                           ctx->d_err, s, fuse ? &tf : nullptr));
+                                           ctx->d_err, sb, fuse ? &tf : nullptr));
       for (int k = sl; k < e; k++) done[k] = 1;
       if (pinned) {
         std::vector<int> rs;
         for (int k = sl; k < e; k++)
           for (int i = ctx->fuse_slab_h[k].x; i < ctx->fuse_slab_h[k].y; i++) rs.push_back(ctx->fuse_req_h[i]);
         if (!rs.empty()) {
-          CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[kChunks + 1], s));
-          CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_copy, ctx->ev_copy[kChunks + 1], 0));
+          CUDA_TRY(ctx, cudaEventRecord(ev_done, sb));
+          CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_copy, ev_done, 0));
           const int cst = copy_back(rs, ctx->s_copy);
           if (cst) return cst;
           for (int r : rs) copied[r] = 1;
@@ -1409,6 +1424,10 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     if ((st = launch_ready(ve))) return st;
   }
   if ((st = launch_ready(V + 1))) return st;
+  for (auto& b : ctx->s_bp) {  // every backprojection launch before the rest of the thickening
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[kChunks + 3], b));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->ev_copy[kChunks + 3], 0));
+  }
   if ((st = fuse ? thicken_boundary(ctx, ctx->s_vol_native, ctx->s_vol, s)
                  : wfbp_thicken(ctx, ctx->s_vol_native, ctx->s_vol, s)))
     return st;

@@ -170,6 +170,7 @@ struct wfbp_ctx {
   float* s_raw = nullptr;
   float* s_vol = nullptr;
   cudaStream_t s_copy = nullptr;    // wfbp_run_host: host-to-device copies of the reading chunks
+  cudaStream_t s_bp[2] = {nullptr, nullptr};  // wfbp_run_host: backprojection launches (alternating)
   std::vector<cudaEvent_t> ev_copy; // one per chunk, plus the caller-stream fence
 
   bool views_set = false;
