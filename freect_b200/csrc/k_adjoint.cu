@@ -172,6 +172,12 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
         const int ix = along_y ? in : o, iy = along_y ? o : in;
         const float x = xcoord(p, ix), y = ycoord(p, iy);
         if (x * x + y * y > p.fov_half2) continue;  // cuda_kernels.cuh:220
+        {
+          // the channel test first (three FMAs), the square root, arcsine
+          // and division of the geometry only for the voxel that passes it
+          const float ph = x * sc.x - y * sc.y;
+          if ((int)floorf(p.kp - (ph * p.ps + p.c0)) != c) continue;
+        }
         const ViewGeo g = view_geo(p, x, y, sc, zt);
         if (!g.valid_p) continue;
         const float pf = floorf(g.p_idx), wp = g.p_idx - pf;
