@@ -36,6 +36,12 @@ DRAM_BYTES_PER_UPDATE = {("fp32", 32): (5.157631e9 + 0.103164e9) / 2.3819501378e
                          ("mixed", 32): (5.689086e9 + 0.103863e9) / 2.3819501378e10,
                          ("fp32", 16): (13.673464e9 + 0.162628e9) / 2.3819501378e10,
                          ("mixed", 16): (14.311128e9 + 0.162348e9) / 2.3819501378e10}
+# warp instructions per contributing update of one backprojection launch (smsp__inst_executed.sum
+# / updates) from the same captures; the kernel's binding limit is instruction issue
+WARP_INST_PER_UPDATE = {("fp32", 32): 4.47e10 / 2.3819501378e10, ("mixed", 32): 4.66e10 / 2.3819501378e10,
+                        ("fp32", 16): 4.4354276467e10 / 2.3819501378e10,
+                        ("mixed", 16): 4.5782817879e10 / 2.3819501378e10}
+SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"
 
 
@@ -544,12 +550,13 @@ def main():
                              % (head["dims"].raw_bytes / 1e9, head["dims"].filtered_bytes / 1e9),
                        "bp_config": head["bp_config"], "bp_tuning_ms": head["tuning"]},
             "s_per_volume": head["ms"] / 1000.0, "updates_per_volume": head["updates"],
-            "stage_ms": head["stage"], "roofline": head["roofline"], "gpu_launches": 4 * args.steps,
+            "stage_ms": head["stage"], "roofline": head["roofline"], "issue_roofline": head["issue"],
+            "gpu_launches": 4 * args.steps,
             "e2e": head["e2e"], "clocks": head["clocks"]}
     if len(forms) == 2:
         f32 = res["fp32"]
-        line["fp32"] = {k: f32[k] for k in ("value", "ms", "stage", "roofline", "e2e", "bp_config", "clocks")
-                        if k in f32}
+        line["fp32"] = {k: f32[k] for k in ("value", "ms", "stage", "roofline", "issue", "e2e", "bp_config",
+                                            "clocks") if k in f32}
         line["mixed_speedup_vs_fp32"] = {"device": f32["ms"] / head["ms"],
                                          "e2e": (f32["e2e"]["ms_per_step"] / head["e2e"]["ms_per_step"])
                                          if head["e2e"] and f32["e2e"] else None}
@@ -717,8 +724,18 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
                 "algorithmic_bytes_per_update": 4 * elem,
                 "note": "4 bilinear taps per contributing update, read from shared memory after one TMA "
                         "staging per view window; the kernel is issue-bound (ncu summaries under profiles/)"}
+    # issue roofline: warp instructions per second the launch needs at this rate, against one
+    # instruction per scheduler per clock at the SM clock sampled during the timed steps
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    wipu = WARP_INST_PER_UPDATE[(form, ctx.bp_config().slab)]
+    ips = wipu * updates / (stage["backproject"] / 1000.0)
+    ipeak = SMS * SCHEDULERS_PER_SM * mhz * 1e6
+    issue = {"kernel": "backproject", "warp_inst_per_update": wipu, "achieved": ips, "peak": ipeak,
+             "unit": "warp instructions/s", "frac": ips / ipeak,
+             "note": "instructions per update from the rows64_short ncu capture of the same slab height; "
+                     "peak = %d SMs x %d schedulers x %.0f MHz" % (SMS, SCHEDULERS_PER_SM, mhz)}
     out = {"value": value, "ms": ms, "stage": stage, "updates": updates, "e2e": e2e, "clocks": clk,
-           "roofline": roofline, "dims": d, "tuning": tuned["times_ms"] if tuned else None,
+           "roofline": roofline, "issue": issue, "dims": d, "tuning": tuned["times_ms"] if tuned else None,
            "bp_config": autotune.config_name(ctx.bp_config().key()),
            "dtype": "f32" if prec == T.PRECISION_FP32 else "f16-storage/f32-accumulate"}
     out["volume"] = vol
