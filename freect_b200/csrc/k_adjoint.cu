@@ -483,12 +483,23 @@ k_taps_grad(const float* __restrict__ raw, const float* __restrict__ gY, const f
   }
 }
 
-__global__ void k_taps_reduce(const float* __restrict__ partial, int nblk, int ntaps, float* __restrict__ out) {
-  const int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= ntaps) return;
+// One CTA per tap: thread i sums partials i, i + TR_THREADS, ... in double,
+// then a tree over the threads in a fixed order (deterministic).
+constexpr int TR_THREADS = 256;
+
+__global__ void __launch_bounds__(TR_THREADS)
+k_taps_reduce(const float* __restrict__ partial, int nblk, int ntaps, float* __restrict__ out) {
+  __shared__ double red[TR_THREADS];
+  const int d = blockIdx.x;
   double acc = 0.0;
-  for (int b = 0; b < nblk; b++) acc += (double)partial[(size_t)b * ntaps + d];
-  out[d] = (float)acc;
+  for (int b = threadIdx.x; b < nblk; b += TR_THREADS) acc += (double)partial[(size_t)b * ntaps + d];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = TR_THREADS / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[d] = (float)red[0];
 }
 
 }  // namespace
@@ -556,7 +567,7 @@ cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float*
   k_taps_grad<<<nblk, TG_THREADS, smem, s>>>(raw, gY, beta, bidx, p, ntaps, partial);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_taps_reduce<<<(ntaps + 127) / 128, 128, 0, s>>>(partial, nblk, ntaps, out);
+  k_taps_reduce<<<ntaps, TR_THREADS, 0, s>>>(partial, nblk, ntaps, out);
   return cudaGetLastError();
 }
 
