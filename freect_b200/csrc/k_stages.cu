@@ -1,6 +1,8 @@
 // Rebin, FP32 Toeplitz filter, thickening and table kernels (sm_100a).
 #include "wfbp_internal.h"
 
+#include <algorithm>
+
 #include <math.h>
 
 // ---------------------------------------------------------------------------
@@ -86,10 +88,33 @@ k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float*
   }
 }
 
+// Without a flying focal spot a sample's view and channel geometry does not
+// depend on the detector row: one thread per (view, output channel) computes
+// it once (wfbp_rebin_taps) and writes the channel's samples of every row,
+// consecutive threads on consecutive channels (coalesced loads and stores).
+constexpr int RBR_CH = 128;
+
+__global__ void __launch_bounds__(RBR_CH)
+k_rebin_f32_rows(const float* __restrict__ raw, float* __restrict__ out, const float* __restrict__ beta_t,
+                 const float* __restrict__ bidx_t, RebinParams p, int vb) {
+  const int v = vb + blockIdx.y;
+  const int c = blockIdx.x * RBR_CH + threadIdx.x;
+  if (c >= p.nch) return;
+  const RebinTaps t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+  float* o = out + (size_t)v * p.nr * p.nch + c;
+#pragma unroll 4
+  for (int i = 0; i < p.nr; i++) o[(size_t)i * p.nch] = rebin_taps_sample(t, i, p.nch);
+}
+
 cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, const float* d_bidx,
                              const RebinParams& p, cudaStream_t s, int vb, int ve) {
   if (ve < 0) ve = p.V;
   if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
+  if (p.G == 1) {
+    dim3 g((unsigned)((p.nch + RBR_CH - 1) / RBR_CH), (unsigned)(ve - vb));
+    k_rebin_f32_rows<<<g, RBR_CH, 0, s>>>(raw, out, d_beta, d_bidx, p, vb);
+    return cudaGetLastError();
+  }
   long rows = (long)(ve - vb) * p.nr;
   dim3 grid((unsigned)((rows + REB_ROWS - 1) / REB_ROWS), (unsigned)((p.nch + REB_QUADS * 4 - 1) / (REB_QUADS * 4)));
   k_rebin_f32<<<grid, REB_ROWS * REB_QUADS, 0, s>>>(raw, out, d_beta, d_bidx, p, vb, ve);
@@ -302,6 +327,61 @@ k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, _
   if (threadIdx.x == 0) view_scale[v] = s_vmax;
 }
 
+// k_rebin_split without a flying focal spot: one thread per channel of the
+// view (taps computed once) walks every row; the per-row maxima go through a
+// warp reduction and one shared-memory atomic per warp and row. The planes,
+// row scales and view scale are those of k_rebin_split.
+__global__ void __launch_bounds__(RS_THREADS)
+k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
+                   float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
+                   const float* __restrict__ bidx_t, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
+  extern __shared__ float s_rowmax[];  // [nrv]
+  const int v = vb + blockIdx.x;
+  const int lane = threadIdx.x % 32;
+  for (int i = threadIdx.x; i < nrv; i += blockDim.x) s_rowmax[i] = 0.0f;
+  __syncthreads();
+  // kp is a multiple of 64, so every warp is either wholly inside [0, kp) or wholly outside
+  for (int c = threadIdx.x; c < kp; c += blockDim.x) {
+    const bool valid = c < p.nch;
+    RebinTaps t;
+    t.ok = false;
+    if (valid) t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+    // four rows' samples (16 independent loads) before their stores and reductions
+    for (int i0 = 0; i0 < nrv; i0 += 4) {
+      float x[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        x[u] = i0 + u < p.nr ? rebin_taps_sample(t, i0 + u, p.nch) : 0.0f;  // 0 off the detector and in the padding
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + u;
+        if (i >= nrv) break;  // warp-uniform
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x[u]);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x[u] - __bfloat162float(hi));
+        const size_t row = (size_t)v * nrv + i;
+        a_hi[row * kp + c] = hi;
+        a_lo[row * kp + c] = lo;
+        // fmaxf semantics of k_rebin_split: a NaN sample does not raise the maximum
+        const float ax = isnan(x[u]) ? 0.0f : fabsf(x[u]);
+        const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(ax));  // ax >= 0: bits order as values
+        if (lane == 0 && m) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)m);
+      }
+    }
+  }
+  __syncthreads();
+  __shared__ float s_vmax;
+  if (threadIdx.x == 0) s_vmax = 0.0f;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nrv; i += blockDim.x) {
+    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
+    const float sc = exp2f(ceilf(log2f(bound)));
+    row_scale[(size_t)v * nrv + i] = sc;
+    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) view_scale[v] = s_vmax;
+}
+
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
                                const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
                                float taps_l1, cudaStream_t s, int vb, int ve) {
@@ -310,7 +390,11 @@ cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale,
   const size_t rows = (size_t)p.V * nrv;
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
   __nv_bfloat16* lo = hi + rows * kp;
-  k_rebin_split<<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(raw, hi, lo, row_scale, view_scale,
-                                                                             d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
+  if (p.G == 1 && kp % 64 == 0)
+    k_rebin_split_rows<<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
+        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
+  else
+    k_rebin_split<<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(raw, hi, lo, row_scale, view_scale,
+                                                                               d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
   return cudaGetLastError();
 }

@@ -14,9 +14,22 @@
 // the whole scan's index angle (v + voff) 2 pi / P, so a window of a scan
 // rebins exactly like the whole scan; texel rows are then taken relative to
 // the window (and clamped to it).
-__device__ __forceinline__ float rebin_sample(const float* __restrict__ rawrow, size_t view_stride, int V,
-                                              int nch, float bidx, float beta, int v, float dth, int q8, int voff) {
-  if (isnan(bidx)) return 0.0f;
+// The part of a sample that depends on the view and the output channel only
+// (not on the detector row): the clamped texel views and raw channels and the
+// two fractional weights. raw0/raw1 point at the two views' last raw row
+// (sheet row 0); sheet row i is nch floats earlier per row.
+struct RebinTaps {
+  const float* raw0;
+  const float* raw1;
+  int c0, c1;  // raw channels of the two texel columns
+  float ax, ay;
+  bool ok;     // false: the fan sample is outside the detector (bidx NaN), value 0
+};
+
+__device__ __forceinline__ RebinTaps rebin_taps(const float* __restrict__ raw, size_t view_stride, int V, int nr,
+                                                int nch, float bidx, float beta, int v, float dth, int q8, int voff) {
+  RebinTaps t;
+  t.ok = !isnan(bidx);
   float theta = (float)(v + voff) * dth;
   float alpha = theta - beta;
   float aidx = alpha / dth;
@@ -28,14 +41,28 @@ __device__ __forceinline__ float rebin_sample(const float* __restrict__ rawrow, 
     ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
     ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
   }
-  int x0 = (int)fx, y0 = (int)fy - voff;
+  int x0 = t.ok ? (int)fx : 0, y0 = (int)fy - voff;
   int x1 = min(max(x0 + 1, 0), nch - 1), y1 = min(max(y0 + 1, 0), V - 1);
   x0 = min(max(x0, 0), nch - 1);
   y0 = min(max(y0, 0), V - 1);
-  const float* r0 = rawrow + (size_t)y0 * view_stride;
-  const float* r1 = rawrow + (size_t)y1 * view_stride;
-  float t00 = __ldg(r0 + (nch - 1 - x0)), t10 = __ldg(r0 + (nch - 1 - x1));
-  float t01 = __ldg(r1 + (nch - 1 - x0)), t11 = __ldg(r1 + (nch - 1 - x1));
+  const float* last = raw + (size_t)(nr - 1) * nch;
+  t.raw0 = last + (size_t)y0 * view_stride;
+  t.raw1 = last + (size_t)y1 * view_stride;
+  t.c0 = nch - 1 - x0;
+  t.c1 = nch - 1 - x1;
+  t.ax = ax;
+  t.ay = ay;
+  return t;
+}
+
+// The bilinear sample of sheet row i (raw row nr-1-i) at the taps.
+__device__ __forceinline__ float rebin_taps_sample(const RebinTaps& t, int i, int nch) {
+  if (!t.ok) return 0.0f;
+  const float* r0 = t.raw0 - (size_t)i * nch;
+  const float* r1 = t.raw1 - (size_t)i * nch;
+  const float ax = t.ax, ay = t.ay;
+  float t00 = __ldg(r0 + t.c0), t10 = __ldg(r0 + t.c1);
+  float t01 = __ldg(r1 + t.c0), t11 = __ldg(r1 + t.c1);
   return (1.0f - ax) * (1.0f - ay) * t00 + ax * (1.0f - ay) * t10 + (1.0f - ax) * ay * t01 + ax * ay * t11;
 }
 
@@ -81,7 +108,14 @@ __device__ __forceinline__ float rebin_sample_ffs(const float* __restrict__ raw,
 __device__ __forceinline__ float wfbp_rebin_sample(const float* __restrict__ raw, const RebinParams& p, float bidx, float beta,
                                            int v, int i) {
   if (p.G > 1) return rebin_sample_ffs(raw, p, bidx, beta, v, i);
-  return rebin_sample(raw + (size_t)(p.nr - 1 - i) * p.nch, (size_t)p.nr * p.nch, p.V, p.nch, bidx, beta, v, p.dth,
-                      p.q8, p.voff);
+  const RebinTaps t = rebin_taps(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, bidx, beta, v, p.dth, p.q8, p.voff);
+  return rebin_taps_sample(t, i, p.nch);
+}
+
+// The taps of output channel (bidx, beta) of view v without a flying focal
+// spot (p.G == 1).
+__device__ __forceinline__ RebinTaps wfbp_rebin_taps(const float* __restrict__ raw, const RebinParams& p, float bidx,
+                                                     float beta, int v) {
+  return rebin_taps(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, bidx, beta, v, p.dth, p.q8, p.voff);
 }
 
