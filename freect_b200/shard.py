@@ -15,6 +15,10 @@ same views in the same order as a reconstruction of the whole scan: the
 stitched slabs equal it bit for bit. The only collective is the optional
 gather of the slabs to one rank at the end.
 
+A batch of scans shards by whole scans instead (assign_scans): each rank
+reconstructs its scans independently (one persistent batch launch per rank)
+and the volumes may be gathered to one rank at the end (gather_volumes).
+
 The reference has no multi-GPU path (ReconstructionMachine runs on one
 device, ReconstructionMachine.cu:141-434).
 """
@@ -151,3 +155,57 @@ def gather_slabs(slab, plans, rank, dst=0):
         dist.recv(buf, p.rank)
         parts.append(buf)
     return torch.cat(parts, dim=0)
+
+
+def scan_cost(cg, rp):
+    """Relative cost of reconstructing one scan: voxel columns x native slices x
+    views per rotation (a voxel of a slice collects about one rotation of
+    contributing views), the estimate the batch planner also sorts by."""
+    nat, _ = wfbp.slice_locations(wfbp.effective_geometry(cg), rp)
+    P = int(cg.projections_per_rotation) // _readings_per_view(cg)
+    return float(rp.nx) * float(rp.ny) * float(nat.size) * float(P)
+
+
+def assign_scans(costs, world):
+    """Whole scans to `world` ranks: largest estimated cost first, each onto the
+    rank with the least total so far (ties to the lower rank). Deterministic, so
+    every rank computes the same assignment. Returns one ascending list of scan
+    indices per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(a) for a in out]
+
+
+def gather_volumes(volumes, assignment, rank, shapes, dst=0, dtype=None, device=None):
+    """Collects the volumes of a batch on rank `dst` (point-to-point). volumes:
+    this rank's volumes in the order of assignment[rank]; shapes: the shape of
+    every scan's volume; dtype / device of the receive buffers (default: those
+    of this rank's first volume, else float32 on the CPU). Returns the list of
+    all volumes in scan order on dst, None elsewhere."""
+    import torch
+    import torch.distributed as dist
+    if dtype is None:
+        dtype = volumes[0].dtype if volumes else torch.float32
+    if device is None:
+        device = volumes[0].device if volumes else "cpu"
+    if rank != dst:
+        for v in volumes:
+            dist.send(v.contiguous(), dst)
+        return None
+    mine = dict(zip(assignment[dst], volumes))
+    out = [None] * len(shapes)
+    for r, scans_r in enumerate(assignment):
+        for i in scans_r:
+            if r == dst:
+                out[i] = mine[i]
+                continue
+            buf = torch.empty(tuple(shapes[i]), dtype=dtype, device=device)
+            dist.recv(buf, r)
+            out[i] = buf
+    return out

@@ -123,3 +123,54 @@ def test_sharded_oracle_ffs_matches_whole(orc):
     for world in (2, 3):
         parts = [_oracle_slab(orc, cg, rp, tube, table, raw, p) for p in shard.plan(cg, rp, table, world)]
         assert np.array_equal(np.concatenate(parts), ref, equal_nan=True), world
+
+
+def test_assign_scans_whole_and_balanced():
+    costs = [5.0, 1.0, 4.0, 2.0, 3.0]
+    a = shard.assign_scans(costs, 2)
+    assert a == [[0, 1, 3], [2, 4]]  # largest first onto the least-loaded rank
+    for world in (1, 3, 4, 7):
+        got = shard.assign_scans(costs, world)
+        assert sorted(i for r in got for i in r) == list(range(len(costs)))
+        loads = [sum(costs[i] for i in r) for r in got]
+        assert max(loads) - min(loads) <= max(costs)
+    with pytest.raises(ValueError):
+        shard.assign_scans(costs, 0)
+    # the cost estimate grows with the matrix and the slices
+    a = scans.tiny(nch=64, nr=6, P=96, rotations=3, nx=24, n_slices=4)
+    b = scans.tiny(nch=64, nr=6, P=96, rotations=3, nx=48, n_slices=8)
+    ca = shard.scan_cost(_geometry(a)[0], a.recon_config())
+    cb = shard.scan_cost(_geometry(b)[0], b.recon_config())
+    assert cb > 4 * ca
+
+
+def _batch_rank_main(rank, world, port, result_path):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        costs = [5.0, 1.0, 4.0, 2.0, 3.0]
+        shapes = [(2, 3, 4), (1, 2, 2), (3, 3, 3), (2, 2, 5), (1, 4, 4)]
+        a = shard.assign_scans(costs, world)
+        # this rank's "reconstructions": scan i's volume filled with i
+        mine = [torch.full(shapes[i], float(i)) for i in a[rank]]
+        got = shard.gather_volumes(mine, a, rank, shapes)
+        if rank == 0:
+            np.save(result_path, np.concatenate([g.numpy().ravel() for g in got]))
+            assert [tuple(g.shape) for g in got] == shapes
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batch_sharded_by_scan_two_ranks(tmp_path):
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "vols.npy")
+    mp.spawn(_batch_rank_main, args=(2, port, out), nprocs=2, join=True)
+    got = np.load(out)
+    shapes = [(2, 3, 4), (1, 2, 2), (3, 3, 3), (2, 2, 5), (1, 4, 4)]
+    ref = np.concatenate([np.full(int(np.prod(s)), float(i), np.float32) for i, s in enumerate(shapes)])
+    assert np.array_equal(got, ref)
