@@ -3,24 +3,27 @@
 // Same algorithm as backproject_kernel (cuda_kernels.cuh:198-287) and
 // k_bp (k_backproject.cu); this kernel is organised for throughput:
 //
-//  * Lanes are slices. A warp owns CPW (x, y) columns and the 32 consecutive
-//    native slices of a slab; lane l holds slice s0 + l of every column. The
-//    geometry of a (column, view) pair -- p_hat, l_hat, the asin term, the
-//    channel index and weight, and the row coordinate as a linear function of
-//    z -- is computed once, by one lane, and broadcast to the 32 lanes through
-//    shared memory.
+//  * Lanes are slices. A warp owns CPW (x, y) columns and the SL consecutive
+//    native slices of a slab (SL = 32, or 16 with the warp's lanes 0-15 and
+//    16-31 on two groups of CPW / 2 columns); lane l holds slice s0 + l % SL
+//    of its group's columns. The geometry of a (column, view) pair -- p_hat,
+//    l_hat, the asin term, the channel index and weight, and the row
+//    coordinate as a linear function of z -- is computed once, by one lane,
+//    and broadcast to the group's lanes through shared memory.
 //  * Filtered rows are read in the backprojection layout [view][channel][row]
-//    (rows contiguous), so the 32 lanes of a warp, which sit at consecutive
-//    rows of the same two channels, read consecutive shared-memory words.
+//    (rows contiguous), so the lanes of a column group, which sit at
+//    consecutive rows of the same two channels, read consecutive shared-memory
+//    words.
 //  * A producer warp walks the half-turn angles theta~ and, for each, selects
 //    the views j = theta~ + k P/2 whose table position can reach the CTA's
 //    slab (the reference's z cull, cuda_kernels.cuh:232, and the detector's
 //    cone), and TMA-loads the channel window each view needs for the CTA's
 //    column tile (all rows) into a 2-stage mbarrier ring.
-//  * For every column the 16 consumer warps accumulate sum(W g) and sum(W)
+//  * For every column the NW consumer warps accumulate sum(W g) and sum(W)
 //    over the staged views of theta~ and add (2 pi/P) sum(W g)/sum(W) to the
 //    column's slice in registers (NaN when no view contributes, like the
-//    reference).
+//    reference). In wfbp_run the write-back also forms the requested slices
+//    that lie inside the slab (fused thickening, bp_fused_thicken).
 //
 // Element types: float (FP32 rows) or uint32_t holding half2 pairs
 // (row r, row r+1) of FP16 rows scaled by a per-view power of two.
@@ -162,7 +165,7 @@ __device__ __forceinline__ void bp_fused_zero(const ThickFuse& tf, int bz, int w
   }
 }
 
-// One column tile (bt.tx x bt.ty columns, 32 slices from slab bz) of one scan.
+// One column tile (bt.tx x bt.ty columns, SL slices from slab bz) of one scan.
 // `ring` counts the theta~ steps this CTA has run through its two-stage
 // ring before this tile (stage = ring & 1, phase = (ring >> 1) & 1), so a
 // persistent CTA continues the barriers' phases from tile to tile. Returns

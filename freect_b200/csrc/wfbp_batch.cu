@@ -5,7 +5,7 @@
 // Per scan the rebin and filter stages run as their own launches (their
 // shapes differ from scan to scan); the backprojection of all scans is ONE
 // persistent launch (k_bp_tma_batch) whose CTAs take work items -- a column
-// tile and 32-slice slab of one scan -- from a list sorted by estimated
+// tile and slab (32 or 16 native slices) of one scan -- from a list sorted by estimated
 // cost, so uneven scans share the GPU without a tail per scan; thickening is
 // again per scan. The whole chain is captured once into a CUDA graph and
 // replayed while the caller's input and output pointers stay the same.
@@ -82,7 +82,7 @@ void free_plan(wfbp_batch* b) {
   b->n_items = 0;
 }
 
-// Views per theta~ reaching each 32-slice slab of a scan, summed over
+// Views per theta~ reaching each slab (of `slab` native slices) of a scan, summed over
 // theta~: the backprojection work of one column of that slab.
 std::vector<double> slab_view_counts(const wfbp_ctx* c, const std::vector<float>& view_z, int slab) {
   const int nslab = (c->nz + slab - 1) / slab;

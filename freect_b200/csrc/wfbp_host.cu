@@ -275,10 +275,11 @@ void mixed_scale_ptrs(const wfbp_ctx* ctx, P rebinned, float** row_sc, float** v
 
 // Sizes the TMA-staged backprojection for this geometry: the column tile, the
 // channel window each view needs for it, and the most views of one theta~ that
-// can reach a 32-slice slab. Returns false if no configuration fits in shared
+// can reach a slab. Returns false if no configuration fits in shared
 // memory (the generic kernel is used then).
 // Slab-level view reach and the most views of one theta~ that can reach a
-// 32-slice slab; both depend only on the geometry and the table positions.
+// 32-slice slab (a bound for 16-slice slabs too); both depend only on the
+// geometry and the table positions.
 void bp_reach(wfbp_ctx* ctx, const std::vector<float>& table) {
   const double R = ctx->cg.distance_source_to_isocenter;
   const double rmax = 0.5 * ctx->cg.acquisition_field_of_view;
