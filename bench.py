@@ -454,11 +454,8 @@ def run_batch(args, rank, world, local, dist):
         d2h = sum(v.numel() * 4 for v in vols)
 
         def e2e_step():
-            for a, b in zip(hr, raws):
-                b.copy_(a, non_blocking=True)
-            batch.run(raws, vols)
-            for a, b in zip(hv, vols):
-                a.copy_(b, non_blocking=True)
+            # wfbp_batch_run_host: the copies overlap the two backprojection launches
+            batch.run_host(hr, hv, stream=stream)
 
         with torch.cuda.stream(stream):
             e2e_step()

@@ -38,6 +38,14 @@ struct wfbp_batch {
   cudaGraphExec_t exec = nullptr;
   std::vector<const void*> key;
   std::string err;
+  std::vector<int4> h_items;          // the cost-sorted work list (host copy)
+  // wfbp_batch_run_host: device copies of the readings and volumes, the copy
+  // stream and its events, and the work list split into two launches
+  std::vector<float*> raw_d, vol_d;
+  cudaStream_t s_copy = nullptr;
+  std::vector<cudaEvent_t> ev;
+  int4* d_items_split = nullptr;
+  int split_k = -1, split_na = 0;
 };
 
 namespace {
@@ -77,9 +85,12 @@ void drop_graph(wfbp_batch* b) {
 void free_plan(wfbp_batch* b) {
   cudaFree(b->d_scans);
   cudaFree(b->d_items);
+  cudaFree(b->d_items_split);
   b->d_scans = nullptr;
   b->d_items = nullptr;
+  b->d_items_split = nullptr;
   b->n_items = 0;
+  b->split_k = -1;
 }
 
 // Views per theta~ reaching each slab (of `slab` native slices) of a scan, summed over
@@ -164,6 +175,7 @@ int build_plan(wfbp_batch* b) {
   BCUDA(b, cudaMalloc(&b->d_items, sizeof(int4) * std::max<size_t>(hw.size(), 1)));
   BCUDA(b, cudaMemcpy(b->d_items, hw.data(), sizeof(int4) * hw.size(), cudaMemcpyHostToDevice));
   b->n_items = (int)hw.size();
+  b->h_items = hw;
   b->smem = smem;
   int sms = 0;
   BCUDA(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
@@ -185,6 +197,10 @@ WFBP_API int wfbp_batch_destroy(wfbp_batch* b) {
     for (float* p : b->native) cudaFree(p);
     cudaFree(b->d_next);
     cudaFree(b->d_err);
+    for (float* p : b->raw_d) cudaFree(p);
+    for (float* p : b->vol_d) cudaFree(p);
+    for (auto e : b->ev) cudaEventDestroy(e);
+    if (b->s_copy) cudaStreamDestroy(b->s_copy);
     if (b->own) cudaStreamDestroy(b->own);
   }
   delete b;
@@ -368,4 +384,112 @@ WFBP_API int wfbp_batch_check_device_status(wfbp_batch* b) {
                  "the batched backprojection reported device error word " + std::to_string(h));
   }
   return WFBP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host buffers in, host buffers out
+// ---------------------------------------------------------------------------
+//
+// The readings are copied scan by scan on a copy stream. The scans split in
+// two groups in copy order: group A, the leading scans holding at least a
+// quarter of the readings' bytes, is rebinned, filtered and backprojected (one
+// persistent launch over its work items) as soon as its copies land, while
+// group B's copies continue; A's volumes are thickened and copied back while
+// group B is rebinned, filtered and backprojected (a second persistent
+// launch). Same kernels and per-voxel sums as wfbp_batch_run: the volumes are
+// identical. Synchronous, like wfbp_run_host.
+WFBP_API int wfbp_batch_run_host(wfbp_batch* b, const float* const* raws_host, float* const* volumes_host,
+                                 void* stream) {
+  if (!b) return WFBP_ERR_INVALID_ARG;
+  const int n = (int)b->ctx.size();
+  if (!raws_host || !volumes_host) return bfail(b, WFBP_ERR_INVALID_ARG, "wfbp_batch_run_host: null pointer array");
+  for (int i = 0; i < n; i++)
+    if (!raws_host[i] || !volumes_host[i])
+      return bfail(b, WFBP_ERR_INVALID_ARG, "wfbp_batch_run_host: null buffer for scan " + std::to_string(i));
+  DevGuard g(b->device);
+  const bool legacy = stream == nullptr;
+  cudaStream_t s = legacy ? b->own : (cudaStream_t)stream;
+  if (legacy) BCUDA(b, cudaStreamSynchronize(0));
+  std::vector<wfbp_dims> d(n);
+  double total = 0.0;
+  for (int i = 0; i < n; i++) {
+    wfbp_query(b->ctx[i], &d[i]);
+    total += (double)d[i].raw_bytes;
+  }
+  if (b->raw_d.empty()) {
+    b->raw_d.assign(n, nullptr);
+    b->vol_d.assign(n, nullptr);
+    for (int i = 0; i < n; i++) {
+      BCUDA(b, cudaMalloc(&b->raw_d[i], d[i].raw_bytes));
+      BCUDA(b, cudaMalloc(&b->vol_d[i], d[i].volume_bytes));
+    }
+  }
+  if (!b->s_copy) BCUDA(b, cudaStreamCreateWithFlags(&b->s_copy, cudaStreamNonBlocking));
+  if (b->ev.empty()) {
+    b->ev.assign(n + 2, nullptr);  // per scan copy, caller order, group A thickened
+    for (auto& e : b->ev) BCUDA(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // group A: the shortest prefix with at least a quarter of the bytes
+  int k = 0;
+  for (double acc = 0.0; k < n && (k == 0 || acc < 0.25 * total); k++) acc += (double)d[k].raw_bytes;
+  if (k >= n) k = n;
+  if (k != b->split_k) {
+    std::vector<int4> split;
+    split.reserve(b->h_items.size());
+    for (const int4& w : b->h_items)
+      if (w.x < k) split.push_back(w);  // stable: each group keeps the cost order
+    const int na = (int)split.size();
+    for (const int4& w : b->h_items)
+      if (w.x >= k) split.push_back(w);
+    cudaFree(b->d_items_split);
+    b->d_items_split = nullptr;
+    BCUDA(b, cudaMalloc(&b->d_items_split, sizeof(int4) * std::max<size_t>(split.size(), 1)));
+    BCUDA(b, cudaMemcpy(b->d_items_split, split.data(), sizeof(int4) * split.size(), cudaMemcpyHostToDevice));
+    b->split_k = k;
+    b->split_na = na;
+  }
+  // copies in scan order, after the caller's earlier work on its stream
+  BCUDA(b, cudaEventRecord(b->ev[n], s));
+  BCUDA(b, cudaStreamWaitEvent(b->s_copy, b->ev[n], 0));
+  for (int i = 0; i < n; i++) {
+    BCUDA(b, cudaMemcpyAsync(b->raw_d[i], raws_host[i], d[i].raw_bytes, cudaMemcpyHostToDevice, b->s_copy));
+    BCUDA(b, cudaEventRecord(b->ev[i], b->s_copy));
+  }
+  const int cpw = b->cfg.tile_x * b->cfg.tile_y / b->cfg.consumer_warps;
+  auto group = [&](int i0, int i1, const int4* items, int n_items) -> int {
+    for (int i = i0; i < i1; i++) {
+      BCUDA(b, cudaStreamWaitEvent(s, b->ev[i], 0));
+      int st = wfbp_rebin(b->ctx[i], b->raw_d[i], b->reb[i], s);
+      if (!st)
+        st = wfbp_detail::filter_stage(b->ctx[i], b->reb[i], b->filt[i], b->scales[i], WFBP_LAYOUT_BACKPROJECTION, s);
+      if (st) return bfail(b, st, "scan " + std::to_string(i) + ": " + wfbp_last_error(b->ctx[i]));
+    }
+    if (n_items > 0) {
+      BCUDA(b, cudaMemsetAsync(b->d_next, 0, sizeof(unsigned), s));
+      BCUDA(b, launch_backproject_tma_batch(b->precision == WFBP_PRECISION_MIXED ? 1 : 0, cpw, b->cfg.cols_per_step,
+                                            b->cfg.consumer_warps, b->cfg.slab, b->d_scans, items, n_items,
+                                            b->d_next, b->d_err, b->smem, b->grid, s));
+    }
+    for (int i = i0; i < i1; i++) {
+      int st = wfbp_thicken(b->ctx[i], b->native[i], b->vol_d[i], s);
+      if (st) return bfail(b, st, "scan " + std::to_string(i) + ": " + wfbp_last_error(b->ctx[i]));
+    }
+    return WFBP_OK;
+  };
+  int st = group(0, k, b->d_items_split, b->split_na);
+  if (st) return st;
+  // group A's volumes go back on the copy stream while group B runs
+  BCUDA(b, cudaEventRecord(b->ev[n + 1], s));
+  BCUDA(b, cudaStreamWaitEvent(b->s_copy, b->ev[n + 1], 0));
+  for (int i = 0; i < k; i++)
+    BCUDA(b, cudaMemcpyAsync(volumes_host[i], b->vol_d[i], d[i].volume_bytes, cudaMemcpyDeviceToHost, b->s_copy));
+  if (k < n) {
+    st = group(k, n, b->d_items_split + b->split_na, b->n_items - b->split_na);
+    if (st) return st;
+    for (int i = k; i < n; i++)
+      BCUDA(b, cudaMemcpyAsync(volumes_host[i], b->vol_d[i], d[i].volume_bytes, cudaMemcpyDeviceToHost, s));
+  }
+  BCUDA(b, cudaStreamSynchronize(b->s_copy));
+  BCUDA(b, cudaStreamSynchronize(s));
+  return wfbp_batch_check_device_status(b);
 }

@@ -61,6 +61,7 @@ _PROTOS = {
     "wfbp_batch_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.POINTER(_VP)]),
     "wfbp_batch_destroy": (C.c_int, [_VP]),
     "wfbp_batch_run": (C.c_int, [_VP, C.POINTER(_VP), C.POINTER(_VP), _VP]),
+    "wfbp_batch_run_host": (C.c_int, [_VP, C.POINTER(_VP), C.POINTER(_VP), _VP]),
     "wfbp_batch_size": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "wfbp_batch_bp_configs": (C.c_int, [_VP, C.POINTER(T.BpConfig), C.c_int, C.POINTER(C.c_int)]),
     "wfbp_batch_get_bp_config": (C.c_int, [_VP, C.POINTER(T.BpConfig)]),
@@ -475,6 +476,20 @@ class Batch:
         ra = (_VP * n)(*[_dptr(r).value for r in raws])
         va = (_VP * n)(*[_dptr(v).value for v in volumes])
         self._check(self._lib.wfbp_batch_run(self._h, ra, va, _stream(stream)), "wfbp_batch_run")
+
+    def run_host(self, raws_host, volumes_host, stream=None):
+        """wfbp_batch_run_host: raws_host / volumes_host are float32 host tensors
+        or arrays (pinned torch tensors overlap the copies with the work)."""
+        import torch
+        n = len(self.contexts)
+        if len(raws_host) != n or len(volumes_host) != n:
+            raise ValueError("need one raw and one volume buffer per scan")
+
+        def ptr(a):
+            return a.data_ptr() if isinstance(a, torch.Tensor) else a.ctypes.data
+        ra = (_VP * n)(*[ptr(r) for r in raws_host])
+        va = (_VP * n)(*[ptr(v) for v in volumes_host])
+        self._check(self._lib.wfbp_batch_run_host(self._h, ra, va, _stream(stream)), "wfbp_batch_run_host")
 
     def bp_configs(self):
         n = C.c_int()

@@ -406,6 +406,17 @@ typedef struct wfbp_batch wfbp_batch;
 int wfbp_batch_create(wfbp_ctx* const* ctxs, int n, wfbp_batch** out);
 int wfbp_batch_destroy(wfbp_batch* batch);
 int wfbp_batch_run(wfbp_batch* batch, const float* const* raws, float* const* volumes, void* stream);
+/* wfbp_batch_run from HOST buffers (pinned for overlap): the readings are
+ * copied scan by scan on a second stream; the leading scans holding a quarter
+ * of the readings' bytes are reconstructed (one persistent backprojection
+ * launch) while the remaining copies land, and their volumes are copied back
+ * while the rest of the batch runs (a second launch). The volumes equal
+ * wfbp_batch_run's. Synchronous. The batch keeps device copies of the
+ * readings and volumes after the first call. Like wfbp_run_host for one scan
+ * (ReconstructionMachine's host-in / host-out RunReconstruction,
+ * ReconstructionMachine.cu:141-434, over several scans). */
+int wfbp_batch_run_host(wfbp_batch* batch, const float* const* raws_host, float* const* volumes_host,
+                        void* stream);
 int wfbp_batch_size(const wfbp_batch* batch, int* n_scans, int* n_items);
 /* Backprojection configurations that fit every scan of the batch, and the
  * one in use (the autotuner times them and sets the fastest; setting one

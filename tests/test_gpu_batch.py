@@ -72,6 +72,30 @@ def test_batch_equals_per_scan_runs(orc, precision):
     batch.close()
 
 
+@pytest.mark.parametrize("precision", [T.PRECISION_FP32, T.PRECISION_MIXED])
+def test_batch_run_host_equals_per_scan_runs(orc, precision):
+    # host buffers in and out: the copies overlap the two backprojection
+    # launches (the leading quarter of the readings' bytes, then the rest);
+    # the volumes equal each scan's own wfbp_run, on two calls in a row
+    specs = scans.batch_specs(seed=5, n=7, reduced=True)
+    ctxs, raws = build(specs, precision, orc)
+    refs = []
+    for c, r in zip(ctxs, raws):
+        v = c.alloc("volume")
+        c.run(r, v)
+        refs.append(v.cpu())
+    batch = wfbp.Batch(ctxs)
+    raws_h = [r.cpu().pin_memory() for r in raws]
+    for it in range(2):
+        vols_h = [torch.full(tuple(ref.shape), -7.0, dtype=torch.float32).pin_memory() for ref in refs]
+        batch.run_host(raws_h, vols_h)
+        for i, (v, ref) in enumerate(zip(vols_h, refs)):
+            assert torch.equal(torch.nan_to_num(v, nan=123.0), torch.nan_to_num(ref, nan=123.0)), (it, i)
+    with pytest.raises(ValueError):
+        batch.run_host(raws_h[:-1], vols_h)
+    batch.close()
+
+
 def test_batch_mixed_vs_fp64(orc):
     specs = scans.batch_specs(seed=4, n=5, reduced=True)
     ctxs, raws = build(specs, T.PRECISION_MIXED, orc)
