@@ -317,10 +317,23 @@ def run_diff(args, rank, world, local, dist):
     raw_h = raw.detach().cpu().pin_memory()
     g_h = torch.empty(64, dtype=torch.float32).pin_memory()
 
+    copy_stream = torch.cuda.Stream(device=dev)
+    ready = [torch.cuda.Event() for _ in range(n_scans)]
+
     def e2e_step():
-        with torch.no_grad():
-            raw.copy_(raw_h, non_blocking=True)
-        l = step()
+        # scan b's readings are copied on a second stream while the forward
+        # reconstructs scan b - 1 (the forward waits for each scan's event)
+        copy_stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.no_grad(), torch.cuda.stream(copy_stream):
+            for b in range(n_scans):
+                raw[b].copy_(raw_h[b], non_blocking=True)
+                ready[b].record(copy_stream)
+        vol = rec(raw, taps, ready)
+        m = mask & torch.isfinite(vol)
+        l = ((vol - tgt)[m] ** 2).mean()
+        raw.grad = None
+        taps.grad = None
+        l.backward()
         g_h.copy_(taps.grad, non_blocking=True)
         return l.item()
 

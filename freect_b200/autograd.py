@@ -74,8 +74,11 @@ class Reconstructor:
             self._buf[name] = torch.empty(shape, dtype=torch.float32, device=self.device)
         return self._buf[name]
 
-    def __call__(self, raw, taps):
-        return WFBPFunction.apply(raw, taps, self)
+    def __call__(self, raw, taps, ready=None):
+        """ready: optional list of CUDA events, one per scan of a batched raw;
+        the forward waits for event b before it reads scan b (so the caller can
+        copy the scans in on another stream while earlier ones reconstruct)."""
+        return WFBPFunction.apply(raw, taps, self, ready)
 
 
 class WFBPFunction(torch.autograd.Function):
@@ -83,7 +86,7 @@ class WFBPFunction(torch.autograd.Function):
     or [readings][rows][channels]; taps: float32 CUDA [n_taps]."""
 
     @staticmethod
-    def forward(fctx, raw, taps, rec):
+    def forward(fctx, raw, taps, rec, ready=None):
         if raw.dtype != torch.float32 or taps.dtype != torch.float32:
             raise TypeError("raw and taps must be float32")
         batched = raw.dim() == 4
@@ -98,7 +101,11 @@ class WFBPFunction(torch.autograd.Function):
         d = ctx.dims
         out = torch.empty((rb.shape[0], d.n_slices_requested, d.ny, d.nx), dtype=torch.float32, device=raw.device)
         reb, filt, vn = rec.buf("rebinned"), rec.buf("filtered"), rec.buf("native")
+        if ready is not None and len(ready) != rb.shape[0]:
+            raise ValueError("need one ready event per scan")
         for b in range(rb.shape[0]):
+            if ready is not None:
+                torch.cuda.current_stream(raw.device).wait_event(ready[b])
             ctx.rebin(rb[b], reb)
             ctx.filter(reb, filt)
             ctx.backproject(filt, vn)
@@ -131,4 +138,4 @@ class WFBPFunction(torch.autograd.Function):
                 g_taps += t_b
         if need_raw and not fctx.batched:
             g_raw = g_raw[0]
-        return g_raw, g_taps, None
+        return g_raw, g_taps, None, None

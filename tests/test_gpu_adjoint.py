@@ -264,3 +264,19 @@ def test_autograd_batch_vs_fp64_gradient(orc):
         g_taps_ref += g_t
     gt = taps.grad.cpu().numpy().astype(np.float64)
     assert np.allclose(gt, g_taps_ref, rtol=2e-3, atol=2e-3 * np.abs(g_taps_ref).max())
+    # scans copied in on another stream, the forward waiting per scan: the same volumes
+    raw_h = raw.detach().cpu().pin_memory()
+    raw2 = torch.zeros_like(raw.detach())
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    ready = [torch.cuda.Event() for _ in range(4)]
+    with torch.cuda.stream(side):
+        for b in range(4):
+            raw2[b].copy_(raw_h[b], non_blocking=True)
+            ready[b].record(side)
+    with torch.no_grad():
+        vol2 = rec(raw2, taps, ready)
+    torch.cuda.synchronize()
+    assert torch.equal(torch.nan_to_num(vol2, nan=7.0), torch.nan_to_num(vol.detach(), nan=7.0))
+    with pytest.raises(ValueError):
+        rec(raw2, taps, ready[:2])
