@@ -53,71 +53,42 @@ cudaError_t launch_rebin_tables(float* d_beta, float* d_bidx, int nch, float c0,
 //
 #include "rebin_sample.cuh"
 
-// grid.x covers [V*nr] output rows (REB_ROWS per block), grid.y covers
-// channel quads; each thread writes 4 consecutive channels with one float4.
-constexpr int REB_ROWS = 4;
-constexpr int REB_QUADS = 64;
-
-__global__ void __launch_bounds__(REB_ROWS * REB_QUADS)
-k_rebin_f32(const float* __restrict__ raw, float* __restrict__ out, const float* __restrict__ beta_t,
-            const float* __restrict__ bidx_t, RebinParams p, int vb, int ve) {
-  __shared__ float s_beta[REB_QUADS * 4], s_bidx[REB_QUADS * 4];
-  const int tq = threadIdx.x % REB_QUADS, tr = threadIdx.x / REB_QUADS;
-  const int c_base = blockIdx.y * REB_QUADS * 4;
-  for (int t = threadIdx.x; t < REB_QUADS * 4; t += blockDim.x) {
-    int c = c_base + t;
-    s_beta[t] = c < p.nch ? beta_t[c] : 0.0f;
-    s_bidx[t] = c < p.nch ? bidx_t[c] : __int_as_float(0x7fc00000);
-  }
-  __syncthreads();
-  const long row = (long)vb * p.nr + (long)blockIdx.x * REB_ROWS + tr;
-  if (row >= (long)ve * p.nr) return;
-  const int v = (int)(row / p.nr), i = (int)(row % p.nr);
-  const int c = c_base + tq * 4;
-  float* o = out + (size_t)row * p.nch;
-  if (c + 3 < p.nch && (p.nch & 3) == 0) {
-    float4 r;
-    r.x = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 0], s_beta[tq * 4 + 0], v, i);
-    r.y = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 1], s_beta[tq * 4 + 1], v, i);
-    r.z = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 2], s_beta[tq * 4 + 2], v, i);
-    r.w = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + 3], s_beta[tq * 4 + 3], v, i);
-    *reinterpret_cast<float4*>(o + c) = r;
-  } else {
-    for (int u = 0; u < 4; u++)
-      if (c + u < p.nch) o[c + u] = wfbp_rebin_sample(raw, p, s_bidx[tq * 4 + u], s_beta[tq * 4 + u], v, i);
-  }
-}
-
-// Without a flying focal spot a sample's view and channel geometry does not
-// depend on the detector row: one thread per (view, output channel) computes
-// it once (wfbp_rebin_taps) and writes the channel's samples of every row,
-// consecutive threads on consecutive channels (coalesced loads and stores).
+// A sample's view and channel geometry does not depend on the detector row
+// (with a flying focal spot: only through the row's focal state, two tap
+// sets): one thread per (view, output channel) computes it once
+// (wfbp_rebin_taps / rebin_taps_ffs) and writes the channel's samples of every
+// row, consecutive threads on consecutive channels (coalesced loads and
+// stores). Same arithmetic per sample as rebin_sample / rebin_sample_ffs.
 constexpr int RBR_CH = 128;
 
+template <bool FFS>
 __global__ void __launch_bounds__(RBR_CH)
 k_rebin_f32_rows(const float* __restrict__ raw, float* __restrict__ out, const float* __restrict__ beta_t,
                  const float* __restrict__ bidx_t, RebinParams p, int vb) {
   const int v = vb + blockIdx.y;
   const int c = blockIdx.x * RBR_CH + threadIdx.x;
   if (c >= p.nch) return;
-  const RebinTaps t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
   float* o = out + (size_t)v * p.nr * p.nch + c;
+  if constexpr (FFS) {
+    const RebinTapsFfs T = rebin_taps_ffs(p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
 #pragma unroll 4
-  for (int i = 0; i < p.nr; i++) o[(size_t)i * p.nch] = rebin_taps_sample(t, i, p.nch);
+    for (int i = 0; i < p.nr; i++) o[(size_t)i * p.nch] = rebin_taps_ffs_sample(raw, p, T, i);
+  } else {
+    const RebinTaps t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+#pragma unroll 4
+    for (int i = 0; i < p.nr; i++) o[(size_t)i * p.nch] = rebin_taps_sample(t, i, p.nch);
+  }
 }
 
 cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, const float* d_bidx,
                              const RebinParams& p, cudaStream_t s, int vb, int ve) {
   if (ve < 0) ve = p.V;
   if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
-  if (p.G == 1) {
-    dim3 g((unsigned)((p.nch + RBR_CH - 1) / RBR_CH), (unsigned)(ve - vb));
-    k_rebin_f32_rows<<<g, RBR_CH, 0, s>>>(raw, out, d_beta, d_bidx, p, vb);
-    return cudaGetLastError();
-  }
-  long rows = (long)(ve - vb) * p.nr;
-  dim3 grid((unsigned)((rows + REB_ROWS - 1) / REB_ROWS), (unsigned)((p.nch + REB_QUADS * 4 - 1) / (REB_QUADS * 4)));
-  k_rebin_f32<<<grid, REB_ROWS * REB_QUADS, 0, s>>>(raw, out, d_beta, d_bidx, p, vb, ve);
+  dim3 g((unsigned)((p.nch + RBR_CH - 1) / RBR_CH), (unsigned)(ve - vb));
+  if (p.G == 1)
+    k_rebin_f32_rows<false><<<g, RBR_CH, 0, s>>>(raw, out, d_beta, d_bidx, p, vb);
+  else
+    k_rebin_f32_rows<true><<<g, RBR_CH, 0, s>>>(raw, out, d_beta, d_bidx, p, vb);
   return cudaGetLastError();
 }
 
@@ -273,7 +244,7 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // rebin for the mixed-precision filter
 // ---------------------------------------------------------------------------
 //
-// Same samples as k_rebin_f32, written as the two BF16 operand planes of the
+// Same samples as k_rebin_f32_rows, written as the two BF16 operand planes of the
 // tensor-core Toeplitz filter: hi = bf16(x), lo = bf16(x - hi). One CTA per
 // view; the view's rows are padded with zero rows to nrv (a power of two that
 // divides the filter's 128-row tile, so no view straddles a tile) and every
@@ -283,54 +254,10 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // value of the row), and per view the largest of its rows' scales.
 constexpr int RS_THREADS = 256;
 
-__global__ void __launch_bounds__(RS_THREADS)
-k_rebin_split(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
-              float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
-              const float* __restrict__ bidx_t, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
-  extern __shared__ float s_rowmax[];  // [nrv]
-  const int v = vb + blockIdx.x;
-  for (int i = threadIdx.x; i < nrv; i += RS_THREADS) s_rowmax[i] = 0.0f;
-  __syncthreads();
-  const int quads = kp / 4;
-  for (int e = threadIdx.x; e < nrv * quads; e += RS_THREADS) {
-    const int i = e / quads, c = (e % quads) * 4;
-    float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    if (i < p.nr) {
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (c + u < p.nch) x[u] = wfbp_rebin_sample(raw, p, __ldg(bidx_t + c + u), __ldg(beta_t + c + u), v, i);
-    }
-    __align__(8) __nv_bfloat16 hi[4], lo[4];
-    float amax = 0.0f;
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      hi[u] = __float2bfloat16_rn(x[u]);
-      lo[u] = __float2bfloat16_rn(x[u] - __bfloat162float(hi[u]));
-      amax = fmaxf(amax, fabsf(x[u]));
-    }
-    const size_t row = (size_t)v * nrv + i;
-    *reinterpret_cast<uint2*>(a_hi + row * kp + c) = *reinterpret_cast<uint2*>(hi);
-    *reinterpret_cast<uint2*>(a_lo + row * kp + c) = *reinterpret_cast<uint2*>(lo);
-    if (amax > 0.0f) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), __float_as_int(amax));  // amax >= 0
-  }
-  __syncthreads();
-  __shared__ float s_vmax;
-  if (threadIdx.x == 0) s_vmax = 0.0f;
-  __syncthreads();
-  for (int i = threadIdx.x; i < nrv; i += RS_THREADS) {
-    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
-    const float sc = exp2f(ceilf(log2f(bound)));
-    row_scale[(size_t)v * nrv + i] = sc;
-    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) view_scale[v] = s_vmax;
-}
-
-// k_rebin_split without a flying focal spot: one thread per channel of the
-// view (taps computed once) walks every row; the per-row maxima go through a
-// warp reduction and one shared-memory atomic per warp and row. The planes,
-// row scales and view scale are those of k_rebin_split.
+// One thread per channel of the view computes the channel's taps once
+// (as k_rebin_f32_rows) and walks every row; the per-row maxima go through a
+// warp reduction and one shared-memory atomic per warp and row.
+template <bool FFS>
 __global__ void __launch_bounds__(RS_THREADS)
 k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
                    float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
@@ -344,14 +271,20 @@ k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_
   for (int c = threadIdx.x; c < kp; c += blockDim.x) {
     const bool valid = c < p.nch;
     RebinTaps t;
+    RebinTapsFfs tf;
     t.ok = false;
-    if (valid) t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+    tf.ok = false;
+    if (valid) {
+      if constexpr (FFS) tf = rebin_taps_ffs(p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+      else t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+    }
     // four rows' samples (16 independent loads) before their stores and reductions
     for (int i0 = 0; i0 < nrv; i0 += 4) {
       float x[4];
 #pragma unroll
       for (int u = 0; u < 4; u++)
-        x[u] = i0 + u < p.nr ? rebin_taps_sample(t, i0 + u, p.nch) : 0.0f;  // 0 off the detector and in the padding
+        x[u] = i0 + u >= p.nr ? 0.0f  // 0 off the detector and in the padding
+               : FFS ? rebin_taps_ffs_sample(raw, p, tf, i0 + u) : rebin_taps_sample(t, i0 + u, p.nch);
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const int i = i0 + u;
@@ -361,7 +294,7 @@ k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_
         const size_t row = (size_t)v * nrv + i;
         a_hi[row * kp + c] = hi;
         a_lo[row * kp + c] = lo;
-        // fmaxf semantics of k_rebin_split: a NaN sample does not raise the maximum
+        // fmaxf semantics: a NaN sample does not raise the maximum
         const float ax = isnan(x[u]) ? 0.0f : fabsf(x[u]);
         const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(ax));  // ax >= 0: bits order as values
         if (lane == 0 && m) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)m);
@@ -390,11 +323,12 @@ cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale,
   const size_t rows = (size_t)p.V * nrv;
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
   __nv_bfloat16* lo = hi + rows * kp;
-  if (p.G == 1 && kp % 64 == 0)
-    k_rebin_split_rows<<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
+  if (kp % 64 != 0) return cudaErrorInvalidValue;  // whole warps per channel run (the row maxima's reduction)
+  if (p.G == 1)
+    k_rebin_split_rows<false><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
         raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
   else
-    k_rebin_split<<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(raw, hi, lo, row_scale, view_scale,
-                                                                               d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
+    k_rebin_split_rows<true><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
+        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
   return cudaGetLastError();
 }

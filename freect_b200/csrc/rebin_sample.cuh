@@ -103,6 +103,63 @@ __device__ __forceinline__ float rebin_sample_ffs(const float* __restrict__ raw,
   return val;
 }
 
+// rebin_sample_ffs split like RebinTaps: for output channel (bidx, beta) of
+// view v, the two focal-state row parities (zs) each have two effective
+// channel taps (weight we, reading weight ay, the two readings' offsets from
+// the raw row); only the raw row depends on the detector row. The sum runs
+// in rebin_sample_ffs's order.
+struct RebinTapsFfs {
+  float we[2][2], ay[2][2];
+  size_t oa[2][2], ob[2][2];
+  bool ok;
+};
+
+__device__ __forceinline__ RebinTapsFfs rebin_taps_ffs(const RebinParams& p, float bidx, float beta, int v) {
+  RebinTapsFfs T;
+  T.ok = !isnan(bidx);
+  const size_t vs = (size_t)p.nr_raw * p.nch_raw;
+  const float nf = ((float)(p.G * (v + p.voff)) * p.dth - beta) / p.dth;
+  const float fx = T.ok ? floorf(bidx) : 0.0f;
+  float ax = T.ok ? bidx - fx : 0.0f;
+  if (p.q8) ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
+#pragma unroll
+  for (int zs = 0; zs < 2; zs++)
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int e = min(max((int)fx + t, 0), p.nch - 1);
+      T.we[zs][t] = t ? ax : 1.0f - ax;
+      const int sp = p.phi ? (e & 1) : 0, b = p.phi ? (e >> 1) : e;
+      const int z = p.zf ? zs : 0;
+      const int rho = (p.G == 4) ? sp + 2 * z : (p.phi ? sp : z);
+      const float mf = (nf - (float)rho) / (float)p.G, m0 = floorf(mf);
+      float ay = mf - m0;
+      if (p.q8) ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
+      T.ay[zs][t] = ay;
+      const int ma = min(max((int)m0 - p.voff, 0), p.V - 1), mb = min(max((int)m0 + 1 - p.voff, 0), p.V - 1);
+      T.oa[zs][t] = (size_t)(p.G * ma + rho) * vs + (size_t)(p.nch_raw - 1 - b);
+      T.ob[zs][t] = (size_t)(p.G * mb + rho) * vs + (size_t)(p.nch_raw - 1 - b);
+    }
+  return T;
+}
+
+// Sample of effective row ie at the taps (rebin_sample_ffs's value).
+__device__ __forceinline__ float rebin_taps_ffs_sample(const float* __restrict__ raw, const RebinParams& p,
+                                                       const RebinTapsFfs& T, int ie) {
+  if (!T.ok) return 0.0f;
+  const int zs = p.zf ? (ie & 1) : 0, iraw = p.zf ? (ie >> 1) : ie;
+  const float* rawrow = raw + (size_t)(p.nr_raw - 1 - iraw) * p.nch_raw;
+  float val = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const float we = zs ? T.we[1][t] : T.we[0][t];
+    const float ay = zs ? T.ay[1][t] : T.ay[0][t];
+    const float t0 = __ldg(rawrow + (zs ? T.oa[1][t] : T.oa[0][t]));
+    const float t1 = __ldg(rawrow + (zs ? T.ob[1][t] : T.ob[0][t]));
+    val += we * ((1.0f - ay) * t0 + ay * t1);
+  }
+  return val;
+}
+
 // One rebinned sample of output view v, row i (flipped row-sheet index),
 // output channel with table entries (bidx, beta).
 __device__ __forceinline__ float wfbp_rebin_sample(const float* __restrict__ raw, const RebinParams& p, float bidx, float beta,
