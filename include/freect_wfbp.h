@@ -17,7 +17,12 @@
  *   - every call takes an explicit CUDA stream (passed as void*),
  *   - errors are returned as status codes instead of exit() (the reference's
  *     gpuErrChk/cufftErrChk call exit(), gpu_error_check.h:38-58),
- *   - no call synchronises the device unless documented.
+ *   - no call synchronises the device unless documented,
+ *   - a context's own scratch (wfbp_run's intermediates, the adjoint's weight
+ *     table, the fused-thickening lists) is shared by the calls on it: call a
+ *     context from one host thread at a time, and do not let wfbp_run /
+ *     wfbp_run_host / the backprojection adjoint of one context overlap on
+ *     the GPU (stage calls into caller buffers on different streams may).
  *
  * All structs keep the reference's field order and types, so host code that
  * fills the reference's structs can pass them unchanged.
