@@ -40,6 +40,7 @@ struct TcParams {
   int BN;         // N tile
   int kblocks;    // Kp / 64
   int np;         // padded N (rows of one B plane)
+  int n_fast;     // 1: blockIdx.x is the N tile (an M tile's N tiles run together and share its A tile in L2)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -118,7 +119,8 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   __shared__ float s_xchg[4][16];  // row 32w of each warp, for the pairs of the warp above
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int m0 = p.mb + blockIdx.x * TC_BM, n0 = blockIdx.y * p.BN;
+  const int mt = p.n_fast ? (int)blockIdx.y : (int)blockIdx.x, nt = p.n_fast ? (int)blockIdx.x : (int)blockIdx.y;
+  const int m0 = p.mb + mt * TC_BM, n0 = nt * p.BN;
 
   if (threadIdx.x == 0) {
     s_fail = 0;
@@ -199,7 +201,7 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     float inv = 1.0f;
     if (o.mode == TC_OUT_F16_ROWS && row_ok) {
       inv = 1.0f / o.row_scale_in[m];
-      if (blockIdx.y == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
+      if (nt == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
     } else if (o.mode == TC_OUT_PAIRS && m < p.me) {
       inv = 1.0f / o.view_scale[v];
     }
@@ -327,7 +329,9 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
   size_t smem = tc_smem_bytes(bn);
   cudaError_t e = cudaFuncSetAttribute(k_toeplitz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((me - mb + TC_BM - 1) / TC_BM), (unsigned)(np / bn));
+  const unsigned mtiles = (unsigned)((me - mb + TC_BM - 1) / TC_BM), ntiles = (unsigned)(np / bn);
+  p.n_fast = mtiles <= 65535u ? 1 : 0;  // gridDim.y limit
+  const dim3 grid = p.n_fast ? dim3(ntiles, mtiles) : dim3(mtiles, ntiles);
   k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(map_a, map_b, p, out, err);
   return cudaGetLastError();
 }
