@@ -1332,11 +1332,27 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[kChunks], s));
   CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_copy, ctx->ev_copy[kChunks], 0));
   const int nchunk = (V + cv - 1) / cv;
-  for (int c = 0; c < nchunk; c++) {
-    const size_t r0 = (size_t)c * cv * G, r1 = (size_t)std::min(V, (c + 1) * cv) * G;
-    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->s_raw + r0 * frame, raw_host + r0 * frame, sizeof(float) * (r1 - r0) * frame,
-                                  cudaMemcpyHostToDevice, ctx->s_copy));
-    CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[c], ctx->s_copy));
+  // From pinned memory every chunk copy is queued at once (the copy stream
+  // then streams them back to back, ahead of the early copies of finished
+  // slices). From pageable memory a copy holds the host until it is staged,
+  // so each is issued just before the first work that needs it and the work
+  // queued before it keeps the GPU busy meanwhile.
+  int copies_issued = 0;
+  auto issue_copies = [&](int upto) -> int {
+    for (; copies_issued <= upto; copies_issued++) {
+      const int c = copies_issued;
+      const size_t r0 = (size_t)c * cv * G, r1 = (size_t)std::min(V, (c + 1) * cv) * G;
+      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->s_raw + r0 * frame, raw_host + r0 * frame,
+                                    sizeof(float) * (r1 - r0) * frame, cudaMemcpyHostToDevice, ctx->s_copy));
+      CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[c], ctx->s_copy));
+    }
+    return WFBP_OK;
+  };
+  {
+    cudaPointerAttributes ra;
+    const bool raw_pinned = cudaPointerGetAttributes(&ra, raw_host) == cudaSuccess && ra.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (raw_pinned && (st = issue_copies(nchunk - 1))) return st;
   }
   // last view each slab needs: views j < K P/2 within the slab's reach in z
   const int SLB = ctx->bpt.slab;
@@ -1419,6 +1435,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   for (int c = 0; c < nchunk; c++) {
     const int vb = c * cv, ve = std::min(V, (c + 1) * cv);
     const int last = std::min(nchunk - 1, (std::min(V, ve + reach) - 1) / cv);
+    if ((st = issue_copies(last))) return st;
     CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->ev_copy[last], 0));
     if ((st = do_rebin(ctx, ctx->s_raw, ctx->s_rebinned, vb, ve, s))) return st;
     if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, s, vb, ve))) return st;
