@@ -448,16 +448,31 @@ WFBP_API int wfbp_batch_run_host(wfbp_batch* b, const float* const* raws_host, f
     b->split_k = k;
     b->split_na = na;
   }
-  // copies in scan order, after the caller's earlier work on its stream
+  // copies in scan order, after the caller's earlier work on its stream. From
+  // pinned memory all are queued at once; from pageable memory (a copy holds
+  // the host until it is staged) each just before its scan's work, so the
+  // work queued earlier keeps the GPU busy meanwhile.
+  bool pinned = true;
+  for (int i = 0; i < n && pinned; i++) {
+    cudaPointerAttributes pa;
+    pinned = cudaPointerGetAttributes(&pa, raws_host[i]) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  }
+  cudaGetLastError();
   BCUDA(b, cudaEventRecord(b->ev[n], s));
   BCUDA(b, cudaStreamWaitEvent(b->s_copy, b->ev[n], 0));
-  for (int i = 0; i < n; i++) {
+  auto copy_in = [&](int i) -> int {
     BCUDA(b, cudaMemcpyAsync(b->raw_d[i], raws_host[i], d[i].raw_bytes, cudaMemcpyHostToDevice, b->s_copy));
     BCUDA(b, cudaEventRecord(b->ev[i], b->s_copy));
-  }
+    return WFBP_OK;
+  };
+  if (pinned)
+    for (int i = 0; i < n; i++)
+      if (int e = copy_in(i)) return e;
   const int cpw = b->cfg.tile_x * b->cfg.tile_y / b->cfg.consumer_warps;
   auto group = [&](int i0, int i1, const int4* items, int n_items) -> int {
     for (int i = i0; i < i1; i++) {
+      if (!pinned)
+        if (int e = copy_in(i)) return e;
       BCUDA(b, cudaStreamWaitEvent(s, b->ev[i], 0));
       int st = wfbp_rebin(b->ctx[i], b->raw_d[i], b->reb[i], s);
       if (!st)
@@ -478,17 +493,18 @@ WFBP_API int wfbp_batch_run_host(wfbp_batch* b, const float* const* raws_host, f
   };
   int st = group(0, k, b->d_items_split, b->split_na);
   if (st) return st;
-  // group A's volumes go back on the copy stream while group B runs
+  // group A's volumes go back on the copy stream while group B runs (issued
+  // after group B's work is queued: a copy to pageable memory holds the host)
   BCUDA(b, cudaEventRecord(b->ev[n + 1], s));
-  BCUDA(b, cudaStreamWaitEvent(b->s_copy, b->ev[n + 1], 0));
-  for (int i = 0; i < k; i++)
-    BCUDA(b, cudaMemcpyAsync(volumes_host[i], b->vol_d[i], d[i].volume_bytes, cudaMemcpyDeviceToHost, b->s_copy));
   if (k < n) {
     st = group(k, n, b->d_items_split + b->split_na, b->n_items - b->split_na);
     if (st) return st;
-    for (int i = k; i < n; i++)
-      BCUDA(b, cudaMemcpyAsync(volumes_host[i], b->vol_d[i], d[i].volume_bytes, cudaMemcpyDeviceToHost, s));
   }
+  BCUDA(b, cudaStreamWaitEvent(b->s_copy, b->ev[n + 1], 0));
+  for (int i = 0; i < k; i++)
+    BCUDA(b, cudaMemcpyAsync(volumes_host[i], b->vol_d[i], d[i].volume_bytes, cudaMemcpyDeviceToHost, b->s_copy));
+  for (int i = k; i < n; i++)
+    BCUDA(b, cudaMemcpyAsync(volumes_host[i], b->vol_d[i], d[i].volume_bytes, cudaMemcpyDeviceToHost, s));
   BCUDA(b, cudaStreamSynchronize(b->s_copy));
   BCUDA(b, cudaStreamSynchronize(s));
   return wfbp_batch_check_device_status(b);

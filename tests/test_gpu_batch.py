@@ -91,6 +91,12 @@ def test_batch_run_host_equals_per_scan_runs(orc, precision):
         batch.run_host(raws_h, vols_h)
         for i, (v, ref) in enumerate(zip(vols_h, refs)):
             assert torch.equal(torch.nan_to_num(v, nan=123.0), torch.nan_to_num(ref, nan=123.0)), (it, i)
+    # pageable host arrays: the copies are issued scan by scan, same volumes
+    raws_n = [r.numpy().copy() for r in raws_h]
+    vols_n = [np.full(tuple(ref.shape), -7.0, np.float32) for ref in refs]
+    batch.run_host(raws_n, vols_n)
+    for i, (v, ref) in enumerate(zip(vols_n, refs)):
+        assert np.array_equal(v, ref.numpy(), equal_nan=True), i
     with pytest.raises(ValueError):
         batch.run_host(raws_h[:-1], vols_h)
     batch.close()
