@@ -9,6 +9,10 @@ it. Inputs (2.2 GB raw frames) are larger than L2, so no flush is needed.
 By default both precision forms run: the mixed form is the headline line,
 the FP32 form is reported beside it ("fp32", "mixed_speedup_vs_fp32"), and
 each form's volume is checked in HU against the FP64 oracle on one slab.
+The rows64 line also carries "batch24": the 24 seeded uneven scans
+reconstructed as one batch (mixed form, one persistent backprojection launch,
+CUDA graph) against per-scan FP32 launches, with each scan's HU error against
+the FP64 oracle on its middle slab (--no-batch skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision both|fp32|mixed] [--workload rows64|small|ffs|batch24|...]
@@ -56,20 +60,27 @@ def parse():
     ap.add_argument("--workload", default="rows64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-slices", type=int, default=1)
+    ap.add_argument("--cpu-slices", type=int, default=8,
+                    help="native slices the CPU baseline backprojects (spread over one rotation's feed)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default backprojection configuration")
     ap.add_argument("--no-hu", action="store_true", help="skip the HU check against the FP64 oracle")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="rows64: skip the batch24 summary (24 uneven scans, one persistent launch)")
+    ap.add_argument("--batch-hu-scans", type=int, default=24,
+                    help="batch24 summary: scans checked against the FP64 oracle on their middle slab")
     ap.add_argument("--bp-config", default=None,
                     help="fixed backprojection configuration, e.g. 16x20/8w20s16 (no tuning)")
     return ap.parse_args()
 
 
 def load_peaks():
+    """(HBM GB/s, BF16 TFLOP/s burst, BF16 TFLOP/s sustained, source)."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
-    return 6650.0, 1590.0, "fallback"
+        return (d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0),
+                "measured")
+    return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 class ClockSampler:
@@ -126,11 +137,26 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(spec, raw_host_fn, n_slices=1):
+def baseline_positions(spec, cg, rp, n=8):
+    """n native slice indices spread evenly over one rotation's table feed
+    centred on the middle of the native slice list: where the CPU baseline
+    samples the backprojection."""
+    from oracle import oracle as O
+    zn, _ = O.slice_locations(cg, rp)
+    mid = zn.size // 2
+    span = max(1, int(round(spec.feed / max(1e-6, abs(float(zn[1] - zn[0]))))))  # native slices per rotation
+    lo = max(0, mid - span // 2)
+    hi = min(zn.size, lo + span)
+    step = max(1, (hi - lo) // n)
+    return [int(lo + step * i) for i in range(n) if lo + step * i < hi]
+
+
+def cpu_baseline(spec, raw_host_fn, positions):
     """The reference's path on the host cores (the oracle's FP32 transcript,
-    all threads): rebin+filter of the view window one slice needs, and the
-    backprojection of n_slices slices at full resolution; scaled to the full
-    volume linearly in views and slices."""
+    all threads): rebin+filter of the window of views the sampled native
+    slices need, and the backprojection of those slices at full
+    resolution; scaled to the full volume linearly in views (rebin+filter)
+    and in slices (backprojection)."""
     import numpy as np
     from freect_b200 import scans  # noqa: F401
     from oracle import oracle as O
@@ -140,10 +166,9 @@ def cpu_baseline(spec, raw_host_fn, n_slices=1):
     cg, gp = O.configure_geometry(spec.meta(), table)
     rp = spec.recon_config()
     zn, zr = O.slice_locations(cg, rp)
-    mid = zn.size // 2
-    zs = zn[mid:mid + n_slices]
+    zs = zn[np.asarray(positions)]
     # views that pass the z cull for these slices, plus the rebin's view reach
-    sel = np.nonzero(np.abs(table - zs.mean()) <= cg.z_rot + 1.0)[0]
+    sel = np.nonzero((table >= zs.min() - cg.z_rot - 1.0) & (table <= zs.max() + cg.z_rot + 1.0))[0]
     reach = int(math.ceil(0.5 * spec.nch * spec.dbeta / (2 * math.pi / spec.P))) + 2
     v0 = max(0, sel[0] - reach)
     v0 -= v0 % (spec.P // 2)  # keep half-turn alignment of theta~
@@ -167,44 +192,55 @@ def cpu_baseline(spec, raw_host_fn, n_slices=1):
     t_rf_full = (t1 - t0) * spec.V / float(v1 - v0)
     t_bp_full = (t2 - t1) * zn.size / float(zs.size)
     return {"t_rf_sample": t1 - t0, "t_bp_sample": t2 - t1, "views": int(v1 - v0), "slices": int(zs.size),
+            "positions": [int(x) for x in positions], "native_slices": int(zn.size),
             "updates_sample": int(n_sample), "t_full_est": t_rf_full + t_bp_full, "cores": nthreads,
-            "bp_updates_per_s": n_sample / (t2 - t1)}
+            "bp_updates_per_s": n_sample / (t2 - t1), "updates_full_est": n_sample * zn.size / float(zs.size)}
 
 
 def run_reference(args, rank):
-    """--impl reference: the reference's path on host cores, bounded sample per step."""
+    """--impl reference: the reference's path on host cores, bounded sample
+    per step: step i rebins and filters the view window of native slice
+    position i mod 8 (8 positions spread over one rotation's table feed at
+    the centre of the volume) and backprojects that slice; each step's time
+    is scaled to the full volume, the line reports the median."""
     import numpy as np
     from freect_b200 import scans
     from oracle import oracle as O
     spec = scans.WORKLOADS[args.workload]()
+    tube, table = spec.views()
+    cg, _ = O.configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    positions = baseline_positions(spec, cg, rp)
     cache = {}
 
     def raw_host(v0, v1):
-        if (v0, v1) not in cache:
-            sub = scans.ScanSpec(**{**spec.__dict__})
-            s = spec.synth()
-            s.n_readings = v1 - v0
-            s.angle0 = s.angle0 + v0 * s.dangle
-            s.z0 = s.z0 + v0 * s.dz
-            cache[(v0, v1)] = O.synth_project(s, spec.ellipsoids())
+        for (a, b), arr in cache.items():
+            if a <= v0 and v1 <= b:
+                return arr[v0 - a:v1 - a]
+        s = spec.synth()
+        s.n_readings = v1 - v0
+        s.angle0 = s.angle0 + v0 * s.dangle
+        s.z0 = s.z0 + v0 * s.dz
+        cache[(v0, v1)] = O.synth_project(s, spec.ellipsoids())
         return cache[(v0, v1)]
 
-    full_updates = None
+    # one synthesis of the window all positions need (outside the timed steps)
+    first = cpu_baseline(spec, raw_host, positions)
     times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(spec, raw_host, n_slices=args.cpu_slices)
+        r = cpu_baseline(spec, raw_host, [positions[i % len(positions)]])
         if i >= args.warmup:
             times.append(r)
-    est = sorted(t["t_full_est"] for t in times)[len(times) // 2]
-    # updates of the full volume: per-slice sample count x slices
-    tube, table = spec.views()
-    cg, _ = O.configure_geometry(spec.meta(), table)
-    zn, _ = O.slice_locations(cg, spec.recon_config())
-    full_updates = times[0]["updates_sample"] * zn.size / times[0]["slices"]
+    ests = sorted(t["t_full_est"] for t in times)
+    est = ests[len(ests) // 2]
+    full_updates = first["updates_full_est"]
     value = full_updates / est
-    sample = ("oracle FP32 transcript (q8 texture weights) on %d host threads: rebin+filter of %d of %d views and "
-              "backprojection of %d of %d native slices at %dx%d, scaled linearly to the full volume"
-              % (times[0]["cores"], times[0]["views"], spec.V, times[0]["slices"], zn.size, spec.nx, spec.ny))
+    sample = ("oracle FP32 transcript (q8 texture weights) on %d host threads; each step: rebin+filter of the ~%d "
+              "views one native slice needs (of %d) and the backprojection of that slice at %dx%d, scaled linearly "
+              "to the full volume (%d native slices); the step's slice cycles through %d positions spread over one "
+              "rotation's table feed; median over steps; updates from the FP64 count of all %d positions"
+              % (times[0]["cores"], times[0]["views"], spec.V, spec.nx, spec.ny, first["native_slices"],
+                 len(positions), len(positions)))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": est * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom)",
@@ -213,7 +249,9 @@ def run_reference(args, rank):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": times[0]["cores"], "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "s_per_volume": est}
+            "s_per_volume": est, "sample_seconds_per_step": sorted(t["t_rf_sample"] + t["t_bp_sample"]
+                                                                   for t in times)[len(times) // 2],
+            "s_per_volume_range": [ests[0], ests[-1]]}
     print(json.dumps(line))
 
 
@@ -367,19 +405,24 @@ def run_diff(args, rank, world, local, dist):
         print(json.dumps(line))
 
 
-def run_batch(args, rank, world, local, dist):
-    """--workload batch24: 24 seeded uneven scans reconstructed as one batch
-    (mixed form: per-scan rebin + tensor-core filter, ONE persistent
-    backprojection launch over all scans, per-scan thickening, replayed as a
-    CUDA graph), against the same scans as per-scan FP32 launches."""
+def measure_batch(args, rank, world, local, dist, candidates=None, hu_scans=24, steps=None, warmup=None):
+    """24 seeded uneven scans reconstructed as one batch (mixed form: per-scan
+    rebin + tensor-core filter, ONE persistent backprojection launch over all
+    scans, per-scan thickening, replayed as a CUDA graph), against the same
+    scans as per-scan FP32 launches; each of the first `hu_scans` scans'
+    mixed volume against the FP64 oracle on its middle slab. candidates:
+    backprojection configuration names the batch autotuner may try (None:
+    all that fit). Returns the summary dict."""
     import numpy as np
     import torch
     from freect_b200 import abi_types as T
     from freect_b200 import autotune, scans, wfbp
 
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     dev = torch.device("cuda", local)
     specs = scans.batch_specs(seed=rank, n=24)
-    ctxs, raws, vols = [], [], []
+    ctxs, raws, vols, views = [], [], [], []
     for sp in specs:
         tube, table = sp.views()
         cg, gp = wfbp.configure_geometry(sp.meta(), table)
@@ -387,6 +430,7 @@ def run_batch(args, rank, world, local, dist):
                          device=local)
         c.set_views(tube, table)
         ctxs.append(c)
+        views.append((cg, tube, table))
         r = c.alloc("raw")
         wfbp.synth_project(sp.synth(), sp.ellipsoids(), r)
         raws.append(r)
@@ -394,11 +438,13 @@ def run_batch(args, rank, world, local, dist):
     torch.cuda.synchronize()
     batch = wfbp.Batch(ctxs)
     stream = torch.cuda.Stream(device=dev)
-    tuned = None if args.no_tune else autotune.tune_batch(batch, raws, vols, use_cache=False)
+    tuned = None
+    if not args.no_tune:
+        tuned = autotune.tune_batch(batch, raws, vols, use_cache=False, candidates=candidates)
 
     # per-scan FP32 launches (the comparison) and the contributing updates
     # (counted once per scan by the FP32 form, outside every timed region)
-    updates, fp32_ms, hu = 0, 0.0, []
+    updates, fp32_ms, v32s = 0, 0.0, []
     for sp, r, v in zip(specs, raws, vols):
         tube, table = sp.views()
         cg, gp = wfbp.configure_geometry(sp.meta(), table)
@@ -420,21 +466,21 @@ def run_batch(args, rank, world, local, dist):
         torch.cuda.synchronize()
         fp32_ms += e0.elapsed_time(e1)
         updates += int(cnt.item())
-        hu.append(v32)
+        v32s.append(v32)
         c32.close()
 
     with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             batch.run(raws, vols)
         stream.synchronize()
         batch.check_device_status()
-        # mixed batch vs FP32 per scan, HU inside the full-coverage mask
-        hu_rms = []
-        for v, v32 in zip(vols, hu):
+        hu_rms_fp32 = []
+        for v, v32 in zip(vols, v32s):
             a, b = v.cpu().numpy(), v32.cpu().numpy()
             m = np.isfinite(a) & np.isfinite(b)
-            hu_rms.append(float(np.sqrt(np.mean(((a[m] - b[m]) * 1000.0 / scans.MU_WATER) ** 2))) if m.any() else None)
-        del hu
+            hu_rms_fp32.append(float(np.sqrt(np.mean(((a[m] - b[m]) * 1000.0 / scans.MU_WATER) ** 2)))
+                               if m.any() else None)
+        del v32s
         clocks = ClockSampler(local)
         clocks.start()
         time.sleep(0.3)
@@ -443,12 +489,12 @@ def run_batch(args, rank, world, local, dist):
         torch.cuda.synchronize()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             batch.run(raws, vols)
         t1.record(stream)
         stream.synchronize()
         clk = clocks.stop()
-    ms = t0.elapsed_time(t1) / args.steps
+    ms = t0.elapsed_time(t1) / steps
     tm = torch.tensor([ms], dtype=torch.float64, device=dev)
     ua = torch.tensor([float(updates)], dtype=torch.float64, device=dev)
     if dist:
@@ -465,46 +511,71 @@ def run_batch(args, rank, world, local, dist):
             a.copy_(b.cpu())
         h2d = sum(r.numel() * 4 for r in raws)
         d2h = sum(v.numel() * 4 for v in vols)
-
-        def e2e_step():
-            # wfbp_batch_run_host: the copies overlap the two backprojection launches
-            batch.run_host(hr, hv, stream=stream)
-
         with torch.cuda.stream(stream):
-            e2e_step()
+            batch.run_host(hr, hv, stream=stream)  # wfbp_batch_run_host: copies overlap the two launches
             stream.synchronize()
             if dist:
                 dist.barrier()
             a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a0.record(stream)
-            for _ in range(args.steps):
-                e2e_step()
+            for _ in range(steps):
+                batch.run_host(hr, hv, stream=stream)
             a1.record(stream)
             stream.synchronize()
-        ems = a0.elapsed_time(a1) / args.steps
+        ems = a0.elapsed_time(a1) / steps
         te = torch.tensor([ems], dtype=torch.float64, device=dev)
         if dist:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         ems = float(te.item())
         e2e = {"value": float(ua.item()) / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        del hr, hv
+
+    # the checker: each scan's mixed volume against the FP64 oracle on its middle slab
+    hu64 = []
+    if rank == 0 and world == 1 and hu_scans and not args.no_hu:
+        for sp, r, v, (cg, tube, table) in list(zip(specs, raws, vols, views))[:hu_scans]:
+            try:
+                h = hu_vs_fp64(sp, cg, sp.recon_config(), tube, table, r, v)
+                hu64.append({"scan": sp.name, "rms": h["rms"], "max": h["max"], "voxels": h["voxels"]})
+            except Exception as ex:  # reported, not fatal
+                hu64.append({"scan": sp.name, "error": repr(ex)})
     n_scans, n_items = batch.size()
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    out = {"value": value, "ms": ms, "updates": updates, "fp32_per_scan_launches_ms": fp32_ms,
+           "speedup_vs_fp32_per_scan": fp32_ms / ms, "hu_rms_mixed_vs_fp32_per_scan": hu_rms_fp32,
+           "hu_vs_fp64_per_scan": hu64,
+           "hu_vs_fp64_rms_max": max((h["rms"] for h in hu64 if "rms" in h), default=None),
+           "scans": n_scans, "work_items": n_items,
+           "shapes": ["%dx%dx%d/%d->%dx%dx%d" % (sp.nch, sp.nr, sp.P, sp.V, sp.nx, sp.ny, sp.n_slices)
+                      for sp in specs],
+           "bp_config": autotune.config_name(batch.bp_config().key()),
+           "bp_tuning_ms": tuned["times_ms"] if tuned else None,
+           "raw_gb": sum(r.numel() for r in raws) * 4 / 1e9,
+           "gpu_launches": (3 * n_scans + 1) * steps, "e2e": e2e, "clocks": clk}
+    batch.close()
+    for c in ctxs:
+        c.close()
+    return out
+
+
+def run_batch(args, rank, world, local, dist):
+    """--workload batch24: the batch as the bench's headline line."""
+    b = measure_batch(args, rank, world, local, dist)
+    line = {"metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": b["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f16-storage/f32-accumulate",
             "data": "synthetic (24 seeded uneven helical scans, ellipsoid phantoms, Poisson noise)",
-            "config": {"workload": "batch24", "scans": n_scans, "work_items": n_items,
-                       "shapes": ["%dx%dx%d/%d->%dx%dx%d" % (sp.nch, sp.nr, sp.P, sp.V, sp.nx, sp.ny, sp.n_slices)
-                                  for sp in specs],
+            "config": {"workload": "batch24", "scans": b["scans"], "work_items": b["work_items"],
+                       "shapes": b["shapes"],
                        "precision": "mixed, one persistent backprojection launch, CUDA graph replay",
                        "parallelism": "independent batch per GPU",
-                       "l2": "inputs larger than L2 (%.1f GB raw frames)" % (sum(r.numel() for r in raws) * 4 / 1e9),
-                       "bp_config": autotune.config_name(batch.bp_config().key()),
-                       "bp_tuning_ms": tuned["times_ms"] if tuned else None},
-            "updates_per_step": updates, "fp32_per_scan_launches_ms": fp32_ms,
-            "speedup_vs_fp32_per_scan": fp32_ms / ms, "hu_rms_mixed_vs_fp32_per_scan": hu_rms,
-            "gpu_launches": (3 * n_scans + 1) * args.steps, "e2e": e2e, "clocks": clk}
-    batch.close()
+                       "l2": "inputs larger than L2 (%.1f GB raw frames)" % b["raw_gb"],
+                       "bp_config": b["bp_config"], "bp_tuning_ms": b["bp_tuning_ms"]},
+            "updates_per_step": b["updates"], "fp32_per_scan_launches_ms": b["fp32_per_scan_launches_ms"],
+            "speedup_vs_fp32_per_scan": b["speedup_vs_fp32_per_scan"],
+            "hu_rms_mixed_vs_fp32_per_scan": b["hu_rms_mixed_vs_fp32_per_scan"],
+            "hu_vs_fp64_per_scan": b["hu_vs_fp64_per_scan"],
+            "gpu_launches": b["gpu_launches"], "e2e": b["e2e"], "clocks": b["clocks"]}
     if rank == 0:
         print(json.dumps(line))
 
@@ -560,16 +631,26 @@ def main():
                              % (head["dims"].raw_bytes / 1e9, head["dims"].filtered_bytes / 1e9),
                        "bp_config": head["bp_config"], "bp_tuning_ms": head["tuning"]},
             "s_per_volume": head["ms"] / 1000.0, "updates_per_volume": head["updates"],
-            "stage_ms": head["stage"], "roofline": head["roofline"], "issue_roofline": head["issue"],
+            "stage_ms": head["stage"], "roofline": head["roofline"], "stage_rooflines": head["stages"],
             "gpu_launches": 4 * args.steps,
             "e2e": head["e2e"], "clocks": head["clocks"]}
     if len(forms) == 2:
         f32 = res["fp32"]
-        line["fp32"] = {k: f32[k] for k in ("value", "ms", "stage", "roofline", "issue", "e2e", "bp_config",
-                                            "clocks") if k in f32}
+        line["fp32"] = {k: f32[k] for k in ("value", "ms", "stage", "roofline", "stages", "e2e", "bp_config",
+                                            "clocks", "updates") if k in f32}
         line["mixed_speedup_vs_fp32"] = {"device": f32["ms"] / head["ms"],
                                          "e2e": (f32["e2e"]["ms_per_step"] / head["e2e"]["ms_per_step"])
                                          if head["e2e"] and f32["e2e"] else None}
+    if args.workload == "rows64" and not args.no_batch:
+        # the batched uneven scans (24 scans, one persistent launch): the batch
+        # autotuner tries the three fastest rows64 mixed shapes that fit
+        tms = head["tuning"] or {}
+        cands = sorted(tms, key=tms.get)[:3] if tms else None
+        try:
+            line["batch24"] = measure_batch(args, rank, world, local, dist, candidates=cands,
+                                            hu_scans=args.batch_hu_scans, steps=min(args.steps, 3), warmup=1)
+        except Exception as ex:  # reported, not fatal
+            line["batch24"] = {"error": repr(ex)}
     if rank == 0 and world == 1 and not args.no_cpu and not args.no_hu:
         # the checker, on the host cores: each form's volume against the FP64 oracle on one slab
         for f in forms:
@@ -583,15 +664,18 @@ def main():
                 line["fp32"]["hu_vs_fp64"] = hu
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cb = cpu_baseline(spec, lambda v0, v1: raw[v0:v1].cpu().numpy(), n_slices=args.cpu_slices)
+            from oracle import oracle as O
+            pos = baseline_positions(spec, O.configure_geometry(spec.meta(), table)[0], rp, n=args.cpu_slices)
+            cb = cpu_baseline(spec, lambda v0, v1: raw[v0:v1].cpu().numpy(), pos)
             full = head["updates"] / cb["t_full_est"]
             line["cpu_baseline"] = {
                 "value": full, "unit": UNIT, "cores": cb["cores"], "kind": "port",
-                "sample": "oracle FP32 transcript: rebin+filter of %d of %d views, backprojection of %d of %d native "
-                          "slices (%d updates) in %.1f s + %.1f s; scaled linearly to the full volume"
-                          % (cb["views"], spec.V, cb["slices"], head["dims"].n_slices_native, cb["updates_sample"],
-                             cb["t_rf_sample"], cb["t_bp_sample"]),
-                "s_per_volume_est": cb["t_full_est"]}
+                "sample": "oracle FP32 transcript (q8 texture weights): rebin+filter of the %d of %d views that %d "
+                          "native slices spread over one rotation's table feed need, backprojection of those %d "
+                          "of %d native slices (%d updates) in %.1f s + %.1f s; scaled linearly to the full volume"
+                          % (cb["views"], spec.V, cb["slices"], cb["slices"], head["dims"].n_slices_native,
+                             cb["updates_sample"], cb["t_rf_sample"], cb["t_bp_sample"]),
+                "s_per_volume_est": cb["t_full_est"], "positions": cb["positions"]}
         except Exception as ex:  # reported, not fatal
             line["cpu_baseline"] = {"error": repr(ex)}
     if rank == 0:
@@ -603,28 +687,74 @@ def main():
 
 def hu_vs_fp64(spec, cg, rp, tube, table, raw, vol):
     """HU error of `vol` against the FP64 oracle on the slab of the middle
-    requested slice: the oracle reconstructs that slab from its own window of
-    readings with the whole scan's slice positions and index angles (the
-    construction of freect_b200.shard), which equals the whole-scan FP64
-    result there. Returns rms, max, voxels."""
-    import numpy as np
-    from freect_b200 import shard
-    from oracle import oracle as O
-    O.set_threads(os.cpu_count() or 1)
-    ce = O.ffs_effective(cg) if (cg.ffs_phi or cg.ffs_z) else cg
-    nat, req = O.slice_locations(ce, rp)
-    plans = shard.plan(cg, rp, table, req.size)
-    p = plans[req.size // 2]
-    a0, a1 = p.readings
-    t0 = time.perf_counter()
-    ref = O.reconstruct_window_f64(shard.sub_geometry(cg, p), rp, spec.window, tube[a0:a1], table[a0:a1],
-                                   raw[a0:a1].cpu().numpy(), a0, nat[p.native[0]:p.native[1]],
-                                   req[p.requested[0]:p.requested[1]])
-    got = vol[p.requested[0]:p.requested[1]].cpu().numpy()
-    rms, mx, n = O.hu_error(got, ref)
-    return {"rms": rms, "max": mx, "voxels": n, "requested_slices": list(p.requested),
-            "oracle_seconds": time.perf_counter() - t0,
-            "note": "FP64 oracle on the slab of the middle requested slice, full-coverage voxels"}
+    requested slice (oracle/slab_check.py). Returns rms, max, voxels."""
+    from oracle.slab_check import hu_vs_fp64_slab
+    return hu_vs_fp64_slab(spec, cg, rp, tube, table, lambda a0, a1: raw[a0:a1].cpu().numpy(),
+                           lambda r0, r1: vol[r0:r1].cpu().numpy())
+
+
+def stage_rooflines(form, ctx, d, updates, stage, clk):
+    """Per-stage roofline fractions of one step, from the library's stage
+    events of the timed steps (ms per stage), the measured peaks and the
+    SM clock sampled during the timed region.
+
+    backproject: instruction issue (the binding limit; ncu: 71-76 % issue
+    active, no memory pipe near its peak): warp instructions per update from
+    the ncu capture of the same kernel x updates / time, against one warp
+    instruction per scheduler per clock. DRAM traffic per launch (the same
+    capture, scaled by updates) is reported against the compulsory bytes
+    (filtered rows read once, native volume written once).
+    rebin: HBM, raw frames read once + rebinned output written once.
+    filter: tensor pipe (mixed: 3 split-BF16 products of 2 (V nr) nch^2
+    FLOP each, against the sustained cuBLAS BF16 rate) or FP32 FFMA (FP32
+    form: 2 (V nr) nch^2 FLOP against 148 SMs x 128 lanes x 2 x clock)."""
+    hbm, bf16, bf16_sus, peak_src = load_peaks()
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    slab = ctx.bp_config().slab
+    t_bp = stage["backproject"] / 1000.0
+    wipu = WARP_INST_PER_UPDATE.get((form, slab))
+    ipeak = SMS * SCHEDULERS_PER_SM * mhz * 1e6
+    dram_per_update = DRAM_BYTES_PER_UPDATE.get((form, slab))
+    traffic = dram_per_update * updates if dram_per_update else None
+    compulsory = d.filtered_bytes + d.native_volume_bytes
+    bp = {"bound": "issue", "kernel": "backproject", "achieved": wipu * updates / t_bp if wipu else None,
+          "peak": ipeak, "unit": "warp instructions/s",
+          "frac": (wipu * updates / t_bp / ipeak) if wipu else None,
+          "traffic": traffic, "compulsory_bytes": compulsory,
+          "traffic_over_compulsory": traffic / compulsory if traffic else None,
+          "dram_gbs": traffic / t_bp / 1e9 if traffic else None,
+          "dram_frac_of_hbm": traffic / t_bp / 1e9 / hbm if traffic else None,
+          "updates_per_s": updates / t_bp,
+          "warp_inst_per_update": wipu,
+          "note": "warp instructions per update and DRAM bytes per update from the ncu capture of the same "
+                  "kernel and slab height on rows64_short (profiles/), scaled by this launch's updates; peak = "
+                  "%d SMs x %d schedulers x %.0f MHz (sampled); taps are shared-memory reads after one TMA "
+                  "staging per view window" % (SMS, SCHEDULERS_PER_SM, mhz)}
+    samples = d.n_views * d.n_rows * d.n_channels
+    rebin_bytes = d.raw_bytes + samples * 4  # FP32 rows, or the two BF16 operand planes
+    t_rb = stage["rebin"] / 1000.0
+    rebin = {"bound": "hbm", "kernel": "rebin", "achieved": rebin_bytes / t_rb / 1e9, "peak": hbm, "unit": "GB/s",
+             "frac": rebin_bytes / t_rb / 1e9 / hbm, "algorithmic_bytes": rebin_bytes,
+             "note": "raw frames read once + %d output samples x 4 B written" % samples}
+    rows = d.n_views * d.n_rows
+    t_f = stage["filter"] / 1000.0
+    if form == "mixed":
+        flop = 3 * 2.0 * rows * d.n_channels * d.n_channels
+        filt = {"bound": "tensor", "kernel": "toeplitz_tc", "achieved": flop / t_f / 1e12, "peak": bf16_sus,
+                "unit": "TFLOP/s", "frac": flop / t_f / 1e12 / bf16_sus, "algorithmic_flop": flop,
+                "note": "3 split-BF16 products (hi*hi, hi*lo, lo*hi) of 2 M K N, M = views x rows, K = N = "
+                        "channels, against the sustained cuBLAS BF16 rate"}
+    else:
+        flop = 2.0 * rows * d.n_channels * d.n_channels
+        fpk = SMS * 128 * 2 * mhz * 1e6 / 1e12
+        filt = {"bound": "fp32", "kernel": "toeplitz_f32", "achieved": flop / t_f / 1e12, "peak": fpk,
+                "unit": "TFLOP/s", "frac": flop / t_f / 1e12 / fpk, "algorithmic_flop": flop,
+                "note": "FP32 FFMA Toeplitz, peak = 148 SMs x 128 lanes x 2 FLOP x sampled clock"}
+    for r in (bp, rebin, filt):
+        r["peak_source"] = peak_src if r is not filt or form == "mixed" else "nominal"
+        r["ms"] = {"backproject": stage["backproject"], "rebin": stage["rebin"], "toeplitz_tc": stage["filter"],
+                   "toeplitz_f32": stage["filter"]}[r["kernel"]]
+    return bp, {"backproject": bp, "rebin": rebin, "filter": filt}
 
 
 def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, local):
@@ -720,32 +850,9 @@ def measure_form(args, form, spec, cg, rp, tube, table, raw, dev, stream, dist, 
         e2e = {"value": float(u_all.item()) / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
                "h2d_bytes_per_step": int(d.raw_bytes), "d2h_bytes_per_step": int(d.volume_bytes)}
 
-    hbm, bf16, peak_src = load_peaks()
-    elem = 4 if prec == T.PRECISION_FP32 else 2
-    achieved = updates * 4 * elem / (stage["backproject"] / 1000.0) / 1e9
-    # DRAM bytes per contributing update of the backprojection from the ncu capture of the
-    # same kernel on the rows64 scanner's short scan, scaled to this launch by its updates
-    dram_per_update = DRAM_BYTES_PER_UPDATE[(form, ctx.bp_config().slab)]
-    roofline = {"bound": "hbm", "kernel": "backproject", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": dram_per_update * updates,
-                "traffic_note": "dram read+write bytes per launch: %.4f B/update from the rows64_short ncu capture "
-                                "x %d updates" % (dram_per_update, updates),
-                "peak_source": peak_src,
-                "algorithmic_bytes_per_update": 4 * elem,
-                "note": "4 bilinear taps per contributing update, read from shared memory after one TMA "
-                        "staging per view window; the kernel is issue-bound (ncu summaries under profiles/)"}
-    # issue roofline: warp instructions per second the launch needs at this rate, against one
-    # instruction per scheduler per clock at the SM clock sampled during the timed steps
-    mhz = (clk or {}).get("sm_mhz") or 1965.0
-    wipu = WARP_INST_PER_UPDATE[(form, ctx.bp_config().slab)]
-    ips = wipu * updates / (stage["backproject"] / 1000.0)
-    ipeak = SMS * SCHEDULERS_PER_SM * mhz * 1e6
-    issue = {"kernel": "backproject", "warp_inst_per_update": wipu, "achieved": ips, "peak": ipeak,
-             "unit": "warp instructions/s", "frac": ips / ipeak,
-             "note": "instructions per update from the rows64_short ncu capture of the same slab height; "
-                     "peak = %d SMs x %d schedulers x %.0f MHz" % (SMS, SCHEDULERS_PER_SM, mhz)}
+    roofline, stages = stage_rooflines(form, ctx, d, updates, stage, clk)
     out = {"value": value, "ms": ms, "stage": stage, "updates": updates, "e2e": e2e, "clocks": clk,
-           "roofline": roofline, "issue": issue, "dims": d, "tuning": tuned["times_ms"] if tuned else None,
+           "roofline": roofline, "stages": stages, "dims": d, "tuning": tuned["times_ms"] if tuned else None,
            "bp_config": autotune.config_name(ctx.bp_config().key()),
            "dtype": "f32" if prec == T.PRECISION_FP32 else "f16-storage/f32-accumulate"}
     out["volume"] = vol

@@ -181,6 +181,10 @@ PRECISION_MIXED = 1
 FILTER_REFERENCE = 0
 FILTER_SHEPP_LOGAN = 1
 FILTER_USER = 2
+RECON_KERNEL_RAMLAK = 0
+RECON_KERNEL_SHEPP_LOGAN = 1
+RECON_KERNEL_HANN = 2
+RECON_KERNEL_HAMMING = 3
 FFS_NONE, FFS_PHI, FFS_Z, FFS_PHIZ = 0, 1, 2, 3
 LAYOUT_REFERENCE = 0
 LAYOUT_BACKPROJECTION = 1

@@ -109,13 +109,14 @@ def batch_signature(batch):
     return "||".join(parts)
 
 
-def tune_batch(batch, raws, volumes, reps=1, use_cache=True, path=None):
+def tune_batch(batch, raws, volumes, reps=1, use_cache=True, path=None, candidates=None):
     """Times the whole batch (graph replay) with each backprojection
-    configuration that fits every scan and keeps the fastest."""
+    configuration that fits every scan (or, given `candidates`, each of those
+    configuration names that fits) and keeps the fastest."""
     import torch
 
     path = path or cache_path()
-    key = batch_signature(batch)
+    key = batch_signature(batch) + ("|cand:" + ",".join(sorted(candidates)) if candidates else "")
     if use_cache:
         hit = _load(path).get(key)
         if hit:
@@ -124,7 +125,11 @@ def tune_batch(batch, raws, volumes, reps=1, use_cache=True, path=None):
     times, keys = {}, {}
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
-        for cfg in batch.bp_configs():
+        cfgs = batch.bp_configs()
+        if candidates:
+            picked = [c for c in cfgs if config_name(c.key()) in candidates]
+            cfgs = picked or cfgs
+        for cfg in cfgs:
             batch.set_bp_config(cfg)
             batch.run(raws, volumes)  # capture + first replay
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -541,6 +541,18 @@ int setup_slices(wfbp_ctx* ctx) {
 }
 }  // namespace
 
+WFBP_API int wfbp_recon_kernel_filter(int recon_kernel, int* window, float* c, float* a) {
+  if (!window || !c || !a) return WFBP_ERR_INVALID_ARG;
+  // ramp.m: a = 1 ramp, 0.5 Hann, 0.54 Hamming; c = 1 (no cut-off)
+  switch (recon_kernel) {
+    case WFBP_RECON_KERNEL_RAMLAK: *window = WFBP_FILTER_REFERENCE; *c = 1.0f; *a = 1.0f; return WFBP_OK;
+    case WFBP_RECON_KERNEL_SHEPP_LOGAN: *window = WFBP_FILTER_SHEPP_LOGAN; *c = 1.0f; *a = 1.0f; return WFBP_OK;
+    case WFBP_RECON_KERNEL_HANN: *window = WFBP_FILTER_REFERENCE; *c = 1.0f; *a = 0.5f; return WFBP_OK;
+    case WFBP_RECON_KERNEL_HAMMING: *window = WFBP_FILTER_REFERENCE; *c = 1.0f; *a = 0.54f; return WFBP_OK;
+    default: return WFBP_ERR_INVALID_ARG;
+  }
+}
+
 WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const wfbp_ext* ext, int device,
                              wfbp_ctx** out) {
   if (!cg || !rp || !out) return WFBP_ERR_INVALID_ARG;
@@ -557,6 +569,14 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     e = *ext;
   }
   if (e.precision != WFBP_PRECISION_FP32 && e.precision != WFBP_PRECISION_MIXED) return WFBP_ERR_INVALID_ARG;
+  // ReconConfig.recon_kernel picks the filter when the extension leaves it at
+  // its default (fct_wfbp parses the field, parse_config.cpp:53, but
+  // generate_filter ignores it, ReconstructionMachine.cu:204)
+  if (e.filter_window == WFBP_FILTER_REFERENCE &&
+      ((e.filter_c == 1.0f && e.filter_a == 1.0f) || (e.filter_c == 0.0f && e.filter_a == 0.0f))) {
+    if (wfbp_recon_kernel_filter(rp->recon_kernel, &e.filter_window, &e.filter_c, &e.filter_a))
+      return WFBP_ERR_INVALID_ARG;
+  }
   if (e.bp_slab != 0 && e.bp_slab != 16 && e.bp_slab != 32) return WFBP_ERR_INVALID_ARG;
   if (e.adjoint_scale_table != 0 && e.adjoint_scale_table != -1) return WFBP_ERR_INVALID_ARG;
   if (e.filtered_layout != WFBP_LAYOUT_REFERENCE && e.filtered_layout != WFBP_LAYOUT_BACKPROJECTION)
@@ -1508,6 +1528,11 @@ bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, in
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
   return do_filter(ctx, rebinned, filtered, scales, layout, stream);
 }
+int backproject_stage(wfbp_ctx* ctx, const void* filtered, const float* scales, float* vol, int layout,
+                      void* stream) {
+  return do_backproject(ctx, filtered, scales, vol, nullptr, layout, stream);
+}
+int run_layout_of(const wfbp_ctx* ctx) { return run_layout(ctx); }
 int n_bp_candidates() { return (int)(sizeof(kBpCandidates) / sizeof(kBpCandidates[0])); }
 void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw, int* slab) {
   *tx = kBpCandidates[i][0];

@@ -284,6 +284,9 @@ BPParams backprojection_params(const wfbp_ctx* ctx);
 void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal);
 bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, int slab, BPTile* out);
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream);
+int backproject_stage(wfbp_ctx* ctx, const void* filtered, const float* scales, float* vol, int layout,
+                      void* stream);
+int run_layout_of(const wfbp_ctx* ctx);  // the layout wfbp_run uses
 int n_bp_candidates();
 void bp_candidate(int i, int* tx, int* ty, int* cu, int* nw, int* slab);
 }  // namespace wfbp_detail

@@ -10,10 +10,18 @@
 // one file-scope device array of fixed size (WFBP_STATIC_SCRATCH_BYTES), which
 // every GPU that loads this library holds until the process exits.
 //
+// It runs the stages of wfbp_run in wfbp_run's own layout (the backprojection
+// layout and the TMA-staged backprojection whenever a launch fits), with the
+// thickening as a separate pass instead of fused into the backprojection's
+// write-back (the fused form would need the context's slab lists, which are
+// allocated on first use); the two forms give the same volume bit for bit.
+//
 // The array's name is only a host-side stand-in for the device symbol, so the
-// host code below never passes it to a kernel: once per device, with that
-// device current, it asks the runtime for the array's device address
-// (cudaGetSymbolAddress) and hands that address to the stage launches.
+// host code below never passes it to a kernel: with the device current, it
+// asks the runtime for the array's device address (cudaGetSymbolAddress) and
+// hands that address to the stage launches. The address is looked up once
+// per device and CUDA context: after the application resets the device
+// (cudaDeviceReset) the next call finds a new context and looks it up again.
 #include "wfbp_internal.h"
 
 #include <mutex>
@@ -26,12 +34,29 @@ static __device__ __align__(256) unsigned char g_static_scratch[WFBP_STATIC_SCRA
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;  // CUDA context the address belongs to (0: none yet)
+  void* addr = nullptr;
+};
+ScratchAddr g_scratch[kMaxDevices];
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
-// Device address of g_static_scratch on `device` (looked up once per device,
-// with that device current). Returns nullptr on failure.
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (the
+// library does not link the driver library directly)
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+template <class F>
+F driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+    return reinterpret_cast<F>(p);
+  return nullptr;
+}
+
+// Device address of g_static_scratch on `device`, which is current. Looked up
+// once per device and context; returns nullptr on failure.
 void* scratch_address(int device, cudaError_t* err) {
   *err = cudaSuccess;
   if (device < 0 || device >= kMaxDevices) {
@@ -39,16 +64,46 @@ void* scratch_address(int device, cudaError_t* err) {
     return nullptr;
   }
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  static const CtxGetCurrentFn get_current = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static const CtxGetIdFn get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+  if (!get_current || !get_id) {
+    *err = cudaErrorNotSupported;
+    return nullptr;
+  }
+  ScratchAddr& s = g_scratch[device];
+  // the context current on this thread (cudaSetDevice binds the device's
+  // primary context); none yet: the symbol lookup binds it
+  CUcontext cu = nullptr;
+  unsigned long long id = 0;
+  void* p = nullptr;
+  if (get_current(&cu) != CUDA_SUCCESS || !cu) {
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess) {
       *err = e;
       return nullptr;
     }
-    g_scratch_addr[device] = p;
+    cu = nullptr;
+    if (get_current(&cu) != CUDA_SUCCESS || !cu) {
+      *err = cudaErrorDeviceUninitialized;
+      return nullptr;
+    }
   }
-  return g_scratch_addr[device];
+  if (get_id(cu, &id) != CUDA_SUCCESS) {
+    *err = cudaErrorDeviceUninitialized;
+    return nullptr;
+  }
+  if (s.ctx_id != id || !s.addr) {
+    if (!p) {
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+      if (e != cudaSuccess) {
+        *err = e;
+        return nullptr;
+      }
+    }
+    s.addr = p;
+    s.ctx_id = id;
+  }
+  return s.addr;
 }
 
 }  // namespace
@@ -63,14 +118,15 @@ WFBP_API int wfbp_run_static(wfbp_ctx* ctx, const float* raw, float* volume, voi
     ctx->err = "wfbp_run_static: wfbp_set_views not called";
     return WFBP_ERR_STATE;
   }
-  wfbp_dims d;
-  int st = wfbp_query(ctx, &d);
-  if (st) return st;
+  const int layout = wfbp_detail::run_layout_of(ctx);
+  size_t reb = 0, filt = 0, scal = 0;
+  wfbp_detail::buffer_bytes(ctx, layout, &reb, &filt, &scal);
+  const size_t nat = sizeof(float) * (size_t)ctx->nz * ctx->ny * ctx->nx;
   // layout: [rebinned][filtered][row scales][native volume], 256-byte aligned
-  const size_t off_filt = align256(d.rebinned_bytes);
-  const size_t off_scal = off_filt + align256(d.filtered_bytes);
-  const size_t off_nat = off_scal + align256(d.row_scale_bytes);
-  const size_t need = off_nat + align256(d.native_volume_bytes);
+  const size_t off_filt = align256(reb);
+  const size_t off_scal = off_filt + align256(filt);
+  const size_t off_nat = off_scal + align256(scal);
+  const size_t need = off_nat + align256(nat);
   if (need > (size_t)WFBP_STATIC_SCRATCH_BYTES) {
     ctx->err = "wfbp_run_static: this geometry needs " + std::to_string(need) +
                " bytes of intermediates, more than the static scratch of " +
@@ -91,11 +147,12 @@ WFBP_API int wfbp_run_static(wfbp_ctx* ctx, const float* raw, float* volume, voi
   // cleared between calls.
   void* rebinned = base;
   void* filtered = base + off_filt;
-  float* scales = d.row_scale_bytes ? reinterpret_cast<float*>(base + off_scal) : nullptr;
+  float* scales = scal ? reinterpret_cast<float*>(base + off_scal) : nullptr;
   float* native = reinterpret_cast<float*>(base + off_nat);
-  if (!(st = wfbp_rebin(ctx, raw, rebinned, stream)) && !(st = wfbp_filter(ctx, rebinned, filtered, scales, stream)) &&
-      !(st = wfbp_backproject(ctx, filtered, scales, native, nullptr, stream)))
-    st = wfbp_thicken(ctx, native, volume, stream);
+  int st = wfbp_rebin(ctx, raw, rebinned, stream);
+  if (!st) st = wfbp_detail::filter_stage(ctx, rebinned, filtered, scales, layout, stream);
+  if (!st) st = wfbp_detail::backproject_stage(ctx, filtered, scales, native, layout, stream);
+  if (!st) st = wfbp_thicken(ctx, native, volume, stream);
   if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
   return st;
 }

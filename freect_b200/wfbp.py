@@ -27,6 +27,8 @@ _PROTOS = {
                                        C.POINTER(C.c_int)]),
     "wfbp_filter_taps": (C.c_int, [C.POINTER(T.CTGeometry), C.c_int, C.c_float, C.c_float, C.POINTER(C.c_float),
                                    C.c_int]),
+    "wfbp_recon_kernel_filter": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                           C.POINTER(C.c_float)]),
     "wfbp_ctx_create": (C.c_int, [C.POINTER(T.CTGeometry), C.POINTER(T.ReconConfig), C.POINTER(T.Ext), C.c_int,
                                   C.POINTER(_VP)]),
     "wfbp_ctx_destroy": (C.c_int, [_VP]),
@@ -178,6 +180,14 @@ def filter_taps(cg, window=T.FILTER_REFERENCE, c=1.0, a=1.0, n=None):
     _check(load().wfbp_filter_taps(C.byref(cg), window, c, a, out.ctypes.data_as(C.POINTER(C.c_float)), n),
            "wfbp_filter_taps")
     return out
+
+
+def recon_kernel_filter(recon_kernel):
+    """(window, c, a) that ReconConfig.recon_kernel selects (wfbp_recon_kernel)."""
+    w, c, a = C.c_int(), C.c_float(), C.c_float()
+    _check(load().wfbp_recon_kernel_filter(recon_kernel, C.byref(w), C.byref(c), C.byref(a)),
+           "wfbp_recon_kernel_filter")
+    return w.value, c.value, a.value
 
 
 def make_ext(precision=T.PRECISION_FP32, filter_window=T.FILTER_REFERENCE, filter_c=1.0, filter_a=1.0,

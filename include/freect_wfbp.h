@@ -151,6 +151,20 @@ enum wfbp_filter_window {
   WFBP_FILTER_USER = 2        /* caller-provided symmetric taps h[0..n-1] */
 };
 
+/* Values of ReconConfig.recon_kernel. fct_wfbp parses the field
+ * (parse_config.cpp:53) but always filters with generate_filter's ramp
+ * (ReconstructionMachine.cu:204); here it selects the window whenever the
+ * wfbp_ext is NULL or leaves filter_window at WFBP_FILTER_REFERENCE with
+ * filter_c = filter_a = 1 (or both 0). 0 reproduces fct_wfbp; other values
+ * are rejected (WFBP_ERR_INVALID_ARG). The Hann and Hamming windows are
+ * generate_filter's `a` parameter (resources/ramp.m: 0.5, 0.54). */
+enum wfbp_recon_kernel {
+  WFBP_RECON_KERNEL_RAMLAK = 0,      /* generate_filter(c = 1, a = 1) */
+  WFBP_RECON_KERNEL_SHEPP_LOGAN = 1, /* WFBP_FILTER_SHEPP_LOGAN */
+  WFBP_RECON_KERNEL_HANN = 2,        /* generate_filter(c = 1, a = 0.5) */
+  WFBP_RECON_KERNEL_HAMMING = 3      /* generate_filter(c = 1, a = 0.54) */
+};
+
 /* Layout of the filtered projections at the wfbp_filter / wfbp_backproject
  * boundary. REFERENCE keeps the reference's [view][row][channel] FP32 (or
  * FP16 + per-row scales); BACKPROJECTION is the channel-major layout the
@@ -237,6 +251,10 @@ int wfbp_slice_locations(const CTGeometry* cg, const ReconConfig* rp,
                          float* native_z, int native_cap, int* n_native,
                          float* requested_z, int requested_cap, int* n_requested);
 
+/* The filter window, c and a that a ReconConfig.recon_kernel value selects
+ * (wfbp_recon_kernel; host only). WFBP_ERR_INVALID_ARG for other values. */
+int wfbp_recon_kernel_filter(int recon_kernel, int* window, float* c, float* a);
+
 /* Filter taps: the spatial-domain kernel of generate_filter
  * (ReconstructionMachine.cu:478-513) before its FFT, as the symmetric half
  * h[0..n-1] (h[-k] = h[k]) in FP32. */
@@ -249,7 +267,8 @@ int wfbp_filter_taps(const CTGeometry* cg, int window, float c, float a, float* 
 /* Creates a context on `device` for one scan geometry and recon config.
  * Replaces the state the reference keeps in ReconstructionMachine
  * (ReconstructionMachine.h:30-48) plus its __constant__ copies
- * (cuda_kernels.cuh:5-7). `ext` may be NULL (FP32, reference filter). */
+ * (cuda_kernels.cuh:5-7). `ext` may be NULL (FP32; the filter of rp->recon_kernel,
+ * wfbp_recon_kernel). */
 int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const wfbp_ext* ext,
                     int device, wfbp_ctx** out);
 int wfbp_ctx_destroy(wfbp_ctx* ctx);

@@ -11,10 +11,18 @@ and stores inputs and outputs as .npz files:
   tex_probe.npz    hardware bilinear texture samples at random coordinates
   tex_ramp.npz     samples of ramp textures on a fine grid of coordinates:
                    the texture unit's effective fractional weights
+  full_ref_small.npz  the small scanner at its full size (672 ch x 16 rows x
+                   3480 readings -> 256^2 x 16 slices, Ram-Lak): the seed, the
+                   SHA-256 of the synthesised raw frames (150 MB, regenerated
+                   from the seed by the test instead of being stored) and the
+                   reference's final volume
 
-Usage (needs a GPU): python tests/golden/make_reference_fixtures.py [outdir]
+Usage (needs a GPU):
+  python tests/golden/make_reference_fixtures.py [outdir]               small cases
+  python tests/golden/make_reference_fixtures.py --small-full [outdir]  full-size small scanner
 """
 import ctypes as C
+import hashlib
 import os
 import sys
 
@@ -110,6 +118,24 @@ def tex_ramp_probe(lib, w=16, h=16, steps=4096):
     return dict(coord=xs, out_x=ox, out_y=oy)
 
 
+SMALL_FULL_SEED = 3
+
+
+def raw_digest(raw):
+    """SHA-256 of the raw frames' bytes (float32, C order)."""
+    return hashlib.sha256(np.ascontiguousarray(raw, np.float32).tobytes()).hexdigest()
+
+
+def small_full(outdir):
+    spec = scans.small(seed=SMALL_FULL_SEED)
+    raw = O.synth_project(spec.synth(), spec.ellipsoids())
+    res = run_reference(load_shim(), spec, raw)
+    np.savez_compressed(os.path.join(outdir, "full_ref_small.npz"), seed=np.int64(SMALL_FULL_SEED),
+                        raw_sha256=np.array(raw_digest(raw)), volume=res["volume"], z_native=res["z_native"],
+                        z_req=res["z_req"])
+    print("small_full", spec.V, spec.nr, spec.nch, res["volume"].shape, raw_digest(raw))
+
+
 def main(outdir):
     os.makedirs(outdir, exist_ok=True)
     lib = load_shim()
@@ -124,4 +150,9 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    out = args[0] if args else os.path.dirname(os.path.abspath(__file__))
+    if "--small-full" in sys.argv:
+        small_full(out)
+    else:
+        main(out)

@@ -1,14 +1,17 @@
 """Writes tests/golden/struct_layout.json: sizeof/offsetof of the reference's
 CTGeometry, ReconConfig and GPUPrecompute, compiled with g++ from the
 reference's own applications/fct_wfbp/include/recon_structs.h.
-Run in a container that has the reference tree (REF below)."""
+Run where the reference tree is present: its root is taken from the
+FREECT_REFERENCE_ROOT environment variable (default /root/reference) or the
+first command-line argument."""
 import json
 import os
 import subprocess
 import sys
 import tempfile
 
-REF = "/root/reference/applications/fct_wfbp/include"
+REF = os.path.join(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FREECT_REFERENCE_ROOT", "/root/reference"),
+                   "applications", "fct_wfbp", "include")
 FIELDS = {
     "CTGeometry": ["total_number_of_projections", "projections_per_rotation", "detector_pixel_size_col",
                    "detector_pixel_size_row", "num_detector_cols", "num_detector_cols_padded",

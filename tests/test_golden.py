@@ -97,3 +97,22 @@ def test_oracle_transcript_matches_reference_kernels(orc, path):
     r64 = orc.reconstruct_f64(spec, raw)
     rms64, mx64, _ = orc.hu_error(r64["volume"], d["volume"])
     assert rms64 < 0.5, (rms64, mx64)
+
+
+def test_oracle_transcript_matches_reference_kernels_full_size(orc):
+    # the small scanner at its full size (672 ch x 16 rows x 3480 readings ->
+    # 256^2 x 16 slices, Ram-Lak): the reference's own kernels ran on a B200
+    # (full_ref_small.npz: seed, SHA-256 of the raw frames, final volume); the
+    # oracle's FP32 transcript reproduces that volume from the regenerated frames
+    import hashlib
+    from freect_b200 import scans
+    d = np.load(os.path.join(GOLD, "full_ref_small.npz"))
+    spec = scans.small(seed=int(d["seed"]))
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    assert hashlib.sha256(np.ascontiguousarray(raw).tobytes()).hexdigest() == str(d["raw_sha256"])
+    ref = orc.reconstruct_ref32(spec, raw, q8=True)
+    assert np.array_equal(ref["z_req"], d["z_req"]) and np.array_equal(ref["z_native"], d["z_native"])
+    rms, mx, n = orc.hu_error(ref["volume"], d["volume"])
+    assert np.array_equal(np.isnan(ref["volume"]), np.isnan(d["volume"]))
+    assert n == np.isfinite(d["volume"]).sum() and n > 0.9 * d["volume"].size
+    assert rms < 0.25 and mx < 1.0, (rms, mx)

@@ -434,3 +434,38 @@ def test_descending_slices_and_origin_offset(orc, precision):
     rms, mx, n = orc.hu_error(got, ref)
     assert n == np.isfinite(ref).sum() and n > 0
     assert rms <= (0.5 if precision == T.PRECISION_FP32 else 1.0), (rms, mx)
+
+
+@pytest.mark.parametrize("rk", [T.RECON_KERNEL_SHEPP_LOGAN, T.RECON_KERNEL_HANN, T.RECON_KERNEL_HAMMING])
+def test_recon_kernel_from_yaml(orc, tmp_path, rk):
+    # a recon YAML with recon_kernel set, read by wfbp_parse_recon_config; the
+    # context (no filter in the extension) filters with that window, checked
+    # against the reference transcript given the same window's taps
+    spec = scans.tiny(seed=21)
+    ref_rp = spec.recon_config()
+    p = tmp_path / "recon.yaml"
+    p.write_text("raw_data_dir: synthetic\noutput_dir: .\nstart_pos: %r\nend_pos: %r\nrecon_fov: %r\n"
+                 "slice_thickness: %r\nslice_pitch: %r\nnx: %d\nny: %d\nrecon_kernel: %d\n"
+                 % (ref_rp.start_pos, ref_rp.end_pos, ref_rp.recon_fov, ref_rp.slice_thickness, ref_rp.slice_pitch,
+                    ref_rp.nx, ref_rp.ny, rk))
+    rp = wfbp.parse_recon_config(str(p))
+    assert rp.recon_kernel == rk
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    ctx = wfbp.Context(cg, rp, wfbp.make_ext(tex_weights=1), device=0)
+    ctx.set_views(tube, table)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    w, c, a = wfbp.recon_kernel_filter(rk)
+    half = wfbp.filter_taps(cg, w, c, a)
+    ref = orc.reconstruct_ref32(spec, raw, taps_half=half, q8=True)
+    got = vol.cpu().numpy()
+    rms, mx, n = orc.hu_error(got, ref["volume"])
+    assert n == got.size
+    assert rms <= 0.5 and mx <= 2.0, (rms, mx)
+    # and it differs from the Ram-Lak reconstruction (the window took effect)
+    ramlak = orc.reconstruct_ref32(spec, raw, q8=True)
+    assert orc.hu_error(got, ramlak["volume"])[0] > 5.0 * max(rms, 0.01)
+    ctx.close()

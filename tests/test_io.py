@@ -56,3 +56,30 @@ def test_meta_requires_geometry_keys(tmp_path):
     (tmp_path / "meta.yaml").write_text("detector_rows: 4\ndetector_channels: 8\n")
     with pytest.raises(wfbp.WfbpError):
         wfbp.read_meta(str(tmp_path))
+
+
+@pytest.mark.parametrize("rk,window,c,a", [(T.RECON_KERNEL_RAMLAK, T.FILTER_REFERENCE, 1.0, 1.0),
+                                           (T.RECON_KERNEL_SHEPP_LOGAN, T.FILTER_SHEPP_LOGAN, 1.0, 1.0),
+                                           (T.RECON_KERNEL_HANN, T.FILTER_REFERENCE, 1.0, 0.5),
+                                           (T.RECON_KERNEL_HAMMING, T.FILTER_REFERENCE, 1.0, 0.54)])
+def test_recon_kernel_selects_filter(orc, tmp_path, rk, window, c, a):
+    # recon_kernel from a recon YAML (parse_config.cpp:53) -> filter window and
+    # generate_filter's (c, a) (resources/ramp.m); taps against the oracle's
+    p = tmp_path / "recon.yaml"
+    p.write_text("recon_fov: 250\nslice_thickness: 1\nnx: 32\nny: 32\nrecon_kernel: %d\n" % rk)
+    rp = wfbp.parse_recon_config(str(p))
+    w, cc, aa = wfbp.recon_kernel_filter(rp.recon_kernel)
+    assert (w, cc) == (window, c) and abs(aa - a) < 1e-7
+    spec = scans.small()
+    tube, table = spec.views()
+    cg, _ = wfbp.configure_geometry(spec.meta(), table)
+    got = wfbp.filter_taps(cg, w, cc, aa)
+    ref = orc.taps_f64(cg, w, cc, aa)
+    # generate_filter in FP32 (ReconstructionMachine.cu:478-513) against the FP64 formula
+    assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+def test_recon_kernel_rejects_unknown_values():
+    for rk in (-1, 4, 100):
+        with pytest.raises(wfbp.WfbpError):
+            wfbp.recon_kernel_filter(rk)

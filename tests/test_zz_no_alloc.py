@@ -4,12 +4,11 @@ Some callers cannot let the library call cudaMalloc -- their device memory
 belongs to their own pool, or they run inside a fixed memory budget, or they
 cannot afford cudaMalloc's synchronisation in their loop. wfbp_run_static
 keeps the intermediates in a static device array instead. These tests call it
-through the C ABI and check it against the same four stages run on
-context-allocated buffers (the context's own layout, as wfbp_run_static
-uses), twice in a row (the array keeps the previous call's contents), and
-that oversized geometries are
-rejected. This file is collected last so that a failure here does not stop a
-run before the other tests.
+through the C ABI and check it against wfbp_run on the same context, bit for
+bit, twice in a row (the array keeps the previous call's contents); that the
+device's free memory does not change across its calls (nothing is allocated);
+and that oversized geometries are rejected. This file is collected last so
+that a failure here does not stop a run before the other tests.
 """
 import ctypes as C
 
@@ -36,35 +35,46 @@ def _ctx(spec, precision):
     return ctx
 
 
+def _static(lib, ctx, raw, vol):
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return lib.wfbp_run_static(ctx.handle, C.c_void_p(raw.data_ptr()), C.c_void_p(vol.data_ptr()), stream)
+
+
 @pytest.mark.parametrize("precision", [T.PRECISION_FP32, T.PRECISION_MIXED])
 def test_run_static_matches_run_twice(orc, precision):
     lib = wfbp.load()
     dev = torch.device("cuda", 0)
-    for seed in (3, 4):  # two different scans, back to back
+    # the first call on a device loads the library's device code that holds the
+    # static array and looks up its address: done once, outside the check
+    warm = scans.tiny(seed=2)
+    wctx = _ctx(warm, precision)
+    wraw = torch.from_numpy(orc.synth_project(warm.synth(), warm.ellipsoids())).to(dev)
+    wvol = wctx.alloc("volume")
+    assert _static(lib, wctx, wraw, wvol) == 0, lib.wfbp_last_error(wctx.handle)
+    torch.cuda.synchronize()
+    wctx.close()
+    for seed in (3, 4):  # two different scans, back to back, each on a fresh context
         spec = scans.tiny(seed=seed)
         raw = torch.from_numpy(orc.synth_project(spec.synth(), spec.ellipsoids())).to(dev)
         ctx = _ctx(spec, precision)
-        ref = ctx.alloc("volume")
-        reb, filt, sc, vn = ctx.alloc("rebinned"), ctx.alloc("filtered"), ctx.alloc("row_scales"), ctx.alloc("native")
-        ctx.rebin(raw, reb)
-        ctx.filter(reb, filt, sc)
-        ctx.backproject(filt, vn, sc)
-        ctx.thicken(vn, ref)
-        got = ctx.alloc("volume")
-        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-        st = lib.wfbp_run_static(ctx.handle, C.c_void_p(raw.data_ptr()), C.c_void_p(got.data_ptr()), stream)
+        got, got2 = ctx.alloc("volume"), ctx.alloc("volume")
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(dev)
+        st = _static(lib, ctx, raw, got)
+        assert st == 0, lib.wfbp_last_error(ctx.handle)
+        st = _static(lib, ctx, raw, got2)  # second call in a row on the same array
         assert st == 0, lib.wfbp_last_error(ctx.handle)
         torch.cuda.synchronize()
-        a, b = got.cpu().numpy(), ref.cpu().numpy()
-        rms, mx, n = orc.hu_error(a, b)
-        assert n == a.size
-        assert rms <= 1e-3 and mx <= 1e-2, (rms, mx)  # same kernels on the same layout
-        # second call in a row on the same array
-        got2 = ctx.alloc("volume")
-        st = lib.wfbp_run_static(ctx.handle, C.c_void_p(raw.data_ptr()), C.c_void_p(got2.data_ptr()), stream)
-        assert st == 0
+        free1, _ = torch.cuda.mem_get_info(dev)
+        assert free1 == free0, "wfbp_run_static changed the device's free memory by %d bytes" % (free0 - free1)
+        # the existing entry point (which allocates its own scratch) on the same context
+        ref = ctx.alloc("volume")
+        ctx.run(raw, ref)
         torch.cuda.synchronize()
-        assert np.array_equal(got2.cpu().numpy(), a)
+        a = got.cpu().numpy()
+        assert np.isfinite(a).any()
+        assert np.array_equal(a, ref.cpu().numpy(), equal_nan=True)
+        assert np.array_equal(got2.cpu().numpy(), a, equal_nan=True)
         ctx.close()
 
 
