@@ -32,6 +32,7 @@
 // in the error word and stops. Window or slot overflows (which the host's
 // sizing rules out) are recorded as well and the affected samples skipped.
 #include "wfbp_internal.h"
+#include "bp_math.cuh"
 #include "wait.cuh"
 
 #include <cuda.h>
@@ -77,7 +78,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 // packed FP32x2 instructions (FFMA2 / FADD2 / FMUL2).
 struct __align__(16) GeoP {
   float2 bq, cq;    // q(z) = bq z + cq
-  float2 qlo, qhi;  // valid for qlo <= q <= qhi
+  float2 qmid, qhw;  // valid for |q - qmid| <= qhw (the row range [qlo, qhi] as centre and half width)
   int2 addr;        // shared-memory byte offset of (channel pf, row 0) of the view's slot
   float2 wp;        // FP32 rows: channel weight; half2 pairs: bits of the half2 (wp, wp)
 };
@@ -334,9 +335,9 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
   }
 
   // ---------------- consumers ----------------
-  float vacc[CPG];
+  float2 vacc[CPG / 2];  // columns (2i, 2i + 1) of this lane's group
 #pragma unroll
-  for (int c = 0; c < CPG; c++) vacc[c] = 0.0f;
+  for (int c = 0; c < CPG / 2; c++) vacc[c] = make_float2(0.0f, 0.0f);
   unsigned long long cnt = 0;
   const float k1 = 2.5f / p.hn;
   GeoP* wgeo = geo + (size_t)warp * bt.nv_max * NPW;
@@ -369,15 +370,28 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
     // geometry of (column gc, view v) for v = gv, gv + VPP, ...
     for (int v = gv; v < nv; v += VPP) {
       const int2 vi = vinfo[s * bt.nv_max + v];
-      const float2 sc = __ldg(view_sc + vi.x);
-      const float zt = __ldg(view_z + vi.x);
-      const float p_hat = gx * sc.x - gy * sc.y;
-      const float l_hat = sqrtf(p.R2 - p_hat * p_hat) - gx * sc.y - gy * sc.x;
-      const float A = p.zr2pi * asinf(p.rR * p_hat);
-      const float inv = 1.0f / (l_hat * p.tanc);
+      float p_hat, t_hat, zt;
+      if constexpr (HALF) {
+        // the mixed form's per-view geometry is FP64 (sin, cos and table
+        // position of the view, from the FP64 tables of wfbp_set_views)
+        const double2 sc = __ldg(p.sc64 + vi.x);
+        const double gxd = (double)gx, gyd = (double)gy;
+        p_hat = (float)fma(gxd, sc.x, -gyd * sc.y);
+        t_hat = (float)fma(gxd, sc.y, gyd * sc.x);
+        zt = (float)__ldg(p.z64 + vi.x);
+      } else {
+        const float2 sc = __ldg(view_sc + vi.x);
+        p_hat = gx * sc.x - gy * sc.y;
+        t_hat = gx * sc.y + gy * sc.x;
+        zt = __ldg(view_z + vi.x);
+      }
+      const float l_hat = bp_sqrt(p.R2 - p_hat * p_hat) - t_hat;
+      const float A = p.zr2pi * bp_asin(p.rR * p_hat);
+      const float inv = bp_rcp(l_hat * p.tanc);
       const float p_idx = p.kp - (p_hat * p.ps + p.c0);
       const float pf = floorf(p_idx);
-      bool valid = gactive && pf >= 0.0f && ceilf(p_idx) <= p.ncm2;
+      // floor(p_idx) >= 0 and ceil(p_idx) <= nch - 2 (cuda_kernels.cuh:259-263)
+      bool valid = gactive && p_idx >= 0.0f && p_idx <= p.ncm2;
       const int cofs = (int)pf - vi.y;
       if (valid && (cofs < 0 || cofs > bt.W - 2)) {
         atomicOr(err, 0x200);  // channel window too narrow: host sizing violated
@@ -389,8 +403,10 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       float* gf = reinterpret_cast<float*>(wgeo + v * NPW + (gc >> 1)) + (gc & 1);
       gf[0] = bq;
       gf[2] = cq;
-      gf[4] = valid ? fmaxf(0.0f, fmaf(zt - p.z_rot, bq, cq)) : 3.0e38f;
-      gf[6] = valid ? fminf(p.nrm2, fmaf(zt + p.z_rot, bq, cq)) : -3.0e38f;
+      // rows q in [0, nr - 2] (cuda_kernels.cuh:259-263) of views within z_rot (:232)
+      const float qlo = fmaxf(0.0f, fmaf(zt - p.z_rot, bq, cq)), qhi = fminf(p.nrm2, fmaf(zt + p.z_rot, bq, cq));
+      gf[4] = valid ? 0.5f * (qlo + qhi) : 0.0f;
+      gf[6] = valid ? 0.5f * (qhi - qlo) : -1.0f;
       reinterpret_cast<int*>(gf)[8] =
           (int)(L.slots + (size_t)(s * bt.nv_max + v) * bt.slot_bytes) + (valid ? cofs : 0) * nrpb;
       if constexpr (HALF) {
@@ -401,7 +417,6 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       }
     }
     __syncwarp();
-    const unsigned my_cols = (active_mask >> (grp * CPG)) & ((1u << CPG) - 1u);  // this group's columns
 #pragma unroll
     for (int c0 = 0; c0 < CPG; c0 += CU) {
       unsigned any = 0u;  // warp-uniform: some group has an active column in this step
@@ -425,8 +440,9 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
         for (int u2 = 0; u2 < CU / 2; u2++) {
           const GeoP g = gpv[u2];
           const float2 q = __ffma2_rn(zl2, g.bq, g.cq);
-          const bool okx = (q.x >= g.qlo.x) && (q.x <= g.qhi.x);
-          const bool oky = (q.y >= g.qlo.y) && (q.y <= g.qhi.y);
+          const float2 dq = __fadd2_rn(q, neg2(g.qmid));
+          const bool okx = fabsf(dq.x) <= g.qhw.x;
+          const bool oky = fabsf(dq.y) <= g.qhw.y;
           // any in-range row for invalid lanes (their weight is 0); NaN -> 0
           const unsigned rx = min((unsigned)__float2int_rz(q.x), nrm2u);
           const unsigned ry = min((unsigned)__float2int_rz(q.y), nrm2u);
@@ -474,30 +490,35 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
           if (COUNT) cnt += (okx ? 1 : 0) + (oky ? 1 : 0);
         }
       }
+      // cuda_kernels.cuh:283, vol += (2 pi / P) (sum W g) / (sum W): the
+      // quotient through the hardware reciprocal (0 / 0 stays NaN), 2 pi / P
+      // applied once at the write-back
 #pragma unroll
-      for (int u2 = 0; u2 < CU / 2; u2++) {
-        const int c = c0 + 2 * u2;
-        // cuda_kernels.cuh:283
-        if ((my_cols >> c) & 1u) vacc[c] += p.dtheta * (1.0f / aw[u2].x) * ag[u2].x;
-        if ((my_cols >> (c + 1)) & 1u) vacc[c + 1] += p.dtheta * (1.0f / aw[u2].y) * ag[u2].y;
-      }
+      for (int u2 = 0; u2 < CU / 2; u2++)
+        vacc[c0 / 2 + u2] = __ffma2_rn(ag[u2], make_float2(bp_rcp(aw[u2].x), bp_rcp(aw[u2].y)), vacc[c0 / 2 + u2]);
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
 
-  // write the slab
+  // write the slab: columns outside the grid or the FOV keep the 0 the
+  // reference leaves there
+  const unsigned my_cols = (active_mask >> (grp * CPG)) & ((1u << CPG) - 1u);
+  float vals[CPG];
+#pragma unroll
+  for (int c = 0; c < CPG; c++)
+    vals[c] = ((my_cols >> c) & 1u) ? p.dtheta * ((c & 1) ? vacc[c / 2].y : vacc[c / 2].x) : 0.0f;
   if (my_s < p.nz) {
     const size_t plane = (size_t)p.nx * p.ny;
 #pragma unroll
     for (int c = 0; c < CPG; c++) {
       const int tt = warp * CPW + grp * CPG + c;
       const int ix = ix0 + tt % bt.tx, iy = iy0 + tt / bt.tx;
-      if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = vacc[c];
+      if (ix < p.nx && iy < p.ny) vol[(size_t)my_s * plane + (size_t)iy * p.nx + ix] = vals[c];
     }
   }
   if (FUSE && tf.out)
-    bp_fused_thicken<CPW, SL, CPG>(tf, vacc, reinterpret_cast<const int*>(smem + L.fuse),
+    bp_fused_thicken<CPW, SL, CPG>(tf, vals, reinterpret_cast<const int*>(smem + L.fuse),
                                    reinterpret_cast<volatile int*>(nvs)[10], warp, lane, ix0, iy0, bt, p);
   if (COUNT) {
 #pragma unroll

@@ -11,27 +11,35 @@
 // lo = bf16(v - hi)); Y = Xhi Thi + Xhi Tlo + Xlo Thi accumulated in FP32 in
 // tensor memory (the dropped Xlo Tlo term is ~2^-16 relative).
 //
-// Tiling: one CTA computes a 128 x BN tile of Y (BN <= 256, a multiple of 16).
-// Warp 0 lane 0 issues TMA loads (128B-swizzled, K-major) of the four operand
-// tiles of each 64-wide K block into a 2-stage ring; warp 1 lane 0 issues the
-// 3 x 4 UMMAs (M128 x N BN x K16) per K block and commits each stage back to
-// the producer; all four warps then read the FP32 accumulator out of tensor
-// memory (tcgen05.ld 32x32b, one row per thread) and store FP32 rows or FP16
-// rows scaled by a per-row power of two. Every mbarrier wait is bounded: on
-// timeout the CTA records an error code, stops issuing work, waits (bounded)
-// for its TMA copies and frees its tensor memory before returning.
+// Tiling: 128 x BN output tiles (BN <= 256, a multiple of 16), the N tiles of
+// one 128-row M tile consecutive (they share the A tile in L2). A persistent
+// CTA per SM walks the tiles with three warp roles: warp 0 lane 0 issues the
+// TMA loads (128B-swizzled, K-major) of the four operand tiles of each 64-wide
+// K block into a 2-stage ring; warp 1 lane 0 issues the 3 x 4 UMMAs
+// (M128 x N BN x K16) per K block into one of two FP32 accumulators in tensor
+// memory and commits each stage back to the producer; warps 2-5 read the
+// other accumulator out of tensor memory (tcgen05.ld 32x32b, one row per
+// thread) and store FP32 rows, FP16 rows scaled by a per-row power of two, or
+// half2 row pairs, while the next tile's MMAs run. Every mbarrier wait is
+// bounded: on timeout the CTA records an error code, every role stops issuing
+// work, and the CTA waits (bounded) for its copies and MMAs before freeing
+// its tensor memory.
 #include "wfbp_internal.h"
 #include "wait.cuh"
 
 #include <cuda.h>
+
+#include <algorithm>
 
 namespace {
 
 constexpr int TC_BM = 128;
 constexpr int TC_BK = 64;  // 64 bf16 = 128 bytes, one swizzle row
 constexpr int TC_STAGES = 2;
-constexpr int TC_THREADS = 128;
-constexpr uint32_t TC_TMEM_COLS = 256;
+constexpr int TC_ACC = 2;            // accumulators in tensor memory (MMAs of tile i+1 overlap the epilogue of i)
+constexpr int TC_EPI_THREADS = 128;  // warps 2-5
+constexpr int TC_THREADS = 64 + TC_EPI_THREADS;
+constexpr uint32_t TC_TMEM_COLS = 512;  // TC_ACC x BN (<= 256) columns, a power of two
 
 struct TcParams {
   int M;          // rows of one operand plane of X (V * nrv)
@@ -40,7 +48,6 @@ struct TcParams {
   int BN;         // N tile
   int kblocks;    // Kp / 64
   int np;         // padded N (rows of one B plane)
-  int n_fast;     // 1: blockIdx.x is the N tile (an M tile's N tiles run together and share its A tile in L2)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -103,6 +110,76 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Named barrier of the four epilogue warps (the CTA-wide barrier 0 is not
+// used while the roles run).
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// One output tile's epilogue: the 32 rows of TMEM lane quarter `q` (rows
+// 32q .. 32q+31 of the tile, one per lane) from accumulator columns `acc`.
+__device__ __forceinline__ void tc_epilogue(const TcParams& p, const TcOutArgs& o, uint32_t tmem_acc, int q, int lane,
+                                            int m0, int n0, float (*s_xchg)[16]) {
+  // row m of the tile: view v = m / nrv, row i = m % nrv (rows i >= nr are zero padding)
+  const int m = m0 + q * 32 + lane;
+  const int v = m / o.nrv, i = m % o.nrv;
+  const bool row_ok = m < p.me && i < o.nr;
+  float inv = 1.0f;
+  if (o.mode == TC_OUT_F16_ROWS && row_ok) {
+    inv = 1.0f / o.row_scale_in[m];
+    if (n0 == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
+  } else if (o.mode == TC_OUT_PAIRS && m < p.me) {
+    inv = 1.0f / o.view_scale[v];
+  }
+  const uint32_t trow = tmem_acc + ((uint32_t)(q * 32) << 16);
+  for (int c = 0; c < p.BN; c += 16) {
+    float val[16];
+    tmem_ld16(trow + (uint32_t)c, val);
+    const int n = n0 + c;
+    if (o.mode == TC_OUT_PAIRS) {
+      // partner row i + 1 lives in the next lane, or in lane 0 of the next quarter
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) s_xchg[q][k] = val[k];
+      }
+      epi_sync();
+      float nxt[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        const float dn = __shfl_down_sync(0xffffffffu, val[k], 1);
+        nxt[k] = lane < 31 ? dn : (q < 3 ? s_xchg[q + 1][k] : 0.0f);
+      }
+      epi_sync();
+      if (row_ok) {
+        const bool last = (i == o.nr - 1);
+        for (int k = 0; k < 16 && n + k < p.nch; k++) {
+          const __half2 h = __floats2half2_rn(val[k] * inv, last ? 0.0f : nxt[k] * inv);
+          o.pairs[((size_t)v * p.nch + (n + k)) * o.nrp + i] = *reinterpret_cast<const uint32_t*>(&h);
+        }
+      }
+      continue;
+    }
+    if (!row_ok || n >= p.nch) continue;
+    if (o.mode == TC_OUT_F16_ROWS) {
+      __half* dst = o.y16 + ((size_t)v * o.nr + i) * p.nch + n;
+      if (n + 16 <= p.nch && ((p.nch & 7) == 0)) {
+        __align__(16) __half h[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) h[k] = __float2half_rn(val[k] * inv);
+        reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<uint4*>(h)[0];
+        reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<uint4*>(h)[1];
+      } else {
+        for (int k = 0; k < 16 && n + k < p.nch; k++) dst[k] = __float2half_rn(val[k] * inv);
+      }
+    } else {
+      float* dst = o.y32 + (size_t)m * p.nch + n;
+      for (int k = 0; k < 16 && n + k < p.nch; k++) dst[k] = val[k];
+    }
+  }
+}
+
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcParams p,
               TcOutArgs o, int* __restrict__ err) {
@@ -113,20 +190,29 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * stage_bytes);
   uint64_t* empty = full + TC_STAGES;
-  uint64_t* done = empty + TC_STAGES;
+  uint64_t* acc_full = empty + TC_STAGES;   // MMA -> epilogue: accumulator a holds a finished tile
+  uint64_t* acc_empty = acc_full + TC_ACC;  // epilogue -> MMA: accumulator a has been read
+  uint64_t* done = acc_empty + TC_ACC;      // every issued MMA has completed (teardown)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   __shared__ int s_fail;
-  __shared__ float s_xchg[4][16];  // row 32w of each warp, for the pairs of the warp above
+  __shared__ float s_xchg[4][16];  // row 32q of each lane quarter, for the pairs of the quarter above
+  __shared__ int s_epi_ok[4];
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int mt = p.n_fast ? (int)blockIdx.y : (int)blockIdx.x, nt = p.n_fast ? (int)blockIdx.x : (int)blockIdx.y;
-  const int m0 = p.mb + mt * TC_BM, n0 = nt * p.BN;
+  const int ntn = p.np / p.BN;                                   // N tiles
+  const int mtiles = (p.me - p.mb + TC_BM - 1) / TC_BM;
+  const int ntiles = mtiles * ntn;
+  volatile int* fail = &s_fail;
 
   if (threadIdx.x == 0) {
     s_fail = 0;
     for (int s = 0; s < TC_STAGES; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < TC_ACC; a++) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], TC_EPI_THREADS);
     }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -143,120 +229,107 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  int issued = 0;  // K blocks whose loads the producer issued
-  if (warp == 0 && lane == 0) {
-    for (int kb = 0; kb < p.kblocks; kb++) {
-      const int s = kb % TC_STAGES;
-      if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1)) {
-        atomicExch(&s_fail, 1);
-        break;
+  uint32_t issued = 0;  // K blocks whose loads the producer issued (over all tiles)
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t g = 0;
+      for (int t = blockIdx.x; t < ntiles && !*fail; t += gridDim.x) {
+        const int m0 = p.mb + (t / ntn) * TC_BM, n0 = (t % ntn) * p.BN;
+        for (int kb = 0; kb < p.kblocks; kb++, g++) {
+          const int s = (int)(g % TC_STAGES);
+          const uint32_t u = g / TC_STAGES;
+          if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1)) {
+            atomicExch(&s_fail, 1);
+            break;
+          }
+          if (*fail) break;
+          uint8_t* st = smem + s * stage_bytes;
+          mbar_expect_tx(&full[s], stage_bytes);
+          const int kx = kb * TC_BK;
+          tma_load_2d(st, &mapA, &full[s], kx, m0);
+          tma_load_2d(st + a_bytes, &mapA, &full[s], kx, p.M + m0);
+          tma_load_2d(st + 2 * a_bytes, &mapB, &full[s], kx, n0);
+          tma_load_2d(st + 2 * a_bytes + b_bytes, &mapB, &full[s], kx, p.np + n0);
+          issued = g + 1;
+        }
       }
-      if (*((volatile int*)&s_fail)) break;
-      uint8_t* st = smem + s * stage_bytes;
-      mbar_expect_tx(&full[s], stage_bytes);
-      const int kx = kb * TC_BK;
-      tma_load_2d(st, &mapA, &full[s], kx, m0);
-      tma_load_2d(st + a_bytes, &mapA, &full[s], kx, p.M + m0);
-      tma_load_2d(st + 2 * a_bytes, &mapB, &full[s], kx, n0);
-      tma_load_2d(st + 2 * a_bytes + b_bytes, &mapB, &full[s], kx, p.np + n0);
-      issued = kb + 1;
     }
-  } else if (warp == 1 && lane == 0) {
-    const uint32_t idesc = idesc_bf16(p.BN);
-    bool ok = true;
-    for (int kb = 0; kb < p.kblocks && ok; kb++) {
-      const int s = kb % TC_STAGES;
-      if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1)) {
-        atomicExch(&s_fail, 1);
-        ok = false;
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(p.BN);
+      uint32_t g = 0, it = 0;
+      for (int t = blockIdx.x; t < ntiles && !*fail; t += gridDim.x, it++) {
+        const int a = (int)(it % TC_ACC);
+        const uint32_t ua = it / TC_ACC;
+        if (ua > 0 && !mbar_wait(&acc_empty[a], (ua - 1) & 1)) {
+          atomicExch(&s_fail, 1);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(a * p.BN);
+        bool ok = true;
+        for (int kb = 0; kb < p.kblocks; kb++, g++) {
+          const int s = (int)(g % TC_STAGES);
+          if (!mbar_wait(&full[s], (g / TC_STAGES) & 1) || *fail) {
+            atomicExch(&s_fail, 1);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t st = smem_u32(smem + s * stage_bytes);
+          const uint32_t ahi = st, alo = st + a_bytes, bhi = st + 2 * a_bytes, blo = bhi + b_bytes;
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; kk++) {
+            const uint32_t off = kk * 32;  // 16 bf16 along K inside the swizzle row
+            umma_bf16(d, sw128_desc(ahi + off), sw128_desc(bhi + off), idesc, (kb | kk) ? 1u : 0u);
+            umma_bf16(d, sw128_desc(ahi + off), sw128_desc(blo + off), idesc, 1u);
+            umma_bf16(d, sw128_desc(alo + off), sw128_desc(bhi + off), idesc, 1u);
+          }
+          umma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&acc_full[a]);  // arrives when the tile's MMAs have completed
+      }
+      umma_commit(done);  // arrives when every issued MMA has completed
+    }
+  } else {
+    // epilogue warps 2-5: TMEM lane quarter q = warp % 4 (tcgen05.ld's access rule)
+    const int q = warp % 4;
+    uint32_t it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+      const int a = (int)(it % TC_ACC);
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait(&acc_full[a], (it / TC_ACC) & 1) && !*fail;
+      // the four epilogue warps agree before the named barriers inside the
+      // epilogue, so that either all of them run it or none does
+      if (lane == 0) s_epi_ok[q] = ok;
+      epi_sync();
+      ok = s_epi_ok[0] & s_epi_ok[1] & s_epi_ok[2] & s_epi_ok[3];
+      epi_sync();  // every warp has read the flags before the next tile overwrites them
+      if (!ok) {
+        if (lane == 0) atomicExch(&s_fail, 1);
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t st = smem_u32(smem + s * stage_bytes);
-      const uint32_t ahi = st, alo = st + a_bytes, bhi = st + 2 * a_bytes, blo = bhi + b_bytes;
-#pragma unroll
-      for (int kk = 0; kk < TC_BK / 16; kk++) {
-        const uint32_t off = kk * 32;  // 16 bf16 along K inside the swizzle row
-        umma_bf16(tmem, sw128_desc(ahi + off), sw128_desc(bhi + off), idesc, (kb | kk) ? 1u : 0u);
-        umma_bf16(tmem, sw128_desc(ahi + off), sw128_desc(blo + off), idesc, 1u);
-        umma_bf16(tmem, sw128_desc(alo + off), sw128_desc(bhi + off), idesc, 1u);
-      }
-      umma_commit(&empty[s]);
+      tc_epilogue(p, o, tmem + (uint32_t)(a * p.BN), q, lane, p.mb + (t / ntn) * TC_BM, (t % ntn) * p.BN, s_xchg);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&acc_empty[a]);
     }
-    umma_commit(done);  // arrives when every issued MMA has completed
   }
   __syncwarp();
 
-  // epilogue: warp w owns TMEM lanes / tile rows 32w .. 32w+31
-  const bool have = mbar_wait(done, 0);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (!have) atomicExch(&s_fail, 1);
-  __syncthreads();
-  const bool failed = *((volatile int*)&s_fail) != 0;
-  if (!failed) {
-    // row m of the tile: view v = m / nrv, row i = m % nrv (rows i >= nr are zero padding)
-    const int m = m0 + warp * 32 + lane;
-    const int v = m / o.nrv, i = m % o.nrv;
-    const bool row_ok = m < p.me && i < o.nr;
-    float inv = 1.0f;
-    if (o.mode == TC_OUT_F16_ROWS && row_ok) {
-      inv = 1.0f / o.row_scale_in[m];
-      if (nt == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
-    } else if (o.mode == TC_OUT_PAIRS && m < p.me) {
-      inv = 1.0f / o.view_scale[v];
-    }
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c = 0; c < p.BN; c += 16) {
-      float val[16];
-      tmem_ld16(trow + (uint32_t)c, val);
-      const int n = n0 + c;
-      if (o.mode == TC_OUT_PAIRS) {
-        // partner row i + 1 lives in the next lane, or in lane 0 of the next warp
-        if (lane == 0) {
-#pragma unroll
-          for (int k = 0; k < 16; k++) s_xchg[warp][k] = val[k];
-        }
-        __syncthreads();
-        float nxt[16];
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-          const float dn = __shfl_down_sync(0xffffffffu, val[k], 1);
-          nxt[k] = lane < 31 ? dn : (warp < 3 ? s_xchg[warp + 1][k] : 0.0f);
-        }
-        __syncthreads();
-        if (row_ok) {
-          const bool last = (i == o.nr - 1);
-          for (int k = 0; k < 16 && n + k < p.nch; k++) {
-            const __half2 h = __floats2half2_rn(val[k] * inv, last ? 0.0f : nxt[k] * inv);
-            o.pairs[((size_t)v * p.nch + (n + k)) * o.nrp + i] = *reinterpret_cast<const uint32_t*>(&h);
-          }
-        }
-        continue;
-      }
-      if (!row_ok || n >= p.nch) continue;
-      if (o.mode == TC_OUT_F16_ROWS) {
-        __half* dst = o.y16 + ((size_t)v * o.nr + i) * p.nch + n;
-        if (n + 16 <= p.nch && ((p.nch & 7) == 0)) {
-          __align__(16) __half h[16];
-#pragma unroll
-          for (int k = 0; k < 16; k++) h[k] = __float2half_rn(val[k] * inv);
-          reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<uint4*>(h)[0];
-          reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<uint4*>(h)[1];
-        } else {
-          for (int k = 0; k < 16 && n + k < p.nch; k++) dst[k] = __float2half_rn(val[k] * inv);
-        }
-      } else {
-        float* dst = o.y32 + (size_t)m * p.nch + n;
-        for (int k = 0; k < 16 && n + k < p.nch; k++) dst[k] = val[k];
-      }
-    }
-  } else if (warp == 0 && lane == 0) {
-    atomicExch(err, WFBP_ERR_TIMEOUT);
-    // let issued copies land before the shared memory is released (bounded)
-    for (int kb = (issued > TC_STAGES ? issued - TC_STAGES : 0); kb < issued; kb++)
-      mbar_wait(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
+  // teardown: every MMA and copy this CTA issued has landed before the tensor
+  // memory and the shared memory go away
+  if (warp == 1 && lane == 0) {
+    if (!mbar_wait(done, 0)) atomicExch(&s_fail, 1);
   }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (*fail && warp == 0 && lane == 0) {
+    atomicExch(err, WFBP_ERR_TIMEOUT);
+    for (uint32_t g = (issued > TC_STAGES ? issued - TC_STAGES : 0); g < issued; g++)
+      mbar_wait(&full[g % TC_STAGES], (g / TC_STAGES) & 1);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
@@ -326,12 +399,16 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
   p.kblocks = kp / TC_BK;
   p.np = np;
   if (out.nrv < 1 || TC_BM % out.nrv != 0) return cudaErrorInvalidValue;  // views must not straddle M tiles
+  if (2 * bn > (int)TC_TMEM_COLS) return cudaErrorInvalidValue;
   size_t smem = tc_smem_bytes(bn);
   cudaError_t e = cudaFuncSetAttribute(k_toeplitz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const unsigned mtiles = (unsigned)((me - mb + TC_BM - 1) / TC_BM), ntiles = (unsigned)(np / bn);
-  p.n_fast = mtiles <= 65535u ? 1 : 0;  // gridDim.y limit
-  const dim3 grid = p.n_fast ? dim3(ntiles, mtiles) : dim3(mtiles, ntiles);
+  int dev = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  // persistent CTAs, one per SM (the shared memory of one ring fills an SM)
+  const long tiles = (long)((me - mb + TC_BM - 1) / TC_BM) * (np / bn);
+  const unsigned grid = (unsigned)std::max(1L, std::min<long>(tiles, sms));
   k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(map_a, map_b, p, out, err);
   return cudaGetLastError();
 }

@@ -261,7 +261,8 @@ template <bool FFS>
 __global__ void __launch_bounds__(RS_THREADS)
 k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
                    float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
-                   const float* __restrict__ bidx_t, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
+                   const float* __restrict__ bidx_t, const double2* __restrict__ chan64, RebinParams p, int kp,
+                   int nrv, float taps_l1, int vb) {
   extern __shared__ float s_rowmax[];  // [nrv]
   const int v = vb + blockIdx.x;
   const int lane = threadIdx.x % 32;
@@ -275,8 +276,13 @@ k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_
     t.ok = false;
     tf.ok = false;
     if (valid) {
-      if constexpr (FFS) tf = rebin_taps_ffs(p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
-      else t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+      if (chan64) {  // FP64 sample coordinates
+        if constexpr (FFS) tf = rebin_taps_ffs64(p, __ldg(chan64 + c), v);
+        else t = rebin_taps64(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, __ldg(chan64 + c), v, p.voff);
+      } else {
+        if constexpr (FFS) tf = rebin_taps_ffs(p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+        else t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+      }
     }
     // four rows' samples (16 independent loads) before their stores and reductions
     for (int i0 = 0; i0 < nrv; i0 += 4) {
@@ -315,20 +321,106 @@ k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_
   if (threadIdx.x == 0) view_scale[v] = s_vmax;
 }
 
+// Without a flying focal spot the same samples with more work per thread:
+// thread t owns the channel pairs t + k * RS_THREADS (k < NP) of the view,
+// keeps their taps in registers and walks the rows two at a time with all its
+// samples' loads (NP x 2 channels x 2 rows x 4 texels) issued before their
+// stores; each row's two channels go out as one 4-byte BF16x2 word per plane,
+// and the row maximum takes one warp reduction per row (over the thread's
+// channels first). Same sample arithmetic, planes and scales bit for bit.
+template <int NP>
+__global__ void __launch_bounds__(RS_THREADS)
+k_rebin_split_pairs(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
+                    float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
+                    const float* __restrict__ bidx_t, const double2* __restrict__ chan64, RebinParams p, int kp,
+                    int nrv, float taps_l1, int vb) {
+  extern __shared__ float s_rowmax[];  // [nrv]
+  const int v = vb + blockIdx.x;
+  const int lane = threadIdx.x % 32;
+  for (int i = threadIdx.x; i < nrv; i += blockDim.x) s_rowmax[i] = 0.0f;
+  RebinTaps t[NP][2];
+  bool pv[NP];  // the pair lies inside [0, kp)
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    const int c0 = 2 * ((int)threadIdx.x + k * RS_THREADS);
+    pv[k] = c0 < kp;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int c = c0 + h;
+      t[k][h].ok = false;
+      t[k][h].raw0 = t[k][h].raw1 = raw;
+      t[k][h].c0 = t[k][h].c1 = 0;
+      t[k][h].ax = t[k][h].ay = 0.0f;
+      if (c < p.nch) {
+        if (chan64) t[k][h] = rebin_taps64(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, __ldg(chan64 + c), v, p.voff);
+        else t[k][h] = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i0 = 0; i0 < nrv; i0 += 2) {
+    float x[NP][2][2];  // [pair][row][channel]
+#pragma unroll
+    for (int k = 0; k < NP; k++)
+#pragma unroll
+      for (int u = 0; u < 2; u++)
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+          x[k][u][h] = i0 + u >= p.nr ? 0.0f  // 0 off the detector and in the padding
+                                      : rebin_taps_sample(t[k][h], i0 + u, p.nch);
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int i = i0 + u;
+      if (i >= nrv) break;  // warp-uniform
+      const size_t row = (size_t)v * nrv + i;
+      float m = 0.0f;
+#pragma unroll
+      for (int k = 0; k < NP; k++) {
+        if (!pv[k]) continue;
+        const int c0 = 2 * ((int)threadIdx.x + k * RS_THREADS);
+        const __nv_bfloat162 hi = __floats2bfloat162_rn(x[k][u][0], x[k][u][1]);
+        const float2 hf = __bfloat1622float2(hi);
+        const __nv_bfloat162 lo = __floats2bfloat162_rn(x[k][u][0] - hf.x, x[k][u][1] - hf.y);
+        *reinterpret_cast<__nv_bfloat162*>(a_hi + row * kp + c0) = hi;
+        *reinterpret_cast<__nv_bfloat162*>(a_lo + row * kp + c0) = lo;
+        // fmaxf semantics: a NaN sample does not raise the maximum
+        m = fmaxf(m, fmaxf(isnan(x[k][u][0]) ? 0.0f : fabsf(x[k][u][0]), isnan(x[k][u][1]) ? 0.0f : fabsf(x[k][u][1])));
+      }
+      const unsigned mm = __reduce_max_sync(0xffffffffu, __float_as_uint(m));  // m >= 0: bits order as values
+      if (lane == 0 && mm) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)mm);
+    }
+  }
+  __syncthreads();
+  __shared__ float s_vmax;
+  if (threadIdx.x == 0) s_vmax = 0.0f;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nrv; i += blockDim.x) {
+    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
+    const float sc = exp2f(ceilf(log2f(bound)));
+    row_scale[(size_t)v * nrv + i] = sc;
+    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) view_scale[v] = s_vmax;
+}
+
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
-                               const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
-                               float taps_l1, cudaStream_t s, int vb, int ve) {
+                               const float* d_beta, const float* d_bidx, const double2* d_chan64,
+                               const RebinParams& p, int kp, int nrv, float taps_l1, cudaStream_t s, int vb, int ve) {
   if (ve < 0) ve = p.V;
   if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
   const size_t rows = (size_t)p.V * nrv;
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
   __nv_bfloat16* lo = hi + rows * kp;
   if (kp % 64 != 0) return cudaErrorInvalidValue;  // whole warps per channel run (the row maxima's reduction)
-  if (p.G == 1)
+  if (p.G == 1 && kp <= 4 * RS_THREADS)
+    k_rebin_split_pairs<2><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
+        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
+  else if (p.G == 1)
     k_rebin_split_rows<false><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
-        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
+        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   else
     k_rebin_split_rows<true><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
-        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, p, kp, nrv, taps_l1, vb);
+        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   return cudaGetLastError();
 }

@@ -55,6 +55,32 @@ __device__ __forceinline__ RebinTaps rebin_taps(const float* __restrict__ raw, s
   return t;
 }
 
+// rebin_taps with FP64 sample coordinates (the mixed form): the source
+// channel index bidx and beta / dtheta come from the context's FP64
+// per-channel table, the fractional view index (v + voff) - beta / dtheta and
+// both fractional weights are formed in double (the FP64 oracle's
+// arithmetic, oracle/wfbp_oracle.c rb64_body) and only the weights rounded to
+// FP32. Exact weights (no 8-bit texture fractions).
+__device__ __forceinline__ RebinTaps rebin_taps64(const float* __restrict__ raw, size_t view_stride, int V, int nr,
+                                                  int nch, double2 ch, int v, int voff) {
+  RebinTaps t;
+  t.ok = !isnan(ch.x);
+  const double aidx = (double)(v + voff) - ch.y;
+  const double fx = t.ok ? floor(ch.x) : 0.0, fy = floor(aidx);
+  int x0 = (int)fx, y0 = (int)fy - voff;
+  int x1 = min(max(x0 + 1, 0), nch - 1), y1 = min(max(y0 + 1, 0), V - 1);
+  x0 = min(max(x0, 0), nch - 1);
+  y0 = min(max(y0, 0), V - 1);
+  const float* last = raw + (size_t)(nr - 1) * nch;
+  t.raw0 = last + (size_t)y0 * view_stride;
+  t.raw1 = last + (size_t)y1 * view_stride;
+  t.c0 = nch - 1 - x0;
+  t.c1 = nch - 1 - x1;
+  t.ax = t.ok ? (float)(ch.x - fx) : 0.0f;
+  t.ay = (float)(aidx - fy);
+  return t;
+}
+
 // The bilinear sample of sheet row i (raw row nr-1-i) at the taps.
 __device__ __forceinline__ float rebin_taps_sample(const RebinTaps& t, int i, int nch) {
   if (!t.ok) return 0.0f;
@@ -135,6 +161,34 @@ __device__ __forceinline__ RebinTapsFfs rebin_taps_ffs(const RebinParams& p, flo
       float ay = mf - m0;
       if (p.q8) ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
       T.ay[zs][t] = ay;
+      const int ma = min(max((int)m0 - p.voff, 0), p.V - 1), mb = min(max((int)m0 + 1 - p.voff, 0), p.V - 1);
+      T.oa[zs][t] = (size_t)(p.G * ma + rho) * vs + (size_t)(p.nch_raw - 1 - b);
+      T.ob[zs][t] = (size_t)(p.G * mb + rho) * vs + (size_t)(p.nch_raw - 1 - b);
+    }
+  return T;
+}
+
+// rebin_taps_ffs with FP64 sample coordinates (the mixed form; exact
+// weights): reading index G (v + voff) - beta / dtheta_reading and the
+// per-state fractional readings in double, as the FP64 oracle's rbf_body.
+__device__ __forceinline__ RebinTapsFfs rebin_taps_ffs64(const RebinParams& p, double2 ch, int v) {
+  RebinTapsFfs T;
+  T.ok = !isnan(ch.x);
+  const size_t vs = (size_t)p.nr_raw * p.nch_raw;
+  const double nf = (double)(p.G * (v + p.voff)) - ch.y;
+  const double fx = T.ok ? floor(ch.x) : 0.0;
+  const float ax = T.ok ? (float)(ch.x - fx) : 0.0f;
+#pragma unroll
+  for (int zs = 0; zs < 2; zs++)
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int e = min(max((int)fx + t, 0), p.nch - 1);
+      T.we[zs][t] = t ? ax : 1.0f - ax;
+      const int sp = p.phi ? (e & 1) : 0, b = p.phi ? (e >> 1) : e;
+      const int z = p.zf ? zs : 0;
+      const int rho = (p.G == 4) ? sp + 2 * z : (p.phi ? sp : z);
+      const double mf = (nf - (double)rho) / (double)p.G, m0 = floor(mf);
+      T.ay[zs][t] = (float)(mf - m0);
       const int ma = min(max((int)m0 - p.voff, 0), p.V - 1), mb = min(max((int)m0 + 1 - p.voff, 0), p.V - 1);
       T.oa[zs][t] = (size_t)(p.G * ma + rho) * vs + (size_t)(p.nch_raw - 1 - b);
       T.ob[zs][t] = (size_t)(p.G * mb + rho) * vs + (size_t)(p.nch_raw - 1 - b);

@@ -163,6 +163,9 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->d_chan_beta);
   free_dev(ctx->d_chan_bidx);
   free_dev(ctx->d_view_sc);
+  free_dev(ctx->d_view_sc64);
+  free_dev(ctx->d_view_z64);
+  free_dev(ctx->d_chan64);
   free_dev(ctx->d_view_z);
   free_dev(ctx->d_z_native);
   free_dev(ctx->d_thick_off);
@@ -188,6 +191,7 @@ void release(wfbp_ctx* ctx) {
   for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
   ctx->ev_copy.clear();
   if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
+  if (ctx->s_back) cudaStreamDestroy(ctx->s_back);
   ctx->s_copy = nullptr;
   for (auto& b : ctx->s_bp) {
     if (b) cudaStreamDestroy(b);
@@ -235,6 +239,8 @@ BPParams bp_params(const wfbp_ctx* ctx) {
   p.nrm2 = (float)(ctx->nr - 2);
   p.ncm2 = (float)(ctx->nch - 2);
   p.dtheta = ctx->gp.two_pi_over_projections_per_rotation;
+  p.sc64 = ctx->d_view_sc64;
+  p.z64 = ctx->d_view_z64;
   return p;
 }
 
@@ -657,6 +663,8 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
   if (!ce) ce = alloc_copy((void**)&ctx->d_chan_beta, nullptr, sizeof(float) * ctx->nch);
   if (!ce) ce = alloc_copy((void**)&ctx->d_chan_bidx, nullptr, sizeof(float) * ctx->nch);
   if (!ce) ce = alloc_copy((void**)&ctx->d_view_sc, nullptr, sizeof(float2) * ctx->V);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_view_sc64, nullptr, sizeof(double2) * ctx->V);
+  if (!ce) ce = alloc_copy((void**)&ctx->d_view_z64, nullptr, sizeof(double) * ctx->V);
   if (!ce) ce = alloc_copy((void**)&ctx->d_view_z, nullptr, sizeof(float) * ctx->V);
   if (!ce) ce = alloc_copy((void**)&ctx->d_err, nullptr, sizeof(int));
   if (!ce) ce = cudaMemset(ctx->d_err, 0, sizeof(int));
@@ -682,6 +690,19 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
         b[plane + (size_t)n * ctx->tc_kp + k] = bf16_rn(h - bf16_to_f(hi));
       }
     ce = alloc_copy(&ctx->d_bplanes, b.data(), sizeof(uint16_t) * b.size());
+    // FP64 sample coordinates of the mixed form's rebin (rebin_kernel,
+    // cuda_kernels.cuh:17-22, in double): per output channel the source
+    // channel index (NaN off the detector) and beta / dtheta per reading
+    const double c0 = cg->detector_central_col, dcol = cg->detector_pixel_size_col,
+                 sdd = cg->distance_source_to_detector;
+    const double dth = 2.0 * M_PI / (double)ctx->cg_read.projections_per_rotation;
+    std::vector<double2> ch(nch);
+    for (int c = 0; c < nch; c++) {
+      const double beta = asin(((double)c - c0) * dcol / sdd);
+      const double bidx = beta * sdd / dcol + c0;
+      ch[c] = make_double2(bidx < 0.0 || bidx >= (double)nch || std::isnan(bidx) ? NAN : bidx, beta / dth);
+    }
+    if (!ce) ce = alloc_copy((void**)&ctx->d_chan64, ch.data(), sizeof(double2) * nch);
   }
   if (!ce) ce = launch_rebin_tables(ctx->d_chan_beta, ctx->d_chan_bidx, ctx->nch, cg->detector_central_col,
                                     cg->detector_pixel_size_col, cg->distance_source_to_detector, 0);
@@ -752,6 +773,18 @@ WFBP_API int wfbp_set_views(wfbp_ctx* ctx, const float* tube, const float* table
   if (!e) e = cudaMemcpy(d_t, tube, sizeof(float) * ctx->V, cudaMemcpyHostToDevice);
   if (!e) e = cudaMemcpy(d_z, table, sizeof(float) * ctx->V, cudaMemcpyHostToDevice);
   if (!e) e = launch_view_tables(d_t, d_z, ctx->d_view_sc, ctx->d_view_z, ctx->V, 0);
+  if (!e) {
+    // FP64 per-view geometry: sin / cos of the tube angle and the table
+    // position in double (the mixed form's backprojection records)
+    std::vector<double2> sc64(ctx->V);
+    std::vector<double> z64(ctx->V);
+    for (int v = 0; v < ctx->V; v++) {
+      sc64[v] = make_double2(sin((double)tube[v]), cos((double)tube[v]));
+      z64[v] = (double)table[v];
+    }
+    e = cudaMemcpy(ctx->d_view_sc64, sc64.data(), sizeof(double2) * ctx->V, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(ctx->d_view_z64, z64.data(), sizeof(double) * ctx->V, cudaMemcpyHostToDevice);
+  }
   if (!e) e = cudaDeviceSynchronize();
   cudaFree(d_t);
   cudaFree(d_z);
@@ -904,7 +937,8 @@ int do_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, int vb, int ve, vo
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
     float *row_sc, *view_sc;
     mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
-    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, row_sc, view_sc, ctx->d_chan_beta, ctx->d_chan_bidx, p,
+    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, row_sc, view_sc, ctx->d_chan_beta, ctx->d_chan_bidx,
+                                     ctx->ext.tex_weights ? nullptr : ctx->d_chan64, p,
                                      ctx->tc_kp, ctx->nrv, ctx->taps_l1, (cudaStream_t)stream, vb, ve));
   } else {
     CUDA_TRY(ctx, launch_rebin_f32(raw, (float*)rebinned, ctx->d_chan_beta, ctx->d_chan_bidx, p, (cudaStream_t)stream,
@@ -1337,6 +1371,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   const int lay = WFBP_LAYOUT_BACKPROJECTION;
   constexpr int kChunks = 8;
   if (!ctx->s_copy) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
+  if (!ctx->s_back) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_back, cudaStreamNonBlocking));
   for (auto& b : ctx->s_bp)
     if (!b) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
   if (ctx->ev_copy.empty()) {
@@ -1393,7 +1428,8 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   const bool mixed = ctx->ext.precision == WFBP_PRECISION_MIXED;
   // fused thickening: the requested slices inside a slab are final when its
   // launch ends; with a pinned destination they are copied back right away
-  // (on the copy stream, behind the launch's event) while later slabs run
+  // (on a stream of their own, behind the launch's event) while later slabs
+  // run, so no later reading chunk's upload waits behind a copy-back
   if ((st = prepare_fuse(ctx))) return st;
   const bool fuse = ctx->fuse_ok;
   const ThickFuse tf = make_fuse(ctx, ctx->s_vol);
@@ -1442,8 +1478,8 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
           for (int i = ctx->fuse_slab_h[k].x; i < ctx->fuse_slab_h[k].y; i++) rs.push_back(ctx->fuse_req_h[i]);
         if (!rs.empty()) {
           CUDA_TRY(ctx, cudaEventRecord(ev_done, sb));
-          CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_copy, ev_done, 0));
-          const int cst = copy_back(rs, ctx->s_copy);
+          CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->s_back, ev_done, 0));
+          const int cst = copy_back(rs, ctx->s_back);
           if (cst) return cst;
           for (int r : rs) copied[r] = 1;
         }
@@ -1474,6 +1510,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     if (!copied[r]) rest.push_back(r);
   if ((st = copy_back(rest, s))) return st;
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->s_copy));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->s_back));
   CUDA_TRY(ctx, cudaStreamSynchronize(s));
   return wfbp_check_device_status(ctx);
 }

@@ -32,6 +32,8 @@ struct BPParams {
   float nrm2;                // nr - 2 (last valid floor row)
   float ncm2;                // nch - 2
   float dtheta;              // two_pi_over_projections_per_rotation
+  const double2* sc64;       // [V] FP64 (sin, cos) of the tube angle (the mixed form's geometry)
+  const double* z64;         // [V] FP64 table position
 };
 
 // Launch configuration of the TMA-staged backprojection (k_bp_tma.cu),
@@ -117,6 +119,9 @@ struct wfbp_ctx {
   float* d_chan_beta = nullptr;     // [nch]
   float* d_chan_bidx = nullptr;     // [nch], NaN where the rebin writes 0
   float2* d_view_sc = nullptr;      // [V] (sinf, cosf) of the tube angle
+  double2* d_view_sc64 = nullptr;   // [V] FP64 (sin, cos) of the tube angle
+  double* d_view_z64 = nullptr;     // [V] FP64 table position
+  double2* d_chan64 = nullptr;      // [nch] mixed form: FP64 (source channel index or NaN, beta / dtheta)
   float* d_view_z = nullptr;        // [V] table position
   float* d_z_native = nullptr;      // [nz]
   int* d_thick_off = nullptr;
@@ -170,6 +175,7 @@ struct wfbp_ctx {
   float* s_raw = nullptr;
   float* s_vol = nullptr;
   cudaStream_t s_copy = nullptr;    // wfbp_run_host: host-to-device copies of the reading chunks
+  cudaStream_t s_back = nullptr;    // wfbp_run_host: device-to-host copies of finished slices
   cudaStream_t s_bp[2] = {nullptr, nullptr};  // wfbp_run_host: backprojection launches (alternating)
   std::vector<cudaEvent_t> ev_copy; // one per chunk, plus the caller-stream fence
 
@@ -194,8 +200,9 @@ cudaError_t launch_backproject_f16(const __half* D, const float* scales, float* 
                                    const float* vz, const float* zs, const BPParams& p, unsigned long long* count,
                                    cudaStream_t s);
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
-                               const float* d_beta, const float* d_bidx, const RebinParams& p, int kp, int nrv,
-                               float taps_l1, cudaStream_t s, int vb = 0, int ve = -1);
+                               const float* d_beta, const float* d_bidx, const double2* d_chan64,
+                               const RebinParams& p, int kp, int nrv, float taps_l1, cudaStream_t s, int vb = 0,
+                               int ve = -1);
 // Output modes of the tensor-core filter epilogue.
 enum TcOut { TC_OUT_F32 = 0, TC_OUT_F16_ROWS = 1, TC_OUT_PAIRS = 2 };
 struct TcOutArgs {

@@ -141,8 +141,10 @@ enum wfbp_status {
 
 enum wfbp_precision {
   WFBP_PRECISION_FP32 = 0,    /* FP32 rebin, FP32 SIMT Toeplitz filter, FP32 rows, FP32 backprojection */
-  WFBP_PRECISION_MIXED = 1    /* split hi+lo BF16 tcgen05 filter (FP32 accumulate in TMEM),
-                                 FP16 filtered rows with per-row scales, FP32 backprojection */
+  WFBP_PRECISION_MIXED = 1    /* rebin with FP64 sample coordinates into split hi+lo BF16 planes,
+                                 tcgen05 filter (FP32 accumulate in TMEM), FP16 filtered rows with
+                                 power-of-two scales, backprojection with FP64 per-view geometry
+                                 and FP32 accumulation */
 };
 
 enum wfbp_filter_window {
@@ -275,7 +277,10 @@ int wfbp_ctx_destroy(wfbp_ctx* ctx);
 int wfbp_query(const wfbp_ctx* ctx, wfbp_dims* dims);
 
 /* Per-view tube angles and table positions, host arrays of n_readings floats
- * (ReconstructionMachine.cu:96-102). Builds the FP64 per-view tables. */
+ * (ReconstructionMachine.cu:96-102). Builds the per-view tables: sinf / cosf
+ * and the table position in FP32, as the reference evaluates them per voxel
+ * (cuda_kernels.cuh:235-238), for the FP32 form, and sin / cos / table
+ * position in FP64 for the mixed form's backprojection geometry. */
 int wfbp_set_views(wfbp_ctx* ctx, const float* tube_angles, const float* table_positions);
 
 /* The geometry the stages work on: the caller's CTGeometry, or for a flying

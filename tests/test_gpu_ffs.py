@@ -59,15 +59,16 @@ def test_ffs_fp32_vs_fp64(orc, mode):
         assert rms < 0.1 and mx < 1.0, (mode, layout, rms, mx)
 
 
+@pytest.mark.parametrize("layout", [T.LAYOUT_REFERENCE, T.LAYOUT_BACKPROJECTION])
 @pytest.mark.parametrize("mode", MODES)
-def test_ffs_mixed_vs_fp64(orc, mode):
+def test_ffs_mixed_vs_fp64(orc, mode, layout):
     spec = scans.tiny_ffs(mode=mode, nch=64, nr=8, P=256)
     raw = orc.synth_project(spec.synth(), spec.ellipsoids())
     r64 = orc.reconstruct_f64(spec, raw)
-    _, got = run(spec, raw, T.PRECISION_MIXED)
+    _, got = run(spec, raw, T.PRECISION_MIXED, layout)
     rms, mx, n = orc.hu_error(got, r64["volume"])
     assert n == np.isfinite(r64["volume"]).sum()
-    assert rms <= 1.0, (mode, rms, mx)
+    assert rms <= 1.0, (mode, layout, rms, mx)
 
 
 def test_ffs_reconstructs_phantom(orc):
