@@ -705,8 +705,9 @@ def stage_rooflines(form, ctx, d, updates, stage, clk):
     capture, scaled by updates) is reported against the compulsory bytes
     (filtered rows read once, native volume written once).
     rebin: HBM, raw frames read once + rebinned output written once.
-    filter: tensor pipe (mixed: 3 split-BF16 products of 2 (V nr) nch^2
-    FLOP each, against the sustained cuBLAS BF16 rate) or FP32 FFMA (FP32
+    filter: tensor pipe (mixed: 3 split-FP16 products of 2 (V nr) nch^2
+    FLOP each, against the sustained cuBLAS BF16 rate, the same tensor rate
+    as FP16) or FP32 FFMA (FP32
     form: 2 (V nr) nch^2 FLOP against 148 SMs x 128 lanes x 2 x clock)."""
     hbm, bf16, bf16_sus, peak_src = load_peaks()
     mhz = (clk or {}).get("sm_mhz") or 1965.0
@@ -731,7 +732,7 @@ def stage_rooflines(form, ctx, d, updates, stage, clk):
                   "%d SMs x %d schedulers x %.0f MHz (sampled); taps are shared-memory reads after one TMA "
                   "staging per view window" % (SMS, SCHEDULERS_PER_SM, mhz)}
     samples = d.n_views * d.n_rows * d.n_channels
-    rebin_bytes = d.raw_bytes + samples * 4  # FP32 rows, or the two BF16 operand planes
+    rebin_bytes = d.raw_bytes + samples * 4  # FP32 rows, or the two FP16 operand planes
     t_rb = stage["rebin"] / 1000.0
     rebin = {"bound": "hbm", "kernel": "rebin", "achieved": rebin_bytes / t_rb / 1e9, "peak": hbm, "unit": "GB/s",
              "frac": rebin_bytes / t_rb / 1e9 / hbm, "algorithmic_bytes": rebin_bytes,
@@ -742,8 +743,8 @@ def stage_rooflines(form, ctx, d, updates, stage, clk):
         flop = 3 * 2.0 * rows * d.n_channels * d.n_channels
         filt = {"bound": "tensor", "kernel": "toeplitz_tc", "achieved": flop / t_f / 1e12, "peak": bf16_sus,
                 "unit": "TFLOP/s", "frac": flop / t_f / 1e12 / bf16_sus, "algorithmic_flop": flop,
-                "note": "3 split-BF16 products (hi*hi, hi*lo, lo*hi) of 2 M K N, M = views x rows, K = N = "
-                        "channels, against the sustained cuBLAS BF16 rate"}
+                "note": "3 split-FP16 products (hi*hi, hi*lo, lo*hi) of 2 M K N, M = views x rows, K = N = "
+                        "channels, against the sustained cuBLAS BF16 rate (FP16 runs at the same tensor rate)"}
     else:
         flop = 2.0 * rows * d.n_channels * d.n_channels
         fpk = SMS * 128 * 2 * mhz * 1e6 / 1e12

@@ -244,62 +244,98 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // rebin for the mixed-precision filter
 // ---------------------------------------------------------------------------
 //
-// Same samples as k_rebin_f32_rows, written as the two BF16 operand planes of the
-// tensor-core Toeplitz filter: hi = bf16(x), lo = bf16(x - hi). One CTA per
-// view; the view's rows are padded with zero rows to nrv (a power of two that
-// divides the filter's 128-row tile, so no view straddles a tile) and every
-// row with zeros to kp (a multiple of 64). The CTA also writes the FP16
-// storage scales: per row, the smallest power of two s with
-// max|x| * sum|h| / s <= 16384 (|y| <= sum|h| max|x| bounds every filtered
-// value of the row), and per view the largest of its rows' scales.
+// Same samples as k_rebin_f32_rows, written as the two FP16 operand planes of
+// the tensor-core Toeplitz filter: with a per-view power of two o (the
+// largest with o max|x| <= 16384, so no operand overflows FP16),
+// hi = f16(o x), lo = f16(o x - hi), 22 bits of x. One CTA per view walks the
+// view twice: the first pass finds the row maxima, the second writes the
+// planes. The view's rows are padded with zero rows to nrv (a power of two
+// that divides the filter's 128-row tile, so no view straddles a tile) and
+// every row with zeros to kp (a multiple of 64). The CTA also writes the FP16
+// storage scales of the filtered rows: per row, the smallest power of two s
+// with max|x| * sum|h| / s <= 16384 (|y| <= sum|h| max|x| bounds every
+// filtered value of the row), per view the largest of its rows' scales, and
+// the operand scale o.
 constexpr int RS_THREADS = 256;
 
 // One thread per channel of the view computes the channel's taps once
 // (as k_rebin_f32_rows) and walks every row; the per-row maxima go through a
 // warp reduction and one shared-memory atomic per warp and row.
+// Scales of one view from its row maxima (shared memory, [nrv]): row and
+// view storage scales of the filtered rows and the operand scale (a power of
+// two; 1 for an all-zero view). Returns the operand scale.
+__device__ float split_view_scales(const float* s_rowmax, int nrv, int v, float taps_l1, float* __restrict__ row_scale,
+                                   float* __restrict__ view_scale, float* __restrict__ op_scale) {
+  __shared__ float s_vmax, s_xmax;
+  if (threadIdx.x == 0) s_vmax = s_xmax = 0.0f;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nrv; i += blockDim.x) {
+    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
+    const float sc = exp2f(ceilf(log2f(bound)));
+    row_scale[(size_t)v * nrv + i] = sc;
+    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
+    atomicMax(reinterpret_cast<int*>(&s_xmax), __float_as_int(s_rowmax[i]));
+  }
+  __syncthreads();
+  const float xm = s_xmax;
+  const float o = xm > 0.0f ? exp2f(floorf(log2f(16384.0f / xm))) : 1.0f;
+  if (threadIdx.x == 0) {
+    view_scale[v] = s_vmax;
+    op_scale[v] = o;
+  }
+  return o;
+}
+
+// Writes o x as FP16 hi / lo.
+__device__ __forceinline__ void split_f16(float x, float o, __half* hi, __half* lo) {
+  const float y = x * o;  // o is a power of two: exact
+  const __half h = __float2half_rn(y);
+  *hi = h;
+  *lo = __float2half_rn(y - __half2float(h));
+}
+
 template <bool FFS>
 __global__ void __launch_bounds__(RS_THREADS)
-k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
-                   float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
-                   const float* __restrict__ bidx_t, const double2* __restrict__ chan64, RebinParams p, int kp,
-                   int nrv, float taps_l1, int vb) {
+k_rebin_split_rows(const float* __restrict__ raw, __half* __restrict__ a_hi, __half* __restrict__ a_lo,
+                   float* __restrict__ row_scale, float* __restrict__ view_scale, float* __restrict__ op_scale,
+                   const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
+                   const double2* __restrict__ chan64, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
   extern __shared__ float s_rowmax[];  // [nrv]
   const int v = vb + blockIdx.x;
   const int lane = threadIdx.x % 32;
   for (int i = threadIdx.x; i < nrv; i += blockDim.x) s_rowmax[i] = 0.0f;
   __syncthreads();
-  // kp is a multiple of 64, so every warp is either wholly inside [0, kp) or wholly outside
-  for (int c = threadIdx.x; c < kp; c += blockDim.x) {
-    const bool valid = c < p.nch;
-    RebinTaps t;
-    RebinTapsFfs tf;
+  auto taps = [&](int c, RebinTaps& t, RebinTapsFfs& tf) {
     t.ok = false;
     tf.ok = false;
-    if (valid) {
-      if (chan64) {  // FP64 sample coordinates
-        if constexpr (FFS) tf = rebin_taps_ffs64(p, __ldg(chan64 + c), v);
-        else t = rebin_taps64(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, __ldg(chan64 + c), v, p.voff);
-      } else {
-        if constexpr (FFS) tf = rebin_taps_ffs(p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
-        else t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
-      }
+    if (c >= p.nch) return;
+    if (chan64) {  // FP64 sample coordinates
+      if constexpr (FFS) tf = rebin_taps_ffs64(p, __ldg(chan64 + c), v);
+      else t = rebin_taps64(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, __ldg(chan64 + c), v, p.voff);
+    } else {
+      if constexpr (FFS) tf = rebin_taps_ffs(p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+      else t = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
     }
-    // four rows' samples (16 independent loads) before their stores and reductions
+  };
+  auto sample = [&](const RebinTaps& t, const RebinTapsFfs& tf, int i) -> float {
+    return i >= p.nr ? 0.0f  // 0 off the detector and in the padding
+                     : FFS ? rebin_taps_ffs_sample(raw, p, tf, i) : rebin_taps_sample(t, i, p.nch);
+  };
+  // pass 1: row maxima; kp is a multiple of 64, so every warp is either wholly
+  // inside [0, kp) or wholly outside
+  for (int c = threadIdx.x; c < kp; c += blockDim.x) {
+    RebinTaps t;
+    RebinTapsFfs tf;
+    taps(c, t, tf);
+    // four rows' samples (16 independent loads) before their reductions
     for (int i0 = 0; i0 < nrv; i0 += 4) {
       float x[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++)
-        x[u] = i0 + u >= p.nr ? 0.0f  // 0 off the detector and in the padding
-               : FFS ? rebin_taps_ffs_sample(raw, p, tf, i0 + u) : rebin_taps_sample(t, i0 + u, p.nch);
+      for (int u = 0; u < 4; u++) x[u] = sample(t, tf, i0 + u);
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const int i = i0 + u;
         if (i >= nrv) break;  // warp-uniform
-        const __nv_bfloat16 hi = __float2bfloat16_rn(x[u]);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(x[u] - __bfloat162float(hi));
-        const size_t row = (size_t)v * nrv + i;
-        a_hi[row * kp + c] = hi;
-        a_lo[row * kp + c] = lo;
         // fmaxf semantics: a NaN sample does not raise the maximum
         const float ax = isnan(x[u]) ? 0.0f : fabsf(x[u]);
         const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(ax));  // ax >= 0: bits order as values
@@ -308,32 +344,40 @@ k_rebin_split_rows(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_
     }
   }
   __syncthreads();
-  __shared__ float s_vmax;
-  if (threadIdx.x == 0) s_vmax = 0.0f;
-  __syncthreads();
-  for (int i = threadIdx.x; i < nrv; i += blockDim.x) {
-    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
-    const float sc = exp2f(ceilf(log2f(bound)));
-    row_scale[(size_t)v * nrv + i] = sc;
-    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
+  const float o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
+  // pass 2: the operand planes
+  for (int c = threadIdx.x; c < kp; c += blockDim.x) {
+    RebinTaps t;
+    RebinTapsFfs tf;
+    taps(c, t, tf);
+    for (int i0 = 0; i0 < nrv; i0 += 4) {
+      float x[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) x[u] = sample(t, tf, i0 + u);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + u;
+        if (i >= nrv) break;
+        const size_t row = (size_t)v * nrv + i;
+        split_f16(x[u], o, a_hi + row * kp + c, a_lo + row * kp + c);
+      }
+    }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) view_scale[v] = s_vmax;
 }
 
 // Without a flying focal spot the same samples with more work per thread:
 // thread t owns the channel pairs t + k * RS_THREADS (k < NP) of the view,
 // keeps their taps in registers and walks the rows two at a time with all its
 // samples' loads (NP x 2 channels x 2 rows x 4 texels) issued before their
-// stores; each row's two channels go out as one 4-byte BF16x2 word per plane,
+// use; each row's two channels go out as one 4-byte FP16x2 word per plane,
 // and the row maximum takes one warp reduction per row (over the thread's
 // channels first). Same sample arithmetic, planes and scales bit for bit.
 template <int NP>
 __global__ void __launch_bounds__(RS_THREADS)
-k_rebin_split_pairs(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a_hi, __nv_bfloat16* __restrict__ a_lo,
-                    float* __restrict__ row_scale, float* __restrict__ view_scale, const float* __restrict__ beta_t,
-                    const float* __restrict__ bidx_t, const double2* __restrict__ chan64, RebinParams p, int kp,
-                    int nrv, float taps_l1, int vb) {
+k_rebin_split_pairs(const float* __restrict__ raw, __half* __restrict__ a_hi, __half* __restrict__ a_lo,
+                    float* __restrict__ row_scale, float* __restrict__ view_scale, float* __restrict__ op_scale,
+                    const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
+                    const double2* __restrict__ chan64, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
   extern __shared__ float s_rowmax[];  // [nrv]
   const int v = vb + blockIdx.x;
   const int lane = threadIdx.x % 32;
@@ -358,69 +402,124 @@ k_rebin_split_pairs(const float* __restrict__ raw, __nv_bfloat16* __restrict__ a
     }
   }
   __syncthreads();
-  for (int i0 = 0; i0 < nrv; i0 += 2) {
-    float x[NP][2][2];  // [pair][row][channel]
+  for (int pass = 0; pass < 2; pass++) {
+    // pass 0: row maxima; pass 1: the operand planes with the view's operand scale
+    float o = 1.0f;
+    if (pass == 1) o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
+    for (int i0 = 0; i0 < nrv; i0 += 2) {
+      float x[NP][2][2];  // [pair][row][channel]
 #pragma unroll
-    for (int k = 0; k < NP; k++)
+      for (int k = 0; k < NP; k++)
 #pragma unroll
-      for (int u = 0; u < 2; u++)
+        for (int u = 0; u < 2; u++)
 #pragma unroll
-        for (int h = 0; h < 2; h++)
-          x[k][u][h] = i0 + u >= p.nr ? 0.0f  // 0 off the detector and in the padding
-                                      : rebin_taps_sample(t[k][h], i0 + u, p.nch);
+          for (int h = 0; h < 2; h++)
+            x[k][u][h] = i0 + u >= p.nr ? 0.0f  // 0 off the detector and in the padding
+                                        : rebin_taps_sample(t[k][h], i0 + u, p.nch);
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
-      const int i = i0 + u;
-      if (i >= nrv) break;  // warp-uniform
-      const size_t row = (size_t)v * nrv + i;
-      float m = 0.0f;
+      for (int u = 0; u < 2; u++) {
+        const int i = i0 + u;
+        if (i >= nrv) break;  // warp-uniform
+        const size_t row = (size_t)v * nrv + i;
+        if (pass == 0) {
+          float m = 0.0f;
 #pragma unroll
-      for (int k = 0; k < NP; k++) {
-        if (!pv[k]) continue;
-        const int c0 = 2 * ((int)threadIdx.x + k * RS_THREADS);
-        const __nv_bfloat162 hi = __floats2bfloat162_rn(x[k][u][0], x[k][u][1]);
-        const float2 hf = __bfloat1622float2(hi);
-        const __nv_bfloat162 lo = __floats2bfloat162_rn(x[k][u][0] - hf.x, x[k][u][1] - hf.y);
-        *reinterpret_cast<__nv_bfloat162*>(a_hi + row * kp + c0) = hi;
-        *reinterpret_cast<__nv_bfloat162*>(a_lo + row * kp + c0) = lo;
-        // fmaxf semantics: a NaN sample does not raise the maximum
-        m = fmaxf(m, fmaxf(isnan(x[k][u][0]) ? 0.0f : fabsf(x[k][u][0]), isnan(x[k][u][1]) ? 0.0f : fabsf(x[k][u][1])));
+          for (int k = 0; k < NP; k++) {
+            if (!pv[k]) continue;
+            // fmaxf semantics: a NaN sample does not raise the maximum
+            m = fmaxf(m, fmaxf(isnan(x[k][u][0]) ? 0.0f : fabsf(x[k][u][0]),
+                               isnan(x[k][u][1]) ? 0.0f : fabsf(x[k][u][1])));
+          }
+          const unsigned mm = __reduce_max_sync(0xffffffffu, __float_as_uint(m));  // m >= 0: bits order as values
+          if (lane == 0 && mm) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)mm);
+        } else {
+#pragma unroll
+          for (int k = 0; k < NP; k++) {
+            if (!pv[k]) continue;
+            const int c0 = 2 * ((int)threadIdx.x + k * RS_THREADS);
+            const float y0 = x[k][u][0] * o, y1 = x[k][u][1] * o;  // o: a power of two, exact
+            const __half2 hi = __floats2half2_rn(y0, y1);
+            const float2 hf = __half22float2(hi);
+            const __half2 lo = __floats2half2_rn(y0 - hf.x, y1 - hf.y);
+            *reinterpret_cast<__half2*>(a_hi + row * kp + c0) = hi;
+            *reinterpret_cast<__half2*>(a_lo + row * kp + c0) = lo;
+          }
+        }
       }
-      const unsigned mm = __reduce_max_sync(0xffffffffu, __float_as_uint(m));  // m >= 0: bits order as values
-      if (lane == 0 && mm) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)mm);
     }
+    __syncthreads();
   }
-  __syncthreads();
-  __shared__ float s_vmax;
-  if (threadIdx.x == 0) s_vmax = 0.0f;
-  __syncthreads();
-  for (int i = threadIdx.x; i < nrv; i += blockDim.x) {
-    const float bound = fmaxf(s_rowmax[i] * taps_l1, 1e-30f) * (1.0f / 16384.0f);
-    const float sc = exp2f(ceilf(log2f(bound)));
-    row_scale[(size_t)v * nrv + i] = sc;
-    atomicMax(reinterpret_cast<int*>(&s_vmax), __float_as_int(sc));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) view_scale[v] = s_vmax;
 }
 
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
-                               const float* d_beta, const float* d_bidx, const double2* d_chan64,
+                               float* op_scale, const float* d_beta, const float* d_bidx, const double2* d_chan64,
                                const RebinParams& p, int kp, int nrv, float taps_l1, cudaStream_t s, int vb, int ve) {
   if (ve < 0) ve = p.V;
   if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
   const size_t rows = (size_t)p.V * nrv;
-  __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(planes);
-  __nv_bfloat16* lo = hi + rows * kp;
+  __half* hi = reinterpret_cast<__half*>(planes);
+  __half* lo = hi + rows * kp;
   if (kp % 64 != 0) return cudaErrorInvalidValue;  // whole warps per channel run (the row maxima's reduction)
   if (p.G == 1 && kp <= 4 * RS_THREADS)
     k_rebin_split_pairs<2><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
-        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
+        raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   else if (p.G == 1)
     k_rebin_split_rows<false><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
-        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
+        raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   else
     k_rebin_split_rows<true><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
-        raw, hi, lo, row_scale, view_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
+        raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// adaptive filtration of the raw readings
+// ---------------------------------------------------------------------------
+//
+// ReconConfig.adaptive_filtration_s, which fct_wfbp parses
+// (parse_config.cpp:57) but never applies, defined here as
+// attenuation-adaptive smoothing of the raw line integrals after Kachelriess,
+// Watzke and Kalender, Med. Phys. 28 (2001) 475-490: with p_max the largest
+// line integral of a reading and p_t = (1 - s) p_max (0 < s <= 1), each sample
+// p becomes p + w (pbar - p), pbar = (p[c-1] + 2 p[c] + p[c+1]) / 4 along its
+// detector row (edge channels repeated), w = clamp((p - p_t) / (p_max - p_t),
+// 0, 1). A reading with p_max <= 0 is copied unchanged. One CTA per reading:
+// the maximum by a block reduction, then the smoothing (the reading, a few
+// hundred KB, is read twice from L2).
+__global__ void __launch_bounds__(256)
+k_adaptive_filter(const float* __restrict__ raw, float* __restrict__ out, int nr, int nch, float s, long r0) {
+  __shared__ float s_max[8];
+  const size_t frame = (size_t)nr * nch;
+  const float* x = raw + (size_t)(r0 + blockIdx.x) * frame;
+  float* y = out + (size_t)(r0 + blockIdx.x) * frame;
+  float m = -INFINITY;
+  for (size_t k = threadIdx.x; k < frame; k += blockDim.x) m = fmaxf(m, __ldg(x + k));  // NaN ignored
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (threadIdx.x % 32 == 0) s_max[threadIdx.x / 32] = m;
+  __syncthreads();
+  float pmax = s_max[0];
+  for (int w = 1; w < (int)(blockDim.x / 32); w++) pmax = fmaxf(pmax, s_max[w]);
+  if (!(pmax > 0.0f)) {
+    for (size_t k = threadIdx.x; k < frame; k += blockDim.x) y[k] = __ldg(x + k);
+    return;
+  }
+  const float pt = (1.0f - s) * pmax;
+  const float inv = 1.0f / (pmax - pt);
+  for (size_t k = threadIdx.x; k < frame; k += blockDim.x) {
+    const int c = (int)(k % (size_t)nch);
+    const float p = __ldg(x + k);
+    const float a = __ldg(x + k - (c > 0 ? 1 : 0)), b = __ldg(x + k + (c < nch - 1 ? 1 : 0));
+    const float pb = 0.25f * (a + 2.0f * p + b);
+    const float w = __saturatef((p - pt) * inv);
+    y[k] = fmaf(w, pb - p, p);
+  }
+}
+
+cudaError_t launch_adaptive_filter(const float* raw, float* out, int nr, int nch, float s, long r0, long r1,
+                                   cudaStream_t st) {
+  if (r1 <= r0) return cudaSuccess;
+  if (!(s > 0.0f) || s > 1.0f) return cudaErrorInvalidValue;
+  k_adaptive_filter<<<(unsigned)(r1 - r0), 256, 0, st>>>(raw, out, nr, nch, s, r0);
+  return cudaGetLastError();
+}
+

@@ -131,19 +131,6 @@ int make_taps(const CTGeometry* cg, int window, float c, float a, const float* u
   return WFBP_OK;
 }
 
-uint16_t bf16_rn(float f) {
-  uint32_t u;
-  memcpy(&u, &f, 4);
-  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
-  u += 0x7fffu + ((u >> 16) & 1u);
-  return (uint16_t)(u >> 16);
-}
-float bf16_to_f(uint16_t b) {
-  uint32_t u = (uint32_t)b << 16;
-  float f;
-  memcpy(&f, &u, 4);
-  return f;
-}
 
 void free_dev(void*& p) {
   if (p) cudaFree(p);
@@ -203,6 +190,7 @@ void release(wfbp_ctx* ctx) {
   free_dev(ctx->s_vol_native);
   free_dev(ctx->s_raw);
   free_dev(ctx->s_vol);
+  free_dev(ctx->s_af);
   cudaSetDevice(prev);
 }
 
@@ -245,8 +233,9 @@ BPParams bp_params(const wfbp_ctx* ctx) {
 }
 
 // Stage buffer sizes for a filtered-row layout.
-//   rebinned: FP32 [V][nr][nch], or (mixed) BF16 planes [2][V*nrv][kp], row
-//             scales [V*nrv] and view scales [V], each 256-byte aligned
+//   rebinned: FP32 [V][nr][nch], or (mixed) FP16 operand planes
+//             [2][V*nrv][kp], row scales [V*nrv], view scales [V] and the
+//             views' operand scales [V], each 256-byte aligned
 //   filtered: reference layout [V][nr][nch] FP32/FP16, or backprojection
 //             layout [V][nch][nrp] of 4-byte elements (FP32 or half2 pairs)
 //   scales:   FP32 [V][nr] row scales (mixed, reference layout) or [V] view
@@ -260,7 +249,7 @@ void stage_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, siz
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
     const size_t rows = (size_t)ctx->V * ctx->nrv;
     *reb = al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t)) + al256(rows * sizeof(float)) +
-           (size_t)ctx->V * sizeof(float);
+           al256((size_t)ctx->V * sizeof(float)) + (size_t)ctx->V * sizeof(float);
     *filt = bpl ? bpl_bytes : sizeof(uint16_t) * samples;
     *scal = bpl ? (size_t)ctx->V * sizeof(float) : (size_t)ctx->V * ctx->nr * sizeof(float);
   } else {
@@ -271,12 +260,14 @@ void stage_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, siz
 }
 
 template <class P>
-void mixed_scale_ptrs(const wfbp_ctx* ctx, P rebinned, float** row_sc, float** view_sc) {
+void mixed_scale_ptrs(const wfbp_ctx* ctx, P rebinned, float** row_sc, float** view_sc, float** op_sc) {
   const size_t rows = (size_t)ctx->V * ctx->nrv;
   uint8_t* b = const_cast<uint8_t*>(reinterpret_cast<const uint8_t*>(rebinned));
-  *row_sc = reinterpret_cast<float*>(b + al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t)));
-  *view_sc = reinterpret_cast<float*>(b + al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t)) +
-                                      al256(rows * sizeof(float)));
+  const size_t o_row = al256(2 * rows * (size_t)ctx->tc_kp * sizeof(uint16_t));
+  const size_t o_view = o_row + al256(rows * sizeof(float));
+  *row_sc = reinterpret_cast<float*>(b + o_row);
+  *view_sc = reinterpret_cast<float*>(b + o_view);
+  *op_sc = reinterpret_cast<float*>(b + o_view + al256((size_t)ctx->V * sizeof(float)));
 }
 
 // Sizes the TMA-staged backprojection for this geometry: the column tile, the
@@ -604,7 +595,8 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
       !(rp->recon_fov > 0) || !(rp->slice_thickness > 0) || !(cg->distance_source_to_isocenter > 0) ||
       !(cg->distance_source_to_detector > 0) || !(cg->detector_pixel_size_col > 0) ||
       !(cg->collimated_slice_width > 0) || cg->num_detector_cols > 8192 || cg->num_detector_rows > 1024 ||
-      cg->total_number_of_projections > (1u << 24) || rp->nx > 8192 || rp->ny > 8192)
+      cg->total_number_of_projections > (1u << 24) || rp->nx > 8192 || rp->ny > 8192 ||
+      std::isnan(rp->adaptive_filtration_s))
     return WFBP_ERR_INVALID_ARG;
 
   wfbp_ctx* ctx = new (std::nothrow) wfbp_ctx();
@@ -667,10 +659,17 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
   if (!ce) ce = alloc_copy((void**)&ctx->d_view_z64, nullptr, sizeof(double) * ctx->V);
   if (!ce) ce = alloc_copy((void**)&ctx->d_view_z, nullptr, sizeof(float) * ctx->V);
   if (!ce) ce = alloc_copy((void**)&ctx->d_err, nullptr, sizeof(int));
+  // adaptive filtration (ReconConfig.adaptive_filtration_s > 0): the filtered
+  // readings live in context memory allocated here, so no stage call allocates
+  ctx->af_s = rp->adaptive_filtration_s > 0.0f ? std::min(rp->adaptive_filtration_s, 1.0f) : 0.0f;
+  if (!ce && ctx->af_s > 0.0f)
+    ce = alloc_copy((void**)&ctx->s_af, nullptr,
+                    sizeof(float) * (size_t)ctx->n_readings * ctx->raw_rows * ctx->raw_ch);
   if (!ce) ce = cudaMemset(ctx->d_err, 0, sizeof(int));
   if (!ce && e.precision == WFBP_PRECISION_MIXED) {
-    // Toeplitz operand T[n][k] = h[|n - k|], split into BF16 hi/lo planes,
-    // zero-padded to [np][kp]
+    // Toeplitz operand T[n][k] = h[|n - k|] scaled by the power of two
+    // tap_scale (the largest with tap_scale max|h| <= 16384), split into FP16
+    // hi / lo planes (22 bits), zero-padded to [np][kp]
     const int nch = ctx->nch;
     ctx->tc_kp = (nch + 63) / 64 * 64;
     ctx->nrv = 1;
@@ -679,15 +678,20 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     ctx->tc_np = (nch + ctx->tc_bn - 1) / ctx->tc_bn * ctx->tc_bn;
     const size_t plane = (size_t)ctx->tc_np * ctx->tc_kp;
     std::vector<uint16_t> b(2 * plane, 0);
-    double l1 = 0.0;
-    for (int d = 0; d < nch; d++) l1 += (d ? 2.0 : 1.0) * fabs((double)ctx->taps[d]);
+    double l1 = 0.0, hmax = 0.0;
+    for (int d = 0; d < nch; d++) {
+      l1 += (d ? 2.0 : 1.0) * fabs((double)ctx->taps[d]);
+      hmax = std::max(hmax, fabs((double)ctx->taps[d]));
+    }
     ctx->taps_l1 = (float)l1;
+    ctx->tap_scale = hmax > 0.0 ? (float)exp2(floor(log2(16384.0 / hmax))) : 1.0f;
     for (int n = 0; n < nch; n++)
       for (int k = 0; k < nch; k++) {
-        float h = ctx->taps[n > k ? n - k : k - n];
-        uint16_t hi = bf16_rn(h);
-        b[(size_t)n * ctx->tc_kp + k] = hi;
-        b[plane + (size_t)n * ctx->tc_kp + k] = bf16_rn(h - bf16_to_f(hi));
+        const float h = ctx->taps[n > k ? n - k : k - n] * ctx->tap_scale;  // power of two: exact
+        const __half hi = __float2half_rn(h);
+        const __half lo = __float2half_rn(h - __half2float(hi));
+        b[(size_t)n * ctx->tc_kp + k] = __half_as_ushort(hi);
+        b[plane + (size_t)n * ctx->tc_kp + k] = __half_as_ushort(lo);
       }
     ce = alloc_copy(&ctx->d_bplanes, b.data(), sizeof(uint16_t) * b.size());
     // FP64 sample coordinates of the mixed form's rebin (rebin_kernel,
@@ -935,9 +939,9 @@ namespace {
 int do_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, int vb, int ve, void* stream) {
   const RebinParams p = rebin_params(ctx);
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
-    float *row_sc, *view_sc;
-    mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
-    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, row_sc, view_sc, ctx->d_chan_beta, ctx->d_chan_bidx,
+    float *row_sc, *view_sc, *op_sc;
+    mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc, &op_sc);
+    CUDA_TRY(ctx, launch_rebin_split(raw, rebinned, row_sc, view_sc, op_sc, ctx->d_chan_beta, ctx->d_chan_bidx,
                                      ctx->ext.tex_weights ? nullptr : ctx->d_chan64, p,
                                      ctx->tc_kp, ctx->nrv, ctx->taps_l1, (cudaStream_t)stream, vb, ve));
   } else {
@@ -948,10 +952,25 @@ int do_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, int vb, int ve, vo
 }
 }  // namespace
 
+namespace {
+// Adaptive filtration of readings [r0, r1) of `raw` into the context's
+// filtered readings (context memory, allocated at creation).
+int adaptive_filter(wfbp_ctx* ctx, const float* raw, long r0, long r1, void* stream) {
+  CUDA_TRY(ctx, launch_adaptive_filter(raw, ctx->s_af, ctx->raw_rows, ctx->raw_ch, ctx->af_s, r0, r1,
+                                       (cudaStream_t)stream));
+  return WFBP_OK;
+}
+}  // namespace
+
 WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream) {
   if (!ctx) return WFBP_ERR_INVALID_ARG;
   if (!raw || !rebinned) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_rebin: null buffer");
   DeviceGuard g(ctx->device);
+  if (ctx->af_s > 0.0f) {
+    const int st = adaptive_filter(ctx, raw, 0, ctx->n_readings, stream);
+    if (st) return st;
+    raw = ctx->s_af;
+  }
   return do_rebin(ctx, raw, rebinned, 0, ctx->V, stream);
 }
 
@@ -966,8 +985,8 @@ int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales
     return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_filter: no backprojection-layout launch fits this geometry");
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
     if (!scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: mixed precision needs scales");
-    float *row_sc, *view_sc;
-    mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc);
+    float *row_sc, *view_sc, *op_sc;
+    mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc, &op_sc);
     TcOutArgs o;
     memset(&o, 0, sizeof(o));
     o.nr = ctx->nr;
@@ -975,6 +994,8 @@ int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales
     o.nrp = ctx->bpt.nrp;
     o.row_scale_in = row_sc;
     o.view_scale = view_sc;
+    o.op_scale = op_sc;
+    o.tap_scale = ctx->tap_scale;
     if (bpl) {
       o.mode = TC_OUT_PAIRS;
       o.pairs = static_cast<uint32_t*>(filtered);
@@ -1149,6 +1170,7 @@ WFBP_API int wfbp_rebin_adjoint(wfbp_ctx* ctx, const float* g_rebinned, float* g
   int st = require_fp32_views(ctx, "wfbp_rebin_adjoint");
   if (st) return st;
   if (ctx->G != 1) return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_rebin_adjoint: flying focal spot scans");
+  if (ctx->af_s > 0.0f) return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_rebin_adjoint: adaptive filtration");
   DeviceGuard g(ctx->device);
   constexpr int kMaxL = 8;
   if (!ctx->d_radj_cnt) {
@@ -1170,6 +1192,7 @@ WFBP_API int wfbp_taps_gradient(wfbp_ctx* ctx, const float* raw, const float* g_
   if (n < 1 || n > ctx->nch) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_taps_gradient: need 1 <= n <= channels");
   int st = require_fp32_views(ctx, "wfbp_taps_gradient");
   if (st) return st;
+  if (ctx->af_s > 0.0f) return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_taps_gradient: adaptive filtration");
   DeviceGuard g(ctx->device);
   const RebinParams p = rebin_params(ctx);
   const size_t need = (size_t)taps_grad_blocks(p) * n;
@@ -1488,12 +1511,20 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
     }
     return WFBP_OK;
   };
+  long af_upto = 0;  // readings adaptively filtered so far
   for (int c = 0; c < nchunk; c++) {
     const int vb = c * cv, ve = std::min(V, (c + 1) * cv);
     const int last = std::min(nchunk - 1, (std::min(V, ve + reach) - 1) / cv);
     if ((st = issue_copies(last))) return st;
     CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->ev_copy[last], 0));
-    if ((st = do_rebin(ctx, ctx->s_raw, ctx->s_rebinned, vb, ve, s))) return st;
+    const float* rin = ctx->s_raw;
+    if (ctx->af_s > 0.0f) {  // the readings copied so far, once each
+      const long upto = std::min<long>(ctx->n_readings, (long)std::min(V, (last + 1) * cv) * G);
+      if ((st = adaptive_filter(ctx, ctx->s_raw, af_upto, upto, s))) return st;
+      af_upto = std::max(af_upto, upto);
+      rin = ctx->s_af;
+    }
+    if ((st = do_rebin(ctx, rin, ctx->s_rebinned, vb, ve, s))) return st;
     if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, s, vb, ve))) return st;
     if ((st = launch_ready(ve))) return st;
   }

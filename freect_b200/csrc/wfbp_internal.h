@@ -158,7 +158,8 @@ struct wfbp_ctx {
   int tc_kp = 0, tc_np = 0, tc_bn = 0;
   int nrv = 0;                      // rows per view in the operand planes (power of two >= nr)
   float taps_l1 = 0.0f;             // sum over |d| < nch of |h[d]|
-  void* d_bplanes = nullptr;        // bf16 [2][tc_np][tc_kp]
+  float tap_scale = 1.0f;           // power of two applied to the taps in d_bplanes
+  void* d_bplanes = nullptr;        // FP16 [2][tc_np][tc_kp] (hi, lo of tap_scale * T)
   int* d_err = nullptr;             // device-side error word (bounded waits)
 
   // TMA-staged backprojection (backprojection layout [V][nch][nrp])
@@ -176,6 +177,8 @@ struct wfbp_ctx {
   float* s_vol = nullptr;
   cudaStream_t s_copy = nullptr;    // wfbp_run_host: host-to-device copies of the reading chunks
   cudaStream_t s_back = nullptr;    // wfbp_run_host: device-to-host copies of finished slices
+  float af_s = 0.0f;                // adaptive filtration strength (ReconConfig.adaptive_filtration_s, <= 1; 0: off)
+  float* s_af = nullptr;            // adaptively filtered readings [n_readings][raw_rows][raw_ch] (af_s > 0)
   cudaStream_t s_bp[2] = {nullptr, nullptr};  // wfbp_run_host: backprojection launches (alternating)
   std::vector<cudaEvent_t> ev_copy; // one per chunk, plus the caller-stream fence
 
@@ -200,7 +203,7 @@ cudaError_t launch_backproject_f16(const __half* D, const float* scales, float* 
                                    const float* vz, const float* zs, const BPParams& p, unsigned long long* count,
                                    cudaStream_t s);
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
-                               const float* d_beta, const float* d_bidx, const double2* d_chan64,
+                               float* op_scale, const float* d_beta, const float* d_bidx, const double2* d_chan64,
                                const RebinParams& p, int kp, int nrv, float taps_l1, cudaStream_t s, int vb = 0,
                                int ve = -1);
 // Output modes of the tensor-core filter epilogue.
@@ -214,6 +217,8 @@ struct TcOutArgs {
   const float* row_scale_in;    // [V*nrv]
   float* row_scale_out;         // [V][nr]
   const float* view_scale;      // [V]
+  const float* op_scale;        // [V] power-of-two scale of the view's FP16 operand rows
+  float tap_scale;              // power-of-two scale of the FP16 Toeplitz operand
 };
 cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
                              const TcOutArgs& out, int* err, cudaStream_t s, int mb = 0, int me = -1);
@@ -281,6 +286,8 @@ int taps_grad_blocks(const RebinParams& p);
 cudaError_t launch_selftest_wait(int* err, unsigned long long limit_ns, cudaStream_t s);
 cudaError_t launch_taps_gradient(const float* raw, const float* gY, const float* beta, const float* bidx,
                                  const RebinParams& p, int ntaps, float* partial, float* out, cudaStream_t s);
+cudaError_t launch_adaptive_filter(const float* raw, float* out, int nr, int nch, float s, long r0, long r1,
+                                   cudaStream_t st);
 cudaError_t launch_synth(const wfbp_synth_scan& scan, const wfbp_ellipsoid* d_e, int ne, float* out,
                          cudaStream_t s);
 

@@ -141,10 +141,10 @@ enum wfbp_status {
 
 enum wfbp_precision {
   WFBP_PRECISION_FP32 = 0,    /* FP32 rebin, FP32 SIMT Toeplitz filter, FP32 rows, FP32 backprojection */
-  WFBP_PRECISION_MIXED = 1    /* rebin with FP64 sample coordinates into split hi+lo BF16 planes,
-                                 tcgen05 filter (FP32 accumulate in TMEM), FP16 filtered rows with
-                                 power-of-two scales, backprojection with FP64 per-view geometry
-                                 and FP32 accumulation */
+  WFBP_PRECISION_MIXED = 1    /* rebin with FP64 sample coordinates into split hi+lo FP16 operand
+                                 planes, tcgen05 filter (FP32 accumulate in TMEM), FP16 filtered
+                                 rows with power-of-two scales, backprojection with FP64 per-view
+                                 geometry and FP32 accumulation */
 };
 
 enum wfbp_filter_window {
@@ -220,7 +220,7 @@ typedef struct wfbp_dims {
   int n_slices_requested;
   int precision;
   size_t raw_bytes;           /* float [n_readings][raw_rows][raw_channels] */
-  size_t rebinned_bytes;      /* stage-1 output (FP32 [V][nr][nch], or the split BF16 operand planes) */
+  size_t rebinned_bytes;      /* stage-1 output (FP32 [V][nr][nch], or the split FP16 operand planes) */
   size_t filtered_bytes;      /* stage-2 output (FP32 or FP16 [V][nr][nch]) */
   size_t row_scale_bytes;     /* FP32 scales: [V][nr] (MIXED, REFERENCE layout) or [V]
                                  (MIXED, BACKPROJECTION layout), else 0 */
@@ -270,7 +270,17 @@ int wfbp_filter_taps(const CTGeometry* cg, int window, float c, float a, float* 
  * Replaces the state the reference keeps in ReconstructionMachine
  * (ReconstructionMachine.h:30-48) plus its __constant__ copies
  * (cuda_kernels.cuh:5-7). `ext` may be NULL (FP32; the filter of rp->recon_kernel,
- * wfbp_recon_kernel). */
+ * wfbp_recon_kernel).
+ * rp->adaptive_filtration_s, which fct_wfbp parses (parse_config.cpp:57) but
+ * never applies, turns on adaptive filtration of the raw readings before the
+ * rebin when > 0 (values above 1 act as 1): with p_max the largest line
+ * integral of a reading and p_t = (1 - s) p_max, each sample p becomes
+ * p + w (pbar - p), pbar = (p[c-1] + 2 p[c] + p[c+1]) / 4 along its detector
+ * row (edge channels repeated), w = clamp((p - p_t) / (p_max - p_t), 0, 1):
+ * attenuation-adaptive smoothing after Kachelriess, Watzke and Kalender,
+ * Med. Phys. 28 (2001) 475-490. The filtered readings live in context memory
+ * (the raw frames' size, allocated here); the rebin adjoint and the tap
+ * gradient refuse such a context (WFBP_ERR_UNSUPPORTED). */
 int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const wfbp_ext* ext,
                     int device, wfbp_ctx** out);
 int wfbp_ctx_destroy(wfbp_ctx* ctx);
@@ -356,7 +366,8 @@ const char* wfbp_status_string(int status);
  * rebin_kernel, cuda_kernels.cuh:11-39): host reshape/flip + rebin of every
  * row in one launch. raw: FP32 [n_readings][raw_rows][raw_channels].
  * rebinned: FP32 [V][nr][nch] (row index = flipped row sheet index), or for
- * WFBP_PRECISION_MIXED the split BF16 operand planes of the filter. */
+ * WFBP_PRECISION_MIXED the split FP16 operand planes of the filter with
+ * their scales. */
 int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream);
 
 /* Stage 2 of RebinAndFilter (ReconstructionMachine.cu:262-290: R2C,

@@ -61,6 +61,7 @@ def load():
             "orc_backproject_adjoint_f64": (None, [G, R, _D, _D, _D, _D, C.c_int, _D]),
             "orc_taps_gradient_f64": (None, [C.c_int, C.c_long, _D, _D, C.c_int, _D]),
             "orc_rebin_adjoint_f64": (None, [G, _D, _D]),
+            "orc_adaptive_filter_f64": (None, [_F, C.c_long, C.c_int, C.c_int, C.c_double, _D]),
         }
         for name, (res, args) in protos.items():
             f = getattr(lib, name)
@@ -145,6 +146,15 @@ def rebin_ref32(cg, raw, q8=False):
     out = np.zeros((V, nr, nch), np.float32)
     r = _f(raw)
     load().orc_rebin_ref32(C.byref(cg), fp(r), int(bool(q8)), fp(out))
+    return out
+
+
+def adaptive_filter_f64(raw, s):
+    """Adaptive filtration of raw readings [n][rows][channels] with strength
+    s (ReconConfig.adaptive_filtration_s), FP64 (wfbp_oracle.c)."""
+    r = _f(raw)
+    out = np.zeros(r.shape, np.float64)
+    load().orc_adaptive_filter_f64(fp(r), r.shape[0], r.shape[1], r.shape[2], float(s), dp(out))
     return out
 
 

@@ -1189,3 +1189,50 @@ ORC_EXPORT void orc_rebin_adjoint_f64(const CTGeometry* cg, const double* g_rebi
   memset(g_raw, 0, sizeof(double) * cg->total_number_of_projections * cg->num_detector_rows * cg->num_detector_cols);
   orc_parallel_for((long)cg->num_detector_rows, 1, rba_body, &a);
 }
+
+/* ------------------------------------------------------------------------ */
+/* adaptive filtration of the raw readings (FP64)                            */
+/* ------------------------------------------------------------------------ */
+/* fct_wfbp parses ReconConfig.adaptive_filtration_s (parse_config.cpp:57)
+ * but never applies it (README: "Need to add adaptive filtration back into
+ * the toolbox"). The product defines it as attenuation-adaptive smoothing of
+ * the raw line integrals, after Kachelriess, Watzke and Kalender, Med. Phys.
+ * 28 (2001) 475-490: with s = min(s, 1) > 0 and p_max the largest line
+ * integral of a reading, each sample p of the reading becomes
+ * p + w (pbar - p), pbar = (p[c-1] + 2 p[c] + p[c+1]) / 4 along its detector
+ * row (edge channels repeated), w = clamp((p - p_t) / (p_max - p_t), 0, 1),
+ * p_t = (1 - s) p_max: the most attenuated (photon-starved) rays are
+ * smoothed most, rays below p_t pass unchanged. s <= 0, or a reading with
+ * p_max <= 0, leaves the samples unchanged. This is the FP64 statement of
+ * that definition; out: [readings][rows][channels]. */
+typedef struct { const float* raw; int nr, nch; double s; double* out; } af_args;
+static void af_body(void* a_, long i0, long i1) {
+  af_args* a = (af_args*)a_;
+  const long fr = (long)a->nr * a->nch;
+  const double s = a->s < 1.0 ? a->s : 1.0;
+  for (long n = i0; n < i1; n++) {
+    const float* x = a->raw + n * fr;
+    double* y = a->out + n * fr;
+    double pmax = -INFINITY;
+    for (long k = 0; k < fr; k++)
+      if (x[k] > pmax) pmax = x[k];
+    if (!(s > 0.0) || !(pmax > 0.0)) {
+      for (long k = 0; k < fr; k++) y[k] = x[k];
+      continue;
+    }
+    const double pt = (1.0 - s) * pmax;
+    for (int r = 0; r < a->nr; r++)
+      for (int c = 0; c < a->nch; c++) {
+        const float* row = x + (long)r * a->nch;
+        const double p = row[c];
+        const double pb = 0.25 * ((double)row[c > 0 ? c - 1 : 0] + 2.0 * p + (double)row[c < a->nch - 1 ? c + 1 : c]);
+        double w = (p - pt) / (pmax - pt);
+        w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+        y[(long)r * a->nch + c] = p + w * (pb - p);
+      }
+  }
+}
+ORC_EXPORT void orc_adaptive_filter_f64(const float* raw, long n_readings, int nr, int nch, double s, double* out) {
+  af_args a = {raw, nr, nch, s, out};
+  orc_parallel_for(n_readings, 4, af_body, &a);
+}

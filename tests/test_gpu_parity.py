@@ -469,3 +469,48 @@ def test_recon_kernel_from_yaml(orc, tmp_path, rk):
     ramlak = orc.reconstruct_ref32(spec, raw, q8=True)
     assert orc.hu_error(got, ramlak["volume"])[0] > 5.0 * max(rms, 0.01)
     ctx.close()
+
+
+def test_adaptive_filtration(orc):
+    # ReconConfig.adaptive_filtration_s > 0: the raw readings are smoothed
+    # (attenuation-adaptive, k_adaptive_filter) before the rebin. FP32 form
+    # against the reference transcript fed with the oracle's filtered readings;
+    # mixed form against the FP64 oracle on the same; the pipelined host path
+    # (filtration chunk by chunk as the readings arrive) equals wfbp_run; the
+    # adjoints refuse it
+    spec = scans.tiny(seed=23)
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    s = 0.35
+    raw_af = orc.adaptive_filter_f64(raw, s).astype(np.float32)
+    assert not np.array_equal(raw_af, raw)
+    tube, table = spec.views()
+    cg, gp = wfbp.configure_geometry(spec.meta(), table)
+    rp = spec.recon_config()
+    rp.adaptive_filtration_s = s
+    ctx = wfbp.Context(cg, rp, wfbp.make_ext(tex_weights=1), device=0)
+    ctx.set_views(tube, table)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    got = vol.cpu().numpy()
+    ref = orc.reconstruct_ref32(spec, raw_af, q8=True)
+    rms, mx, n = orc.hu_error(got, ref["volume"])
+    assert n == got.size and rms <= 0.5 and mx <= 2.0, (rms, mx)
+    plain = orc.reconstruct_ref32(spec, raw, q8=True)
+    assert orc.hu_error(got, plain["volume"])[0] > 5.0 * max(rms, 0.01)  # the filtration took effect
+    vh = np.zeros_like(got)
+    ctx.run_host(raw, vh)
+    assert np.array_equal(vh, got)
+    g = ctx.alloc("rebinned")
+    with pytest.raises(wfbp.WfbpError):
+        ctx.rebin_adjoint(g, ctx.alloc("raw"))
+    ctx.close()
+    ctx = wfbp.Context(cg, rp, wfbp.make_ext(precision=T.PRECISION_MIXED), device=0)
+    ctx.set_views(tube, table)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    r64 = orc.reconstruct_f64(spec, raw_af)
+    rms, mx, n = orc.hu_error(vol.cpu().numpy(), r64["volume"])
+    assert n == np.isfinite(r64["volume"]).sum() and rms <= 1.0, (rms, mx)
+    ctx.close()

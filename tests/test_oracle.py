@@ -180,3 +180,31 @@ def test_nan_where_no_half_turn_contributes(orc):
     v64, n = orc.backproject_f64(cg, rp, filt.astype(np.float64), tube.astype(np.float64),
                                  table.astype(np.float64), np.array([500.0]))
     assert n == 0 and np.isnan(v64).sum() == np.isnan(v).sum()
+
+
+def test_adaptive_filter_oracle(orc):
+    # ReconConfig.adaptive_filtration_s (parsed, never applied by fct_wfbp):
+    # attenuation-adaptive smoothing of the raw line integrals, restated here
+    # in numpy from its definition and checked against the C oracle
+    rng = np.random.default_rng(3)
+    raw = rng.uniform(0.0, 6.0, (5, 3, 17)).astype(np.float32)
+    raw[2] = 1.5  # a uniform reading: smoothing changes nothing
+    raw[3] = -rng.uniform(0.0, 1.0, (3, 17))  # no attenuation: p_max <= 0, unchanged
+    s = 0.4
+    got = orc.adaptive_filter_f64(raw, s)
+    x = raw.astype(np.float64)
+    pmax = x.reshape(5, -1).max(1)[:, None, None]
+    pt = (1.0 - s) * pmax
+    left = np.concatenate([x[..., :1], x[..., :-1]], -1)
+    right = np.concatenate([x[..., 1:], x[..., -1:]], -1)
+    pb = 0.25 * (left + 2.0 * x + right)
+    w = np.clip((x - pt) / (pmax - pt), 0.0, 1.0)
+    ref = np.where(pmax > 0, x + w * (pb - x), x)
+    assert np.allclose(got, ref, rtol=1e-14, atol=1e-14)
+    assert np.array_equal(got[2], x[2]) and np.array_equal(got[3], x[3])
+    # below the threshold nothing changes; the reading's maximum is fully smoothed
+    assert np.array_equal(got[x < pt], x[x < pt])
+    r, c = np.unravel_index(np.argmax(x[0]), x[0].shape)
+    assert abs(got[0, r, c] - pb[0, r, c]) < 1e-12
+    # s = 0 is the reference's behaviour (off)
+    assert np.array_equal(orc.adaptive_filter_f64(raw, 0.0), x)
