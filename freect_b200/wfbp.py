@@ -27,6 +27,9 @@ _PROTOS = {
                                        C.POINTER(C.c_int)]),
     "wfbp_filter_taps": (C.c_int, [C.POINTER(T.CTGeometry), C.c_int, C.c_float, C.c_float, C.POINTER(C.c_float),
                                    C.c_int]),
+    "wfbp_dicom_read_meta": (C.c_int, [C.c_char_p, C.POINTER(T.ScanMeta)]),
+    "wfbp_dicom_read_frames": (C.c_int, [C.c_char_p, C.POINTER(T.ScanMeta), C.c_int, C.c_int, C.POINTER(C.c_float),
+                                         C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "wfbp_recon_kernel_filter": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float),
                                            C.POINTER(C.c_float)]),
     "wfbp_ctx_create": (C.c_int, [C.POINTER(T.CTGeometry), C.POINTER(T.ReconConfig), C.POINTER(T.Ext), C.c_int,
@@ -434,6 +437,25 @@ def read_frames(directory, meta, first=0, count=None, out=None):
                                    tube.ctypes.data_as(_VP), table.ctypes.data_as(_VP), C.c_void_p(ptr)),
            "wfbp_read_frames " + str(directory))
     return tube, table, out
+
+
+def dicom_read_meta(directory):
+    """Scan metadata of a DICOM-CT-PD directory (wfbp_dicom_read_meta)."""
+    m = T.ScanMeta()
+    _check(load().wfbp_dicom_read_meta(directory.encode(), C.byref(m)), "wfbp_dicom_read_meta")
+    return m
+
+
+def dicom_read_frames(directory, meta, first=0, count=None):
+    """Readings [first, first + count) of a DICOM-CT-PD directory:
+    (tube angles, table positions, raw [count][rows][channels])."""
+    count = meta.total_num_projections - first if count is None else count
+    raw = np.zeros((count, meta.detector_rows, meta.detector_channels), np.float32)
+    ang = np.zeros(count, np.float32)
+    z = np.zeros(count, np.float32)
+    _check(load().wfbp_dicom_read_frames(directory.encode(), C.byref(meta), first, count, _fptr(ang)[1], _fptr(z)[1],
+                                         _fptr(raw)[1]), "wfbp_dicom_read_frames")
+    return ang, z, raw
 
 
 def write_scan(directory, meta, tube_angles, table_positions, raw):

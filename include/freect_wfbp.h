@@ -535,6 +535,26 @@ int wfbp_read_frames(const char* dir, const wfbp_scan_meta* meta, int first, int
 int wfbp_write_scan(const char* dir, const wfbp_scan_meta* meta, const float* tube_angles,
                     const float* table_positions, const float* raw);
 
+/* DICOM-CT-PD projection data, one reading per file (the TCIA LDCT format),
+ * as fct_read's DicomDataSet reads it with DCMTK
+ * (modules/fct_read/src/DicomDataSet.cpp): the directory's regular files in
+ * name order (:156-162); wfbp_dicom_read_meta fills the scan metadata from the
+ * first file (readMetadata, :232-316: detector rows (7029,1010), channels
+ * (7029,1011), transverse / axial spacing (7029,1002) / (7029,1006), source to
+ * isocentre (7031,1003) and to detector (7031,1031), readings per rotation
+ * (7033,1013), central channel and row (7031,1033), flying-focal-spot mode
+ * (7033,100E)); wfbp_dicom_read_frames reads readings [first, first+count):
+ * tube angle (7031,1001), table position (7031,1002) and the uint16 pixel
+ * data times the rescale slope plus intercept ((0028,1053), (0028,1052)) as
+ * float [count][rows][channels], from a [rows][channels] or a
+ * [channels][rows] image (DicomFrame::readFromFile, :56-155).
+ * tube_angles / table_positions may be NULL. Implicit and explicit VR little
+ * endian only; WFBP_ERR_INVALID_ARG for a missing element, another transfer
+ * syntax or a size that does not match. Host only. */
+int wfbp_dicom_read_meta(const char* dir, wfbp_scan_meta* meta);
+int wfbp_dicom_read_frames(const char* dir, const wfbp_scan_meta* meta, int first, int count, float* tube_angles,
+                           float* table_positions, float* raw);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic scans (test-data generator; no counterpart in the reference)    */
 /* ------------------------------------------------------------------------ */

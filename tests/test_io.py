@@ -83,3 +83,111 @@ def test_recon_kernel_rejects_unknown_values():
     for rk in (-1, 4, 100):
         with pytest.raises(wfbp.WfbpError):
             wfbp.recon_kernel_filter(rk)
+
+
+# ---------------------------------------------------------------------------
+# DICOM-CT-PD: files written here by an encoder of the test's own (DICOM Part
+# 10 element encoding: tag, VR, length, value; little endian), read back
+# through the C ABI
+# ---------------------------------------------------------------------------
+import struct
+
+_LONG = {"OB", "OW", "OF", "SQ", "UT", "UN"}
+
+
+def _el(tag, vr, value, explicit):
+    g, e = tag >> 16, tag & 0xFFFF
+    if len(value) % 2:
+        value += b" " if vr in ("CS", "LO", "DS", "UI", "IS") else b"\0"
+    if not explicit:
+        return struct.pack("<HHI", g, e, len(value)) + value
+    if vr in _LONG:
+        return struct.pack("<HH2sHI", g, e, vr.encode(), 0, len(value)) + value
+    return struct.pack("<HH2sH", g, e, vr.encode(), len(value)) + value
+
+
+def _dicom_file(path, elems, explicit=True, with_sequence=False):
+    ts = b"1.2.840.10008.1.2.1" if explicit else b"1.2.840.10008.1.2"
+    meta = _el(0x00020010, "UI", ts + b"\0", True)
+    body = b""
+    if with_sequence:  # an undefined-length sequence the reader must skip
+        item = _el(0x00081150, "UI", b"1.2.3\0", explicit)
+        seq_hdr = struct.pack("<HH2sHI", 0x0008, 0x1140, b"SQ", 0, 0xFFFFFFFF) if explicit else \
+            struct.pack("<HHI", 0x0008, 0x1140, 0xFFFFFFFF)
+        body += seq_hdr + struct.pack("<HHI", 0xFFFE, 0xE000, 0xFFFFFFFF) + item + \
+            struct.pack("<HHI", 0xFFFE, 0xE00D, 0) + struct.pack("<HHI", 0xFFFE, 0xE0DD, 0)
+    for tag, vr, val in sorted(elems, key=lambda t: t[0]):
+        body += _el(tag, vr, val, explicit)
+    with open(path, "wb") as f:
+        f.write(b"\0" * 128 + b"DICM" + meta + body)
+
+
+def _write_ctpd(d, raw, angles, zs, explicit, transpose, ffs="FFSNONE"):
+    n, nr, nch = raw.shape
+    slope, icpt = 0.5, -1024.0
+    for k in range(n):
+        counts = np.round((raw[k] - icpt) / slope).astype(np.uint16)
+        img = counts.T if transpose else counts  # [channels][rows] or [rows][channels]
+        elems = [
+            (0x00080070, "LO", b"SYNTH"),
+            (0x00280010, "US", struct.pack("<H", img.shape[0])),
+            (0x00280011, "US", struct.pack("<H", img.shape[1])),
+            (0x00281052, "DS", b"%g" % icpt),
+            (0x00281053, "DS", b"%g" % slope),
+            (0x70291010, "US", struct.pack("<H", nr)),
+            (0x70291011, "US", struct.pack("<H", nch)),
+            (0x70291002, "FL", struct.pack("<f", 1.2858)),
+            (0x70291006, "FL", struct.pack("<f", 1.0947)),
+            (0x7029100B, "CS", b"CYLINDRICAL"),
+            (0x70311001, "FL", struct.pack("<f", angles[k])),
+            (0x70311002, "FL", struct.pack("<f", zs[k])),
+            (0x70311003, "FL", struct.pack("<f", 595.0)),
+            (0x70311031, "FL", struct.pack("<f", 1085.6)),
+            (0x70311033, "FL", struct.pack("<ff", 366.25, 15.5)),
+            (0x7033100B, "FL", struct.pack("<f", 0.0)),
+            (0x7033100C, "FL", struct.pack("<f", 0.0)),
+            (0x7033100D, "FL", struct.pack("<f", 0.0)),
+            (0x7033100E, "CS", ffs.encode()),
+            (0x70331013, "US", struct.pack("<H", 1152)),
+            (0x70371009, "CS", b"AXIAL"),
+            (0x7037100A, "CS", b"FANBEAM"),
+            (0x7FE00010, "OW", np.ascontiguousarray(img).astype("<u2").tobytes()),
+        ]
+        _dicom_file(str(d / ("proj_%05d.dcm" % k)), elems, explicit, with_sequence=(k == 0))
+    return slope, icpt
+
+
+@pytest.mark.parametrize("explicit,transpose", [(True, False), (False, True), (True, True)])
+def test_dicom_ctpd_reader(tmp_path, explicit, transpose):
+    rng = np.random.default_rng(7)
+    n, nr, nch = 5, 4, 12
+    slope, icpt = 0.5, -1024.0
+    counts = rng.integers(0, 4000, (n, nr, nch))
+    raw = (counts * slope + icpt).astype(np.float32)
+    angles = rng.uniform(-3, 3, n).astype(np.float32)
+    zs = rng.uniform(-50, 50, n).astype(np.float32)
+    _write_ctpd(tmp_path, raw, angles, zs, explicit, transpose, ffs="FFSXYZ")
+    m = wfbp.dicom_read_meta(str(tmp_path))
+    assert (m.total_num_projections, m.detector_rows, m.detector_channels, m.projections_per_rotation) == (n, nr, nch, 1152)
+    assert m.ffs_mode == T.FFS_PHIZ
+    assert np.float32(m.detector_transverse_spacing) == np.float32(1.2858)
+    assert np.float32(m.detector_axial_spacing) == np.float32(1.0947)
+    assert (m.dist_source_to_isocenter, m.dist_source_to_detector) == (np.float32(595.0), np.float32(1085.6))
+    assert (m.detector_central_channel, m.detector_central_row) == (366.25, 15.5)
+    a, z, got = wfbp.dicom_read_frames(str(tmp_path), m)
+    assert np.array_equal(a, angles) and np.array_equal(z, zs) and np.array_equal(got, raw)
+    a2, z2, got2 = wfbp.dicom_read_frames(str(tmp_path), m, first=2, count=2)
+    assert np.array_equal(got2, raw[2:4]) and np.array_equal(a2, angles[2:4])
+
+
+def test_dicom_ctpd_rejects_bad_input(tmp_path):
+    (tmp_path / "a.dcm").write_bytes(b"\0" * 140)  # no DICM marker
+    with pytest.raises(wfbp.WfbpError):
+        wfbp.dicom_read_meta(str(tmp_path))
+    d = tmp_path / "big"
+    d.mkdir()
+    raw = np.zeros((2, 2, 3), np.float32)
+    _write_ctpd(d, raw, np.zeros(2, np.float32), np.zeros(2, np.float32), True, False)
+    m = wfbp.dicom_read_meta(str(d))
+    with pytest.raises(wfbp.WfbpError):
+        wfbp.dicom_read_frames(str(d), m, first=1, count=5)  # past the last file
