@@ -245,11 +245,13 @@ cudaError_t launch_thicken(const float* vn, float* out, const int* off, const in
 // ---------------------------------------------------------------------------
 //
 // Same samples as k_rebin_f32_rows, written as the two FP16 operand planes of
-// the tensor-core Toeplitz filter: with a per-view power of two o (the
-// largest with o max|x| <= 16384, so no operand overflows FP16),
-// hi = f16(o x), lo = f16(o x - hi), 22 bits of x. One CTA per view walks the
-// view twice: the first pass finds the row maxima, the second writes the
-// planes. The view's rows are padded with zero rows to nrv (a power of two
+// the tensor-core Toeplitz filter: hi = f16(o x), lo = f16(o x - hi), 22
+// bits of x, with a per-view power of two o. One CTA per view writes the
+// planes with o = 1 while it finds the row maxima; a view whose largest
+// sample exceeds 16384 (far above any line integral, but FP16 ends at 65504)
+// is written again with the largest o that brings it to 16384. (FP16 keeps
+// 22 bits of the split down to |x| ~ 0.125 and an absolute 3e-8 below, far
+// inside the filter's error budget.) The view's rows are padded with zero rows to nrv (a power of two
 // that divides the filter's 128-row tile, so no view straddles a tile) and
 // every row with zeros to kp (a multiple of 64). The CTA also writes the FP16
 // storage scales of the filtered rows: per row, the smallest power of two s
@@ -262,8 +264,9 @@ constexpr int RS_THREADS = 256;
 // (as k_rebin_f32_rows) and walks every row; the per-row maxima go through a
 // warp reduction and one shared-memory atomic per warp and row.
 // Scales of one view from its row maxima (shared memory, [nrv]): row and
-// view storage scales of the filtered rows and the operand scale (a power of
-// two; 1 for an all-zero view). Returns the operand scale.
+// view storage scales of the filtered rows and the operand scale (1, or for
+// a view whose largest sample exceeds 16384 the power of two that brings it
+// to 16384). Returns the operand scale.
 __device__ float split_view_scales(const float* s_rowmax, int nrv, int v, float taps_l1, float* __restrict__ row_scale,
                                    float* __restrict__ view_scale, float* __restrict__ op_scale) {
   __shared__ float s_vmax, s_xmax;
@@ -278,7 +281,7 @@ __device__ float split_view_scales(const float* s_rowmax, int nrv, int v, float 
   }
   __syncthreads();
   const float xm = s_xmax;
-  const float o = xm > 0.0f ? exp2f(floorf(log2f(16384.0f / xm))) : 1.0f;
+  const float o = xm > 16384.0f ? exp2f(floorf(log2f(16384.0f / xm))) : 1.0f;
   if (threadIdx.x == 0) {
     view_scale[v] = s_vmax;
     op_scale[v] = o;
@@ -321,13 +324,13 @@ k_rebin_split_rows(const float* __restrict__ raw, __half* __restrict__ a_hi, __h
     return i >= p.nr ? 0.0f  // 0 off the detector and in the padding
                      : FFS ? rebin_taps_ffs_sample(raw, p, tf, i) : rebin_taps_sample(t, i, p.nch);
   };
-  // pass 1: row maxima; kp is a multiple of 64, so every warp is either wholly
-  // inside [0, kp) or wholly outside
+  // pass 1: the planes with o = 1 and the row maxima; kp is a multiple of 64,
+  // so every warp is either wholly inside [0, kp) or wholly outside
   for (int c = threadIdx.x; c < kp; c += blockDim.x) {
     RebinTaps t;
     RebinTapsFfs tf;
     taps(c, t, tf);
-    // four rows' samples (16 independent loads) before their reductions
+    // four rows' samples (16 independent loads) before their stores and reductions
     for (int i0 = 0; i0 < nrv; i0 += 4) {
       float x[4];
 #pragma unroll
@@ -340,12 +343,15 @@ k_rebin_split_rows(const float* __restrict__ raw, __half* __restrict__ a_hi, __h
         const float ax = isnan(x[u]) ? 0.0f : fabsf(x[u]);
         const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(ax));  // ax >= 0: bits order as values
         if (lane == 0 && m) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)m);
+        const size_t row = (size_t)v * nrv + i;
+        split_f16(x[u], 1.0f, a_hi + row * kp + c, a_lo + row * kp + c);
       }
     }
   }
   __syncthreads();
   const float o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
-  // pass 2: the operand planes
+  if (o == 1.0f) return;  // block-uniform
+  // a view beyond FP16's comfortable range: the planes again with o < 1
   for (int c = threadIdx.x; c < kp; c += blockDim.x) {
     RebinTaps t;
     RebinTapsFfs tf;
@@ -403,9 +409,13 @@ k_rebin_split_pairs(const float* __restrict__ raw, __half* __restrict__ a_hi, __
   }
   __syncthreads();
   for (int pass = 0; pass < 2; pass++) {
-    // pass 0: row maxima; pass 1: the operand planes with the view's operand scale
+    // pass 0: the planes with o = 1 and the row maxima; pass 1 (only a view
+    // whose largest sample exceeds 16384): the planes again with o < 1
     float o = 1.0f;
-    if (pass == 1) o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
+    if (pass == 1) {
+      o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
+      if (o == 1.0f) break;  // block-uniform
+    }
     for (int i0 = 0; i0 < nrv; i0 += 2) {
       float x[NP][2][2];  // [pair][row][channel]
 #pragma unroll
@@ -432,7 +442,8 @@ k_rebin_split_pairs(const float* __restrict__ raw, __half* __restrict__ a_hi, __
           }
           const unsigned mm = __reduce_max_sync(0xffffffffu, __float_as_uint(m));  // m >= 0: bits order as values
           if (lane == 0 && mm) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)mm);
-        } else {
+        }
+        {
 #pragma unroll
           for (int k = 0; k < NP; k++) {
             if (!pv[k]) continue;
