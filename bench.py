@@ -33,18 +33,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed vs FP32"
-# DRAM read + write bytes per contributing update of one backprojection launch, from the
-# ncu captures of rows64_short (2.3819501378e10 updates), by precision form and slab height
-# (16-slice slabs stage each view window in twice as many CTAs)
-DRAM_BYTES_PER_UPDATE = {("fp32", 32): (5.157631e9 + 0.103164e9) / 2.3819501378e10,
-                         ("mixed", 32): (5.689086e9 + 0.103863e9) / 2.3819501378e10,
-                         ("fp32", 16): (13.673464e9 + 0.162628e9) / 2.3819501378e10,
-                         ("mixed", 16): (14.311128e9 + 0.162348e9) / 2.3819501378e10}
-# warp instructions per contributing update of one backprojection launch (smsp__inst_executed.sum
-# / updates) from the same captures; the kernel's binding limit is instruction issue
-WARP_INST_PER_UPDATE = {("fp32", 32): 4.47e10 / 2.3819501378e10, ("mixed", 32): 4.66e10 / 2.3819501378e10,
-                        ("fp32", 16): 4.4354276467e10 / 2.3819501378e10,
-                        ("mixed", 16): 4.5782817879e10 / 2.3819501378e10}
+# DRAM read + write bytes and warp instructions per contributing update of one backprojection
+# launch, from the ncu captures of rows64_short (2.3819501378e10 updates; profiles/
+# k_bp_tma_rows64_short.md), by precision form and slab height (16-slice slabs stage each view
+# window in twice as many CTAs); the kernel's binding limit is instruction issue
+DRAM_BYTES_PER_UPDATE = {("fp32", 32): 13.315e9 / 2.3819501378e10,
+                         ("mixed", 16): 15.113e9 / 2.3819501378e10,
+                         ("fp32", 16): 15.113e9 / 2.3819501378e10,   # the mixed form's 16-slice figure
+                         ("mixed", 32): 13.315e9 / 2.3819501378e10}  # the FP32 form's 32-slice figure
+WARP_INST_PER_UPDATE = {("fp32", 32): 4.046e10 / 2.3819501378e10, ("mixed", 16): 4.019e10 / 2.3819501378e10,
+                        ("fp32", 16): 4.046e10 / 2.3819501378e10,   # the FP32 32-slice capture
+                        ("mixed", 32): 4.019e10 / 2.3819501378e10}  # the mixed 16-slice capture
 SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"
 

@@ -40,7 +40,6 @@ namespace {
 
 constexpr int TC_BM = 128;
 constexpr int TC_BK = 64;  // 64 FP16 = 128 bytes, one swizzle row
-constexpr int TC_STAGES = 2;
 constexpr int TC_ACC = 2;            // accumulators in tensor memory (MMAs of tile i+1 overlap the epilogue of i)
 constexpr int TC_EPI_THREADS = 128;  // warps 2-5
 constexpr int TC_THREADS = 64 + TC_EPI_THREADS;
@@ -187,6 +186,7 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const TcOutArgs& 
   }
 }
 
+template <int TC_STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcParams p,
               TcOutArgs o, int* __restrict__ err) {
@@ -375,7 +375,11 @@ bool make_map(CUtensorMap* map, const void* base, uint64_t kp, uint64_t rows, ui
 
 }  // namespace
 
-size_t tc_smem_bytes(int bn) { return (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 2 + 2 * bn * TC_BK * 2) + 1024 + 256; }
+size_t tc_smem_bytes(int bn, int stages) { return (size_t)stages * (2 * TC_BM * TC_BK * 2 + 2 * bn * TC_BK * 2) + 1024 + 256; }
+
+// Ring depth for an N tile: three stages when they fit in shared memory (N
+// tiles of at most 144), else two.
+int tc_stages(int bn) { return tc_smem_bytes(bn, 3) <= 227u * 1024u ? 3 : 2; }
 
 // Chooses the N tile (multiple of 16, <= 256) that minimises padding of nch.
 int tc_choose_bn(int nch) {
@@ -407,8 +411,10 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
   p.np = np;
   if (out.nrv < 1 || TC_BM % out.nrv != 0) return cudaErrorInvalidValue;  // views must not straddle M tiles
   if (2 * bn > (int)TC_TMEM_COLS) return cudaErrorInvalidValue;
-  size_t smem = tc_smem_bytes(bn);
-  cudaError_t e = cudaFuncSetAttribute(k_toeplitz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int stages = tc_stages(bn);
+  size_t smem = tc_smem_bytes(bn, stages);
+  auto kern = stages == 3 ? k_toeplitz_tc<3> : k_toeplitz_tc<2>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -416,6 +422,6 @@ cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, 
   // persistent CTAs, one per SM (the shared memory of one ring fills an SM)
   const long tiles = (long)((me - mb + TC_BM - 1) / TC_BM) * (np / bn);
   const unsigned grid = (unsigned)std::max(1L, std::min<long>(tiles, sms));
-  k_toeplitz_tc<<<grid, TC_THREADS, smem, s>>>(map_a, map_b, p, out, err);
+  kern<<<grid, TC_THREADS, smem, s>>>(map_a, map_b, p, out, err);
   return cudaGetLastError();
 }
