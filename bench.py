@@ -39,11 +39,10 @@ METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed
 # window in twice as many CTAs); the kernel's binding limit is instruction issue
 DRAM_BYTES_PER_UPDATE = {("fp32", 32): 13.315e9 / 2.3819501378e10,
                          ("mixed", 16): 15.113e9 / 2.3819501378e10,
-                         ("fp32", 16): 15.113e9 / 2.3819501378e10,   # the mixed form's 16-slice figure
-                         ("mixed", 32): 13.315e9 / 2.3819501378e10}  # the FP32 form's 32-slice figure
+                         ("fp32", 16): 20.910e9 / 2.3819501378e10,
+                         ("mixed", 32): 13.203e9 / 2.3819501378e10}
 WARP_INST_PER_UPDATE = {("fp32", 32): 4.046e10 / 2.3819501378e10, ("mixed", 16): 4.019e10 / 2.3819501378e10,
-                        ("fp32", 16): 4.046e10 / 2.3819501378e10,   # the FP32 32-slice capture
-                        ("mixed", 32): 4.019e10 / 2.3819501378e10}  # the mixed 16-slice capture
+                        ("fp32", 16): 3.898e10 / 2.3819501378e10, ("mixed", 32): 4.225e10 / 2.3819501378e10}
 SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"
 
