@@ -335,7 +335,7 @@ __global__ void k_rebin_adj_cols(const float* __restrict__ bidx_t, int nch, int 
     if (x1 == x) wgt += ax;
     if (x0 != x && x1 != x) continue;
     if (n == maxl) {
-      atomicOr(err, 0x400);
+      atomicOr(err, WFBP_ERRBIT_ADJ_LIST);
       break;
     }
     cidx[x * maxl + n] = c;

@@ -26,7 +26,8 @@
 //    that lie inside the slab (fused thickening, bp_fused_thicken).
 //
 // Element types: float (FP32 rows) or uint32_t holding half2 pairs
-// (row r, row r+1) of FP16 rows scaled by a per-view power of two.
+// (row r, row r+1) of FP16 rows divided by one power of two for the whole
+// scan, which the host folds into the write-back's 2 pi / P.
 //
 // Every mbarrier wait is bounded; on timeout the CTA records WFBP_ERR_TIMEOUT
 // in the error word and stops. Window or slot overflows (which the host's
@@ -175,9 +176,9 @@ __device__ __forceinline__ void bp_fused_zero(const ThickFuse& tf, int bz, int w
 // the reference leaves there). A bounded wait that gave up sets the failure
 // word (the CTA must stop).
 template <typename T, int CPW, int CU, int NW, int SL, bool COUNT, bool FUSE>
-__device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __restrict__ view_scale,
-                                        float* __restrict__ vol, const float2* __restrict__ view_sc,
-                                        const float* __restrict__ view_z, const float* __restrict__ zslices,
+__device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict__ vol,
+                                        const float2* __restrict__ view_sc, const float* __restrict__ view_z,
+                                        const float* __restrict__ zslices,
                                         const BPParams& p, const BPTile& bt, int bx, int by, int bz,
                                         unsigned long long* __restrict__ count, int* __restrict__ err, uint8_t* smem,
                                         uint32_t ring, const ThickFuse& tf) {
@@ -192,7 +193,6 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
   const BpSmem L = bp_smem_layout(bt, CPW);
   uint8_t* slots = smem + L.slots;                            // [STAGES][nv_max][slot_bytes]
   int2* vinfo = reinterpret_cast<int2*>(smem + L.vinfo);      // [STAGES][nv_max] (view, first channel)
-  float* vsv = reinterpret_cast<float*>(smem + L.vsv);        // [STAGES][nv_max] per-view scale
   int* nvs = reinterpret_cast<int*>(smem + BT_OFF_NVS);       // [STAGES] views, [8] failure flag
   GeoP* geo = reinterpret_cast<GeoP*>(smem + L.geo);          // [warps][nv_max][NPW]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -303,9 +303,8 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
         if (sel) {
           if (pos < bt.nv_max) {
             vinfo[s * bt.nv_max + pos] = make_int2(j, c_lo);
-            vsv[s * bt.nv_max + pos] = HALF ? __ldg(view_scale + j) : 1.0f;
           } else {
-            atomicOr(err, 0x100);  // more views than slots: host sizing violated
+            atomicOr(err, WFBP_ERRBIT_BP_SLOTS);  // more views than slots: host sizing violated
           }
         }
         nv = min(nv + __popc(m), bt.nv_max);
@@ -394,7 +393,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       bool valid = gactive && p_idx >= 0.0f && p_idx <= p.ncm2;
       const int cofs = (int)pf - vi.y;
       if (valid && (cofs < 0 || cofs > bt.W - 2)) {
-        atomicOr(err, 0x200);  // channel window too narrow: host sizing violated
+        atomicOr(err, WFBP_ERRBIT_BP_WINDOW);  // channel window too narrow: host sizing violated
         valid = false;
       }
       const float bq = inv * p.hn;
@@ -430,11 +429,6 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
         aw[u2] = make_float2(0.0f, 0.0f);
       }
       for (int v = 0; v < nv; v++) {
-        float2 sv2 = make_float2(1.0f, 1.0f);
-        if constexpr (HALF) {
-          const float sv = vsv[s * bt.nv_max + v];
-          sv2 = make_float2(sv, sv);
-        }
         const GeoP* gpv = wgeo + v * NPW + (grp * CPG + c0) / 2;
 #pragma unroll
         for (int u2 = 0; u2 < CU / 2; u2++) {
@@ -443,10 +437,16 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
           const float2 dq = __fadd2_rn(q, neg2(g.qmid));
           const bool okx = fabsf(dq.x) <= g.qhw.x;
           const bool oky = fabsf(dq.y) <= g.qhw.y;
-          // any in-range row for invalid lanes (their weight is 0); NaN -> 0
-          const unsigned rx = min((unsigned)__float2int_rz(q.x), nrm2u);
-          const unsigned ry = min((unsigned)__float2int_rz(q.y), nrm2u);
-          const float2 wq = __fadd2_rn(q, make_float2(-(float)rx, -(float)ry));
+          // Row index and fraction through the FP32 pipe: for 0 <= q < 2^23,
+          // q + 2^23 rounded down is 2^23 + floor(q), an integer held in the
+          // low mantissa bits, and subtracting 2^23 again is exact. Invalid
+          // lanes (weight 0; negative, huge or NaN q) read any in-range row:
+          // the unsigned difference of the bit patterns is clamped to nr - 2.
+          const float2 tq = __fadd2_rd(q, make_float2(8388608.0f, 8388608.0f));
+          const float2 fq = __fadd2_rn(tq, make_float2(-8388608.0f, -8388608.0f));
+          const unsigned rx = min(__float_as_uint(tq.x) - 0x4B000000u, nrm2u);
+          const unsigned ry = min(__float_as_uint(tq.y) - 0x4B000000u, nrm2u);
+          const float2 wq = __fadd2_rn(q, neg2(fq));
           const uint8_t* ex = smem + g.addr.x + (rx << 2);
           const uint8_t* ey = smem + g.addr.y + (ry << 2);
           float2 top, bot;
@@ -475,8 +475,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
             top = make_float2(fx.x, fy.x);
             bot = make_float2(fx.y, fy.y);
           }
-          float2 gval = __ffma2_rn(wq, __fadd2_rn(bot, neg2(top)), top);
-          if constexpr (HALF) gval = __fmul2_rn(gval, sv2);
+          const float2 gval = __ffma2_rn(wq, __fadd2_rn(bot, neg2(top)), top);
           // W(q) of cuda_kernels.cuh:79-93 with |q_hat| = |q - hn| / hn
           const float2 a = __fadd2_rn(q, mhn2);
           const float2 tt = __fmul2_rn(make_float2(__saturatef(fmaf(fabsf(a.x), k1, -1.5f)),
@@ -492,7 +491,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
       }
       // cuda_kernels.cuh:283, vol += (2 pi / P) (sum W g) / (sum W): the
       // quotient through the hardware reciprocal (0 / 0 stays NaN), 2 pi / P
-      // applied once at the write-back
+      // (times the FP16 rows' scale) applied once at the write-back
 #pragma unroll
       for (int u2 = 0; u2 < CU / 2; u2++)
         vacc[c0 / 2 + u2] = __ffma2_rn(ag[u2], make_float2(bp_rcp(aw[u2].x), bp_rcp(aw[u2].y)), vacc[c0 / 2 + u2]);
@@ -531,14 +530,13 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, const float* __re
 // One tile per CTA: grid (tiles x, tiles y, SL-slice slabs).
 template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
 __global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
-k_bp_tma(const __grid_constant__ CUtensorMap map, const float* __restrict__ view_scale, float* __restrict__ vol,
-         const float2* __restrict__ view_sc, const float* __restrict__ view_z, const float* __restrict__ zslices,
-         BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {
+k_bp_tma(const __grid_constant__ CUtensorMap map, float* __restrict__ vol, const float2* __restrict__ view_sc,
+         const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {
   // the dynamic shared memory is the only shared memory of this kernel, so
   // it starts at the (128-byte aligned) base of the CTA's window
   extern __shared__ __align__(128) uint8_t smem[];
   bp_init_barriers(smem, NW);
-  bp_tile<T, CPW, CU, NW, SL, COUNT, true>(&map, view_scale, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
+  bp_tile<T, CPW, CU, NW, SL, COUNT, true>(&map, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
                                  bt.zb0 + blockIdx.z, count, err, smem, 0u, tf);
 }
 
@@ -562,7 +560,7 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
     const BpScan* sd = scans + w.x;
     const BPParams p = sd->p;
     const BPTile bt = sd->bt;
-    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false, false>(&sd->map, sd->view_scale, sd->vol, sd->view_sc, sd->view_z,
+    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false, false>(&sd->map, sd->vol, sd->view_sc, sd->view_z,
                                                  sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring,
                                                  sd->tf);
     __syncthreads();  // the tile's shared memory and words[9] are free again
@@ -582,7 +580,7 @@ cudaError_t prepare_kernel(K* kern, int smem) {
 }
 
 template <typename T, int CPW, int CU, int NW, int SL>
-cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
+cudaError_t launch_one(const CUtensorMap& map, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                        unsigned long long* count, int* err, cudaStream_t s, const ThickFuse& tf) {
   const int nslab = (p.nz + SL - 1) / SL;
@@ -594,13 +592,13 @@ cudaError_t launch_one(const CUtensorMap& map, const float* view_scale, float* v
   if (count) {
     e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, true>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
-                                                                         count, err, tf);
+    k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, vol, sc, vz, zs, p, bt, count,
+                                                                         err, tf);
   } else {
     e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, false>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, view_scale, vol, sc, vz, zs, p, bt,
-                                                                          count, err, tf);
+    k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, vol, sc, vz, zs, p, bt, count,
+                                                                          err, tf);
   }
   return cudaGetLastError();
 }
@@ -630,12 +628,12 @@ cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items
   X(16, 4, 8, 32) X(16, 8, 8, 32) X(16, 4, 8, 16) X(16, 8, 8, 16)
 
 template <typename T>
-cudaError_t launch_elem(const CUtensorMap& map, const float* view_scale, float* vol, const float2* sc,
+cudaError_t launch_elem(const CUtensorMap& map, float* vol, const float2* sc,
                         const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                         unsigned long long* count, int* err, cudaStream_t s, const ThickFuse& tf) {
   const int cpw = bt.tx * bt.ty / bt.nw;
 #define WFBP_ONE(C, U, N, S) \
-  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return launch_one<T, C, U, N, S>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s, tf);
+  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return launch_one<T, C, U, N, S>(map, vol, sc, vz, zs, p, bt, count, err, s, tf);
   WFBP_BP_SHAPES(WFBP_ONE)
 #undef WFBP_ONE
   return cudaErrorInvalidValue;
@@ -674,10 +672,14 @@ cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, 
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
-                                   const float2* sc, const float* vz, const float* zs, const BPParams& p,
+cudaError_t launch_backproject_tma(const void* D, int elem_half2, float row_scale, float* vol,
+                                   const float2* sc, const float* vz, const float* zs, const BPParams& p0,
                                    const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s,
                                    const ThickFuse* tf) {
+  // half2 pairs hold the rows divided by row_scale (a power of two): the
+  // write-back's 2 pi / P takes it back, exactly
+  BPParams p = p0;
+  if (elem_half2) p.dtheta *= row_scale;
   if (!bp_tma_supported(bt)) return cudaErrorInvalidValue;
   CUtensorMap map;
   cudaError_t e = bp_tma_encode_map(D, elem_half2, p, bt, &map);
@@ -685,8 +687,8 @@ cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* v
   ThickFuse none;
   memset(&none, 0, sizeof(none));
   const ThickFuse& f = tf ? *tf : none;
-  if (elem_half2) return launch_elem<uint32_t>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s, f);
-  return launch_elem<float>(map, view_scale, vol, sc, vz, zs, p, bt, count, err, s, f);
+  if (elem_half2) return launch_elem<uint32_t>(map, vol, sc, vz, zs, p, bt, count, err, s, f);
+  return launch_elem<float>(map, vol, sc, vz, zs, p, bt, count, err, s, f);
 }
 
 cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,

@@ -126,7 +126,7 @@ __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" :::
 // One output tile's epilogue: the 32 rows of TMEM lane quarter `q` (rows
 // 32q .. 32q+31 of the tile, one per lane) from accumulator columns `acc`.
 __device__ __forceinline__ void tc_epilogue(const TcParams& p, const TcOutArgs& o, uint32_t tmem_acc, int q, int lane,
-                                            int m0, int n0, float (*s_xchg)[16]) {
+                                            int m0, int n0, float (*s_xchg)[16], int* err) {
   // row m of the tile: view v = m / nrv, row i = m % nrv (rows i >= nr are zero padding)
   const int m = m0 + q * 32 + lane;
   const int v = m / o.nrv, i = m % o.nrv;
@@ -137,7 +137,7 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const TcOutArgs& 
     inv /= o.row_scale_in[m];
     if (n0 == 0) o.row_scale_out[(size_t)v * o.nr + i] = o.row_scale_in[m];
   } else if (o.mode == TC_OUT_PAIRS && m < p.me) {
-    inv /= o.view_scale[v];
+    inv /= o.pair_scale;
   }
   const uint32_t trow = tmem_acc + ((uint32_t)(q * 32) << 16);
   for (int c = 0; c < p.BN; c += 16) {
@@ -160,10 +160,16 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const TcOutArgs& 
       epi_sync();
       if (row_ok) {
         const bool last = (i == o.nr - 1);
+        bool over = false;
         for (int k = 0; k < 16 && n + k < p.nch; k++) {
-          const __half2 h = __floats2half2_rn(val[k] * inv, last ? 0.0f : nxt[k] * inv);
+          const float a = val[k] * inv, b = last ? 0.0f : nxt[k] * inv;
+          // |x| <= 16384 keeps the half2 differences of the backprojection's
+          // channel interpolation finite
+          over |= fabsf(a) > 16384.0f || fabsf(b) > 16384.0f;
+          const __half2 h = __floats2half2_rn(a, b);
           o.pairs[((size_t)v * p.nch + (n + k)) * o.nrp + i] = *reinterpret_cast<const uint32_t*>(&h);
         }
+        if (over) atomicOr(err, WFBP_ERRBIT_F16_RANGE);
       }
       continue;
     }
@@ -318,7 +324,7 @@ k_toeplitz_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      tc_epilogue(p, o, tmem + (uint32_t)(a * p.BN), q, lane, p.mb + (t / ntn) * TC_BM, (t % ntn) * p.BN, s_xchg);
+      tc_epilogue(p, o, tmem + (uint32_t)(a * p.BN), q, lane, p.mb + (t / ntn) * TC_BM, (t % ntn) * p.BN, s_xchg, err);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acc_empty[a]);
     }

@@ -526,6 +526,20 @@ k_adaptive_filter(const float* __restrict__ raw, float* __restrict__ out, int nr
   }
 }
 
+namespace {
+__global__ void k_fill(float* __restrict__ dst, float value, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = value;
+}
+}  // namespace
+
+cudaError_t launch_fill(float* dst, float value, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 1184);
+  k_fill<<<blocks, 256, 0, s>>>(dst, value, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_adaptive_filter(const float* raw, float* out, int nr, int nch, float s, long r0, long r1,
                                    cudaStream_t st) {
   if (r1 <= r0) return cudaSuccess;

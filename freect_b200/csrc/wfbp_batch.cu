@@ -141,7 +141,9 @@ int build_plan(wfbp_batch* b) {
     if (bp_tma_encode_map(b->filt[i], b->precision == WFBP_PRECISION_MIXED ? 1 : 0, hs[i].p, bt, &hs[i].map) !=
         cudaSuccess)
       return bfail(b, WFBP_ERR_CUDA, "tensor map encoding failed for scan " + std::to_string(i));
-    hs[i].view_scale = b->precision == WFBP_PRECISION_MIXED ? b->scales[i] : nullptr;
+    // FP16 row pairs hold the rows divided by the scan's pair_scale (a power
+    // of two): the write-back's 2 pi / P takes it back, exactly
+    if (b->precision == WFBP_PRECISION_MIXED) hs[i].p.dtheta *= c->pair_scale;
     hs[i].vol = b->native[i];
     hs[i].view_sc = c->d_view_sc;
     hs[i].view_z = c->d_view_z;
@@ -382,6 +384,11 @@ WFBP_API int wfbp_batch_check_device_status(wfbp_batch* b) {
     cudaMemset(b->d_err, 0, sizeof(int));
     return bfail(b, h == WFBP_ERR_TIMEOUT ? WFBP_ERR_TIMEOUT : WFBP_ERR_CUDA,
                  "the batched backprojection reported device error word " + std::to_string(h));
+  }
+  // the scans' rebin and filter stages report through their contexts' words
+  for (int i = 0; i < (int)b->ctx.size(); i++) {
+    const int st = wfbp_check_device_status(b->ctx[i]);
+    if (st) return bfail(b, st, "scan " + std::to_string(i) + ": " + wfbp_last_error(b->ctx[i]));
   }
   return WFBP_OK;
 }

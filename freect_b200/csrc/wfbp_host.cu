@@ -25,6 +25,12 @@ int fail(wfbp_ctx* ctx, int code, const std::string& msg) {
   return code;
 }
 
+std::string hex_word(int h) {
+  char b[16];
+  snprintf(b, sizeof(b), "%x", (unsigned)h);
+  return b;
+}
+
 #define CUDA_TRY(ctx, call)                                                                  \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
@@ -685,6 +691,11 @@ WFBP_API int wfbp_ctx_create(const CTGeometry* cg, const ReconConfig* rp, const 
     }
     ctx->taps_l1 = (float)l1;
     ctx->tap_scale = hmax > 0.0 ? (float)exp2(floor(log2(16384.0 / hmax))) : 1.0f;
+    // FP16 row pairs of the backprojection layout: one power of two >= the
+    // taps' L1 norm divides every filtered row of the scan, so a stored value
+    // is at most max|rebinned sample| (|y| <= max|x| sum|h|) and keeps FP16's
+    // 11 significant bits; the backprojection multiplies it back once
+    ctx->pair_scale = l1 > 0.0 ? (float)exp2(ceil(log2(l1))) : 1.0f;
     for (int n = 0; n < nch; n++)
       for (int k = 0; k < nch; k++) {
         const float h = ctx->taps[n > k ? n - k : k - n] * ctx->tap_scale;  // power of two: exact
@@ -885,7 +896,12 @@ WFBP_API int wfbp_check_device_status(wfbp_ctx* ctx) {
   CUDA_TRY(ctx, cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h != 0) {
     cudaMemset(ctx->d_err, 0, sizeof(int));
-    return fail(ctx, h, "a bounded device-side wait gave up (tensor-core filter pipeline)");
+    if (h == WFBP_ERR_TIMEOUT) return fail(ctx, WFBP_ERR_TIMEOUT, "a bounded device-side wait gave up");
+    if (h & WFBP_ERRBIT_F16_RANGE)
+      return fail(ctx, WFBP_ERR_UNSUPPORTED,
+                  "mixed precision: a filtered row exceeds the FP16 row pairs' range (16384 x the scan's "
+                  "power-of-two scale; rebinned samples above 16384)");
+    return fail(ctx, WFBP_ERR_CUDA, "device-side sizing check failed (error word 0x" + hex_word(h) + ")");
   }
   return WFBP_OK;
 }
@@ -985,21 +1001,22 @@ int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales
     return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_filter: no backprojection-layout launch fits this geometry");
   if (ctx->ext.precision == WFBP_PRECISION_MIXED) {
     if (!scales) return fail(ctx, WFBP_ERR_INVALID_ARG, "wfbp_filter: mixed precision needs scales");
-    float *row_sc, *view_sc, *op_sc;
+    float *row_sc, *view_sc, *op_sc;  // view_sc: the rebin's largest row scale per view (not read here)
     mixed_scale_ptrs(ctx, rebinned, &row_sc, &view_sc, &op_sc);
+    (void)view_sc;
     TcOutArgs o;
     memset(&o, 0, sizeof(o));
     o.nr = ctx->nr;
     o.nrv = ctx->nrv;
     o.nrp = ctx->bpt.nrp;
     o.row_scale_in = row_sc;
-    o.view_scale = view_sc;
     o.op_scale = op_sc;
     o.tap_scale = ctx->tap_scale;
     if (bpl) {
       o.mode = TC_OUT_PAIRS;
       o.pairs = static_cast<uint32_t*>(filtered);
-      CUDA_TRY(ctx, cudaMemcpyAsync(scales + vb, view_sc + vb, sizeof(float) * (ve - vb), cudaMemcpyDeviceToDevice, s));
+      o.pair_scale = ctx->pair_scale;
+      CUDA_TRY(ctx, launch_fill(scales + vb, ctx->pair_scale, (size_t)(ve - vb), s));
     } else {
       o.mode = TC_OUT_F16_ROWS;
       o.y16 = static_cast<__half*>(filtered);
@@ -1029,7 +1046,7 @@ int do_backproject(wfbp_ctx* ctx, const void* filtered, const float* scales, flo
   if (layout == WFBP_LAYOUT_BACKPROJECTION) {
     if (!ctx->bp_tma_ok)
       return fail(ctx, WFBP_ERR_UNSUPPORTED, "wfbp_backproject: no backprojection-layout launch fits this geometry");
-    CUDA_TRY(ctx, launch_backproject_tma(filtered, mixed ? 1 : 0, scales, vol, ctx->d_view_sc, ctx->d_view_z,
+    CUDA_TRY(ctx, launch_backproject_tma(filtered, mixed ? 1 : 0, ctx->pair_scale, vol, ctx->d_view_sc, ctx->d_view_z,
                                          ctx->d_z_native, p, ctx->bpt, update_count, ctx->d_err, s, tf));
     return WFBP_OK;
   }
@@ -1392,12 +1409,17 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   int st = ensure_scratch(ctx);
   if (st) return st;
   const int lay = WFBP_LAYOUT_BACKPROJECTION;
-  constexpr int kChunks = 8;
+  // chunks of about 64 MB of readings (8 to 64): the first backprojection
+  // waits for the copies of the views its slabs reach, so smaller chunks
+  // start it sooner (rows64, 2.24 GB: 8 chunks 261.5 ms, 35 chunks 256 ms)
+  const size_t raw_bytes = sizeof(float) * (size_t)ctx->n_readings * ctx->raw_rows * ctx->raw_ch;
+  const int kChunks = (int)std::max<size_t>(8, std::min<size_t>(64, (raw_bytes + (64u << 20) - 1) / (64u << 20)));
   if (!ctx->s_copy) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking));
   if (!ctx->s_back) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->s_back, cudaStreamNonBlocking));
   for (auto& b : ctx->s_bp)
     if (!b) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
-  if (ctx->ev_copy.empty()) {
+  if (ctx->ev_copy.size() != (size_t)kChunks + 4) {
+    for (auto& e : ctx->ev_copy) cudaEventDestroy(e);
     // chunk copies, caller order, a launch's slices final, views filtered, streams joined
     ctx->ev_copy.resize(kChunks + 4);
     for (auto& e : ctx->ev_copy) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1491,7 +1513,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
       const cudaStream_t sb = ctx->s_bp[nlaunch++ % 2];
       CUDA_TRY(ctx, cudaEventRecord(ev_filt, s));
       CUDA_TRY(ctx, cudaStreamWaitEvent(sb, ev_filt, 0));
-      CUDA_TRY(ctx, launch_backproject_tma(ctx->s_filtered, mixed ? 1 : 0, ctx->s_scales, ctx->s_vol_native,
+      CUDA_TRY(ctx, launch_backproject_tma(ctx->s_filtered, mixed ? 1 : 0, ctx->pair_scale, ctx->s_vol_native,
                                            ctx->d_view_sc, ctx->d_view_z, ctx->d_z_native, p, bt, nullptr,
                                            ctx->d_err, sb, fuse ? &tf : nullptr));
       for (int k = sl; k < e; k++) done[k] = 1;

@@ -52,13 +52,21 @@ struct BPTile {
   int zb0, nzb;      // slabs [zb0, zb0 + nzb) of this launch (nzb 0: all)
 };
 
+// Bits of the device-side error word besides WFBP_ERR_TIMEOUT (which a
+// bounded wait that gave up stores whole): conditions the host's sizing rules
+// out, and values outside the range of the mixed form's FP16 row pairs.
+constexpr int WFBP_ERRBIT_BP_SLOTS = 0x100;   // backprojection: more views in a stage than slots
+constexpr int WFBP_ERRBIT_BP_WINDOW = 0x200;  // backprojection: channel window too narrow
+constexpr int WFBP_ERRBIT_ADJ_LIST = 0x400;   // rebin adjoint: per-channel source list full
+constexpr int WFBP_ERRBIT_F16_RANGE = 0x800;  // filter: |filtered row / pair_scale| > 16384
+
 // Byte offsets of the TMA backprojection's shared-memory regions; the same
 // function sizes the launch on the host and carves the buffer on the device.
 constexpr int BT_CWARPS = 16;  // default consumer warps of the TMA backprojection
 constexpr int BT_STAGES = 2;   // view-window ring depth
 constexpr int BT_FUSE_WORDS = 384;  // shared-memory words for one slab's fused-thickening records
 struct BpSmem {
-  unsigned slots, vinfo, vsv, geo, fuse, total;
+  unsigned slots, vinfo, geo, fuse, total;
 };
 // Bytes 0..127 hold the ring's mbarriers and a few words (fixed across the
 // tiles of a persistent launch); the per-scan regions follow.
@@ -69,8 +77,6 @@ __host__ __device__ inline BpSmem bp_smem_layout(const BPTile& bt, int cpw) {
   o += (unsigned)(BT_STAGES * bt.nv_max * bt.slot_bytes);
   L.vinfo = o;
   o += (unsigned)(BT_STAGES * bt.nv_max * 8);
-  L.vsv = o;
-  o += (unsigned)(BT_STAGES * bt.nv_max * 4);
   o = (o + 15u) & ~15u;
   L.geo = o;
   o += (unsigned)(bt.nw * bt.nv_max * (cpw / 2) * 48);  // column-pair geometry records
@@ -159,8 +165,9 @@ struct wfbp_ctx {
   int nrv = 0;                      // rows per view in the operand planes (power of two >= nr)
   float taps_l1 = 0.0f;             // sum over |d| < nch of |h[d]|
   float tap_scale = 1.0f;           // power of two applied to the taps in d_bplanes
+  float pair_scale = 1.0f;          // power of two >= taps_l1 dividing the FP16 row pairs (backprojection layout)
   void* d_bplanes = nullptr;        // FP16 [2][tc_np][tc_kp] (hi, lo of tap_scale * T)
-  int* d_err = nullptr;             // device-side error word (bounded waits)
+  int* d_err = nullptr;             // device-side error word (WFBP_ERR_TIMEOUT, or WFBP_ERRBIT_* bits)
 
   // TMA-staged backprojection (backprojection layout [V][nch][nrp])
   bool bp_tma_ok = false;
@@ -216,10 +223,12 @@ struct TcOutArgs {
   uint32_t* pairs;              // TC_OUT_PAIRS: [V][nch][nrp] half2 (row i, row i+1)
   const float* row_scale_in;    // [V*nrv]
   float* row_scale_out;         // [V][nr]
-  const float* view_scale;      // [V]
+  float pair_scale;             // TC_OUT_PAIRS: power of two dividing every stored row of the scan
   const float* op_scale;        // [V] power-of-two scale of the view's FP16 operand rows
   float tap_scale;              // power-of-two scale of the FP16 Toeplitz operand
 };
+// dst[0..n) = value
+cudaError_t launch_fill(float* dst, float value, size_t n, cudaStream_t s);
 cudaError_t launch_filter_tc(const void* a_planes, const void* b_planes, int M, int nch, int kp, int np, int bn,
                              const TcOutArgs& out, int* err, cudaStream_t s, int mb = 0, int me = -1);
 cudaError_t launch_filter_f32_tr(const float* x, float* yt, const float* d_taps, long rows, int nch, int nr, int nrp,
@@ -247,7 +256,6 @@ struct alignas(64) BpScan {
   CUtensorMap map;              // filtered rows [V][nch][nrp], box {nrp, W, 1}
   BPParams p;
   BPTile bt;
-  const float* view_scale;      // per-view scales (FP16 row pairs) or null
   float* vol;                   // native volume
   const float2* view_sc;
   const float* view_z;
@@ -260,7 +268,7 @@ cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw
                                          int grid, cudaStream_t s);
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);
 bool bp_tma_supported(const BPTile& bt);
-cudaError_t launch_backproject_tma(const void* D, int elem_half2, const float* view_scale, float* vol,
+cudaError_t launch_backproject_tma(const void* D, int elem_half2, float row_scale, float* vol,
                                    const float2* sc, const float* vz, const float* zs, const BPParams& p,
                                    const BPTile& bt, unsigned long long* count, int* err, cudaStream_t s,
                                    const ThickFuse* tf = nullptr);

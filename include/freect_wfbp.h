@@ -171,9 +171,12 @@ enum wfbp_recon_kernel {
  * boundary. REFERENCE keeps the reference's [view][row][channel] FP32 (or
  * FP16 + per-row scales); BACKPROJECTION is the channel-major layout the
  * TMA-staged backprojection reads: [view][channel][nrp] FP32, or half2 pairs
- * (row r, row r+1) with one power-of-two scale per view, nrp = nr rounded up
- * to a multiple of 4. wfbp_run always uses BACKPROJECTION internally when the
- * geometry allows it. */
+ * (row r, row r+1) of the rows divided by one power of two for the whole
+ * scan (the smallest >= the taps' L1 norm sum|h|, so a stored value is at
+ * most the largest rebinned sample); nrp = nr rounded up to a multiple of 4.
+ * wfbp_filter writes that scale into every view's entry of row_scales [V]
+ * and wfbp_backproject applies it. wfbp_run always uses BACKPROJECTION
+ * internally when the geometry allows it. */
 enum wfbp_layout {
   WFBP_LAYOUT_REFERENCE = 0,
   WFBP_LAYOUT_BACKPROJECTION = 1
@@ -342,8 +345,12 @@ int wfbp_set_bp_config(wfbp_ctx* ctx, const wfbp_bp_config* config);
 
 /* Reads and clears the context's device-side error word, which kernels
  * with bounded waits set instead of hanging (synchronous). Returns
- * WFBP_ERR_TIMEOUT if a wait gave up since the last check. No counterpart
- * in the reference, which has no device-side waits. */
+ * WFBP_ERR_TIMEOUT if a wait gave up since the last check,
+ * WFBP_ERR_UNSUPPORTED if the mixed form's filter met a filtered value
+ * beyond the range of its FP16 row pairs (16384 x the scan's scale, which
+ * takes rebinned samples above 16384), WFBP_ERR_CUDA if a device-side sizing
+ * check failed. No counterpart in the reference, which has no device-side
+ * waits. */
 int wfbp_check_device_status(wfbp_ctx* ctx);
 
 /* Failure-detection self-test: launches a kernel whose mbarrier wait can
@@ -373,7 +380,8 @@ int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* stream);
 /* Stage 2 of RebinAndFilter (ReconstructionMachine.cu:262-290: R2C,
  * multiply_filter, C2R, reshape_rebin_into_final_array) as a Toeplitz
  * contraction. filtered: FP32 [V][nr][nch] (FP32) or FP16 [V][nr][nch]
- * plus row_scales FP32 [V][nr] (MIXED; row_scales may be NULL for FP32). */
+ * plus row_scales FP32 [V][nr] (MIXED; row_scales may be NULL for FP32), in
+ * the reference layout; in the backprojection layout see wfbp_layout. */
 int wfbp_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* row_scales,
                 void* stream);
 
@@ -464,7 +472,8 @@ int wfbp_batch_size(const wfbp_batch* batch, int* n_scans, int* n_items);
 int wfbp_batch_bp_configs(const wfbp_batch* batch, wfbp_bp_config* out, int cap, int* n);
 int wfbp_batch_get_bp_config(const wfbp_batch* batch, wfbp_bp_config* config);
 int wfbp_batch_set_bp_config(wfbp_batch* batch, const wfbp_bp_config* config);
-/* Reads and clears the batch's device-side error word (synchronous). */
+/* Reads and clears the batch's device-side error word and those of its
+ * scans' contexts (synchronous); statuses as wfbp_check_device_status. */
 int wfbp_batch_check_device_status(wfbp_batch* batch);
 const char* wfbp_batch_last_error(const wfbp_batch* batch);
 

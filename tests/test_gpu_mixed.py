@@ -124,10 +124,34 @@ def test_mixed_backprojection_layout_stages(orc, which):
     ctx.thicken(vn, vol)
     torch.cuda.synchronize()
     ctx.check_device_status()
+    # one power of two for the whole scan, the smallest >= the taps' L1 norm
     s = sc.cpu().numpy()[: spec.V]
-    assert np.all(s > 0) and np.all(np.log2(s) == np.round(np.log2(s)))
+    taps = wfbp.filter_taps(cg).astype(np.float64)
+    l1 = abs(taps[0]) + 2 * np.abs(taps[1:]).sum()
+    assert np.all(s == s[0]) and s[0] >= l1 and s[0] / 2 < l1
+    assert np.log2(s[0]) == np.round(np.log2(s[0]))
     r64 = orc.reconstruct_f64(spec, raw)
     got = vol.cpu().numpy()
     rms, mx, n = orc.hu_error(got, r64["volume"])
     assert n == np.isfinite(r64["volume"]).sum()
+    assert rms <= 1.0, (rms, mx)
+
+
+def test_mixed_pairs_range_is_reported(orc):
+    # rebinned samples far above 16384 overflow the FP16 row pairs: the filter
+    # records it and check_device_status reports it; the context stays usable
+    spec = scans.tiny()
+    raw = orc.synth_project(spec.synth(), spec.ellipsoids())
+    ctx, cg, gp = make_ctx(spec, filtered_layout=T.LAYOUT_BACKPROJECTION)
+    vol = ctx.alloc("volume")
+    ctx.run(dev(raw * 1.0e7), vol)
+    torch.cuda.synchronize()
+    with pytest.raises(wfbp.WfbpError) as e:
+        ctx.check_device_status()
+    assert e.value.status == 5 and "FP16" in str(e.value)  # WFBP_ERR_UNSUPPORTED
+    ctx.run(dev(raw), vol)
+    torch.cuda.synchronize()
+    ctx.check_device_status()
+    r64 = orc.reconstruct_f64(spec, raw)
+    rms, mx, n = orc.hu_error(vol.cpu().numpy(), r64["volume"])
     assert rms <= 1.0, (rms, mx)
