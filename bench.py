@@ -37,11 +37,11 @@ METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed
 # launch, from the ncu captures of rows64_short (2.3819501378e10 updates; profiles/
 # k_bp_tma_rows64_short.md), by precision form and slab height (16-slice slabs stage each view
 # window in twice as many CTAs); the kernel's binding limit is instruction issue
-DRAM_BYTES_PER_UPDATE = {("fp32", 32): 15.01e9 / 2.3819501378e10,
-                         ("mixed", 16): 14.82e9 / 2.3819501378e10,
+DRAM_BYTES_PER_UPDATE = {("fp32", 32): 14.42e9 / 2.3819501378e10,
+                         ("mixed", 16): 14.39e9 / 2.3819501378e10,
                          ("fp32", 16): 20.84e9 / 2.3819501378e10,
                          ("mixed", 32): 13.13e9 / 2.3819501378e10}
-WARP_INST_PER_UPDATE = {("fp32", 32): 3.854e10 / 2.3819501378e10, ("mixed", 16): 3.783e10 / 2.3819501378e10,
+WARP_INST_PER_UPDATE = {("fp32", 32): 3.537e10 / 2.3819501378e10, ("mixed", 16): 3.428e10 / 2.3819501378e10,
                         ("fp32", 16): 3.819e10 / 2.3819501378e10, ("mixed", 32): 3.952e10 / 2.3819501378e10}
 SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"

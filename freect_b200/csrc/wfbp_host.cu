@@ -992,8 +992,11 @@ WFBP_API int wfbp_rebin(wfbp_ctx* ctx, const float* raw, void* rebinned, void* s
 
 namespace {
 
+// publish: write the FP16 pairs' scale into scales[vb..ve) (the stage API's
+// contract); the context's own runs skip it, their backprojection applies
+// the context's scale directly.
 int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream, int vb = 0,
-              int ve = -1) {
+              int ve = -1, bool publish = true) {
   const cudaStream_t s = (cudaStream_t)stream;
   if (ve < 0) ve = ctx->V;
   const bool bpl = layout == WFBP_LAYOUT_BACKPROJECTION;
@@ -1016,7 +1019,7 @@ int do_filter(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales
       o.mode = TC_OUT_PAIRS;
       o.pairs = static_cast<uint32_t*>(filtered);
       o.pair_scale = ctx->pair_scale;
-      CUDA_TRY(ctx, launch_fill(scales + vb, ctx->pair_scale, (size_t)(ve - vb), s));
+      if (publish) CUDA_TRY(ctx, launch_fill(scales + vb, ctx->pair_scale, (size_t)(ve - vb), s));
     } else {
       o.mode = TC_OUT_F16_ROWS;
       o.y16 = static_cast<__half*>(filtered);
@@ -1337,7 +1340,7 @@ int run_stages(wfbp_ctx* ctx, const float* raw, float* vol, void* stream, cudaEv
   nvtxRangePop();
   if (ev) cudaEventRecord(ev[1], s);
   nvtxRangePushA("filter");
-  if (!st) st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, stream);
+  if (!st) st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, stream, 0, -1, false);
   nvtxRangePop();
   if (ev) cudaEventRecord(ev[2], s);
   // with the backprojection layout the thickening of the slices inside one
@@ -1547,7 +1550,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
       rin = ctx->s_af;
     }
     if ((st = do_rebin(ctx, rin, ctx->s_rebinned, vb, ve, s))) return st;
-    if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, s, vb, ve))) return st;
+    if ((st = do_filter(ctx, ctx->s_rebinned, ctx->s_filtered, ctx->s_scales, lay, s, vb, ve, false))) return st;
     if ((st = launch_ready(ve))) return st;
   }
   if ((st = launch_ready(V + 1))) return st;
@@ -1616,7 +1619,7 @@ bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, in
   return size_bp_tile(ctx, tx, ty, cu, nw, slab, out);
 }
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream) {
-  return do_filter(ctx, rebinned, filtered, scales, layout, stream);
+  return do_filter(ctx, rebinned, filtered, scales, layout, stream, 0, -1, false);
 }
 int backproject_stage(wfbp_ctx* ctx, const void* filtered, const float* scales, float* vol, int layout,
                       void* stream) {

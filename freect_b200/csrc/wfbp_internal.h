@@ -305,6 +305,8 @@ int set_error(wfbp_ctx* ctx, int code, const std::string& msg);
 BPParams backprojection_params(const wfbp_ctx* ctx);
 void buffer_bytes(const wfbp_ctx* ctx, int layout, size_t* reb, size_t* filt, size_t* scal);
 bool size_backprojection(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, int slab, BPTile* out);
+// wfbp_filter without writing the FP16 pairs' scale into `scales` (the
+// context's backprojection applies the scale itself)
 int filter_stage(wfbp_ctx* ctx, const void* rebinned, void* filtered, float* scales, int layout, void* stream);
 int backproject_stage(wfbp_ctx* ctx, const void* filtered, const float* scales, float* vol, int layout,
                       void* stream);
