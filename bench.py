@@ -39,10 +39,10 @@ METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed
 # window in twice as many CTAs); the kernel's binding limit is instruction issue
 DRAM_BYTES_PER_UPDATE = {("fp32", 32): 14.42e9 / 2.3819501378e10,
                          ("mixed", 16): 14.39e9 / 2.3819501378e10,
-                         ("fp32", 16): 20.84e9 / 2.3819501378e10,
-                         ("mixed", 32): 13.13e9 / 2.3819501378e10}
+                         ("fp32", 16): 21.08e9 / 2.3819501378e10,
+                         ("mixed", 32): 13.18e9 / 2.3819501378e10}
 WARP_INST_PER_UPDATE = {("fp32", 32): 3.537e10 / 2.3819501378e10, ("mixed", 16): 3.428e10 / 2.3819501378e10,
-                        ("fp32", 16): 3.819e10 / 2.3819501378e10, ("mixed", 32): 3.952e10 / 2.3819501378e10}
+                        ("fp32", 16): 3.475e10 / 2.3819501378e10, ("mixed", 32): 3.631e10 / 2.3819501378e10}
 SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"
 
