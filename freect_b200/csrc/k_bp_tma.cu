@@ -74,15 +74,27 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// Geometry of a pair of columns for one view, stored so that three 16-byte
+// Geometry of a pair of columns for one view, stored so that 16-byte
 // shared-memory loads give both columns' fields as float2 operands of the
-// packed FP32x2 instructions (FFMA2 / FADD2 / FMUL2).
+// packed FP32x2 instructions (FFMA2 / FADD2 / FMUL2). GeoP carries the row
+// range the table-position cull leaves (cuda_kernels.cuh:232); when the
+// host has shown that the cull never removes a sample whose row lies in
+// [0, nr - 2] (the detector's cone is shorter than z_rot), that range is
+// [0, nr - 2] for every record, GeoQ drops it and the test uses its centre
+// and half width (nr - 2) / 2 as constants: the same compare on the same
+// values, so both records give the same samples.
 struct __align__(16) GeoP {
   float2 bq, cq;    // q(z) = bq z + cq
   float2 qmid, qhw;  // valid for |q - qmid| <= qhw (the row range [qlo, qhi] as centre and half width)
   int2 addr;        // shared-memory byte offset of (channel pf, row 0) of the view's slot
   float2 wp;        // FP32 rows: channel weight; half2 pairs: bits of the half2 (wp, wp)
 };
+struct __align__(16) GeoQ {
+  float2 bq, cq;    // q(z) = bq z + cq (an invalid record: bq = 0, cq = -1e30)
+  int2 addr;
+  float2 wp;
+};
+static_assert(sizeof(GeoP) == BP_GEO_BYTES_ZCULL && sizeof(GeoQ) == BP_GEO_BYTES, "record sizes of bp_smem_layout");
 
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
@@ -175,7 +187,7 @@ __device__ __forceinline__ void bp_fused_zero(const ThickFuse& tf, int bz, int w
 // outside the reconstruction FOV (whose voxels are written as 0, the value
 // the reference leaves there). A bounded wait that gave up sets the failure
 // word (the CTA must stop).
-template <typename T, int CPW, int CU, int NW, int SL, bool COUNT, bool FUSE>
+template <typename T, int CPW, int CU, int NW, int SL, bool ZC, bool COUNT, bool FUSE>
 __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict__ vol,
                                         const float2* __restrict__ view_sc, const float* __restrict__ view_z,
                                         const float* __restrict__ zslices,
@@ -183,6 +195,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
                                         unsigned long long* __restrict__ count, int* __restrict__ err, uint8_t* smem,
                                         uint32_t ring, const ThickFuse& tf) {
   constexpr bool HALF = !std::is_same<T, float>::value;
+  using Geo = typename std::conditional<ZC, GeoP, GeoQ>::type;
   constexpr int NPW = CPW / 2;  // column pairs per warp
   // SL = 32: the warp's 32 lanes are 32 slices of each of its CPW columns.
   // SL = 16: lanes 0-15 and 16-31 are 16 slices of two column groups of
@@ -190,11 +203,11 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
   constexpr int NG = 32 / SL, CPG = CPW / NG;  // column groups per warp, columns per group
   static_assert(SL == 32 || SL == 16, "slab of 32 or 16 slices");
   static_assert(CU % 2 == 0 && CPG % CU == 0, "columns per step must be even and divide the columns per group");
-  const BpSmem L = bp_smem_layout(bt, CPW);
+  const BpSmem L = bp_smem_layout(bt, CPW);  // bt.zc == ZC (the launch picks the instantiation)
   uint8_t* slots = smem + L.slots;                            // [STAGES][nv_max][slot_bytes]
   int2* vinfo = reinterpret_cast<int2*>(smem + L.vinfo);      // [STAGES][nv_max] (view, first channel)
   int* nvs = reinterpret_cast<int*>(smem + BT_OFF_NVS);       // [STAGES] views, [8] failure flag
-  GeoP* geo = reinterpret_cast<GeoP*>(smem + L.geo);          // [warps][nv_max][NPW]
+  Geo* geo = reinterpret_cast<Geo*>(smem + L.geo);            // [warps][nv_max][NPW]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + BT_STAGES;
   volatile int* s_fail = nvs + 8;
@@ -339,7 +352,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
   for (int c = 0; c < CPG / 2; c++) vacc[c] = make_float2(0.0f, 0.0f);
   unsigned long long cnt = 0;
   const float k1 = 2.5f / p.hn;
-  GeoP* wgeo = geo + (size_t)warp * bt.nv_max * NPW;
+  Geo* wgeo = geo + (size_t)warp * bt.nv_max * NPW;
   constexpr int VPP = 32 / CPW;  // views per geometry pass
   const int gc = lane % CPW, gv = lane / CPW;
   const int gt = warp * CPW + gc;  // tile column handled by this lane in geometry passes
@@ -355,6 +368,8 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
   const float2 pi2 = make_float2(3.14159265f, 3.14159265f);
   const float2 half2c = make_float2(0.5f, 0.5f);
   const unsigned nrm2u = (unsigned)(p.nr - 2);
+  const float hrow = 0.5f * p.nrm2;  // rows [0, nr - 2] as centre and half width (records without the cull)
+  const float2 mhrow2 = make_float2(-hrow, -hrow);
 
   for (int t = 0; t < p.P2; t++) {
     const uint32_t g = ring + (uint32_t)t;
@@ -400,19 +415,28 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
       const float cq = p.hn * fmaf(A - zt, inv, 1.0f);
       const float wp = p_idx - pf;
       float* gf = reinterpret_cast<float*>(wgeo + v * NPW + (gc >> 1)) + (gc & 1);
-      gf[0] = bq;
-      gf[2] = cq;
-      // rows q in [0, nr - 2] (cuda_kernels.cuh:259-263) of views within z_rot (:232)
-      const float qlo = fmaxf(0.0f, fmaf(zt - p.z_rot, bq, cq)), qhi = fminf(p.nrm2, fmaf(zt + p.z_rot, bq, cq));
-      gf[4] = valid ? 0.5f * (qlo + qhi) : 0.0f;
-      gf[6] = valid ? 0.5f * (qhi - qlo) : -1.0f;
-      reinterpret_cast<int*>(gf)[8] =
+      constexpr int O = ZC ? 4 : 0;  // float offset of addr / wp behind the row range
+      if constexpr (ZC) {
+        gf[0] = bq;
+        gf[2] = cq;
+        // rows q in [0, nr - 2] (cuda_kernels.cuh:259-263) of views within z_rot (:232)
+        const float qlo = fmaxf(0.0f, fmaf(zt - p.z_rot, bq, cq)), qhi = fminf(p.nrm2, fmaf(zt + p.z_rot, bq, cq));
+        gf[4] = valid ? 0.5f * (qlo + qhi) : 0.0f;
+        gf[6] = valid ? 0.5f * (qhi - qlo) : -1.0f;
+      } else {
+        // rows q in [0, nr - 2] (cuda_kernels.cuh:259-263); an invalid record
+        // gives every lane q = -1e30, outside the rows, and finite row weights
+        // (a NaN q would make 0 x NaN in the column's sums)
+        gf[0] = valid ? bq : 0.0f;
+        gf[2] = valid ? cq : -1.0e30f;
+      }
+      reinterpret_cast<int*>(gf)[4 + O] =
           (int)(L.slots + (size_t)(s * bt.nv_max + v) * bt.slot_bytes) + (valid ? cofs : 0) * nrpb;
       if constexpr (HALF) {
         const __half2 w2 = __float2half2_rn(wp);
-        gf[10] = __uint_as_float(*reinterpret_cast<const uint32_t*>(&w2));
+        gf[6 + O] = __uint_as_float(*reinterpret_cast<const uint32_t*>(&w2));
       } else {
-        gf[10] = wp;
+        gf[6 + O] = wp;
       }
     }
     __syncwarp();
@@ -429,14 +453,21 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
         aw[u2] = make_float2(0.0f, 0.0f);
       }
       for (int v = 0; v < nv; v++) {
-        const GeoP* gpv = wgeo + v * NPW + (grp * CPG + c0) / 2;
+        const Geo* gpv = wgeo + v * NPW + (grp * CPG + c0) / 2;
 #pragma unroll
         for (int u2 = 0; u2 < CU / 2; u2++) {
-          const GeoP g = gpv[u2];
+          const Geo g = gpv[u2];
           const float2 q = __ffma2_rn(zl2, g.bq, g.cq);
-          const float2 dq = __fadd2_rn(q, neg2(g.qmid));
-          const bool okx = fabsf(dq.x) <= g.qhw.x;
-          const bool oky = fabsf(dq.y) <= g.qhw.y;
+          bool okx, oky;
+          if constexpr (ZC) {
+            const float2 dq = __fadd2_rn(q, neg2(g.qmid));
+            okx = fabsf(dq.x) <= g.qhw.x;
+            oky = fabsf(dq.y) <= g.qhw.y;
+          } else {
+            const float2 dq = __fadd2_rn(q, mhrow2);
+            okx = fabsf(dq.x) <= hrow;
+            oky = fabsf(dq.y) <= hrow;
+          }
           // Row index and fraction through the FP32 pipe: for 0 <= q < 2^23,
           // q + 2^23 rounded down is 2^23 + floor(q), an integer held in the
           // low mantissa bits, and subtracting 2^23 again is exact. Invalid
@@ -528,22 +559,23 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
 }
 
 // One tile per CTA: grid (tiles x, tiles y, SL-slice slabs).
-template <typename T, int CPW, int CU, int NW, int SL, bool COUNT>
+template <typename T, int CPW, int CU, int NW, int SL, bool ZC, bool COUNT>
 __global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
 k_bp_tma(const __grid_constant__ CUtensorMap map, float* __restrict__ vol, const float2* __restrict__ view_sc,
-         const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, BPTile bt, unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {
+         const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, BPTile bt,
+         unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {
   // the dynamic shared memory is the only shared memory of this kernel, so
   // it starts at the (128-byte aligned) base of the CTA's window
   extern __shared__ __align__(128) uint8_t smem[];
   bp_init_barriers(smem, NW);
-  bp_tile<T, CPW, CU, NW, SL, COUNT, true>(&map, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
+  bp_tile<T, CPW, CU, NW, SL, ZC, COUNT, true>(&map, vol, view_sc, view_z, zslices, p, bt, blockIdx.x, blockIdx.y,
                                  bt.zb0 + blockIdx.z, count, err, smem, 0u, tf);
 }
 
 // Persistent launch over the column tiles of several scans: each CTA takes
 // the next work item (scan, tile x, tile y, slab) from a global counter until
 // the list is exhausted. Items are listed by decreasing estimated cost.
-template <typename T, int CPW, int CU, int NW, int SL>
+template <typename T, int CPW, int CU, int NW, int SL, bool ZC>
 __global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
 k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items, int n_items,
                unsigned* __restrict__ next, int* __restrict__ err) {
@@ -560,7 +592,7 @@ k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items,
     const BpScan* sd = scans + w.x;
     const BPParams p = sd->p;
     const BPTile bt = sd->bt;
-    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, false, false>(&sd->map, sd->vol, sd->view_sc, sd->view_z,
+    ring += (uint32_t)bp_tile<T, CPW, CU, NW, SL, ZC, false, false>(&sd->map, sd->vol, sd->view_sc, sd->view_z,
                                                  sd->zslices, p, bt, w.y, w.z, w.w, nullptr, err, smem, ring,
                                                  sd->tf);
     __syncthreads();  // the tile's shared memory and words[9] are free again
@@ -579,7 +611,7 @@ cudaError_t prepare_kernel(K* kern, int smem) {
   return e;
 }
 
-template <typename T, int CPW, int CU, int NW, int SL>
+template <typename T, int CPW, int CU, int NW, int SL, bool ZC>
 cudaError_t launch_one(const CUtensorMap& map, float* vol, const float2* sc,
                        const float* vz, const float* zs, const BPParams& p, const BPTile& bt,
                        unsigned long long* count, int* err, cudaStream_t s, const ThickFuse& tf) {
@@ -590,23 +622,23 @@ cudaError_t launch_one(const CUtensorMap& map, float* vol, const float2* sc,
   constexpr int threads = (NW + 1) * 32;
   cudaError_t e;
   if (count) {
-    e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, true>, bt.smem_bytes);
+    e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, ZC, true>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, NW, SL, true><<<grid, threads, bt.smem_bytes, s>>>(map, vol, sc, vz, zs, p, bt, count,
-                                                                         err, tf);
+    k_bp_tma<T, CPW, CU, NW, SL, ZC, true><<<grid, threads, bt.smem_bytes, s>>>(map, vol, sc, vz, zs, p, bt, count,
+                                                                             err, tf);
   } else {
-    e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, false>, bt.smem_bytes);
+    e = prepare_kernel<NW>(k_bp_tma<T, CPW, CU, NW, SL, ZC, false>, bt.smem_bytes);
     if (e != cudaSuccess) return e;
-    k_bp_tma<T, CPW, CU, NW, SL, false><<<grid, threads, bt.smem_bytes, s>>>(map, vol, sc, vz, zs, p, bt, count,
-                                                                          err, tf);
+    k_bp_tma<T, CPW, CU, NW, SL, ZC, false><<<grid, threads, bt.smem_bytes, s>>>(map, vol, sc, vz, zs, p, bt, count,
+                                                                              err, tf);
   }
   return cudaGetLastError();
 }
 
 template <typename T, int CPW, int CU, int NW, int SL>
-cudaError_t launch_batch_one(const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
+cudaError_t launch_batch_one(int zc, const BpScan* scans, const int4* items, int n_items, unsigned* next, int* err,
                              int smem_bytes, int grid, cudaStream_t s) {
-  auto kern = k_bp_tma_batch<T, CPW, CU, NW, SL>;
+  auto kern = zc ? k_bp_tma_batch<T, CPW, CU, NW, SL, true> : k_bp_tma_batch<T, CPW, CU, NW, SL, false>;
   cudaError_t e = prepare_kernel<NW>(kern, smem_bytes);
   if (e != cudaSuccess) return e;
   // grid = SMs; persistent CTAs: as many per SM as fit
@@ -633,7 +665,9 @@ cudaError_t launch_elem(const CUtensorMap& map, float* vol, const float2* sc,
                         unsigned long long* count, int* err, cudaStream_t s, const ThickFuse& tf) {
   const int cpw = bt.tx * bt.ty / bt.nw;
 #define WFBP_ONE(C, U, N, S) \
-  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S) return launch_one<T, C, U, N, S>(map, vol, sc, vz, zs, p, bt, count, err, s, tf);
+  if (cpw == C && bt.cu == U && bt.nw == N && bt.slab == S)                                                      \
+    return bt.zc ? launch_one<T, C, U, N, S, true>(map, vol, sc, vz, zs, p, bt, count, err, s, tf)               \
+                 : launch_one<T, C, U, N, S, false>(map, vol, sc, vz, zs, p, bt, count, err, s, tf);
   WFBP_BP_SHAPES(WFBP_ONE)
 #undef WFBP_ONE
   return cudaErrorInvalidValue;
@@ -691,13 +725,13 @@ cudaError_t launch_backproject_tma(const void* D, int elem_half2, float row_scal
   return launch_elem<float>(map, vol, sc, vz, zs, p, bt, count, err, s, f);
 }
 
-cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, int zc, const BpScan* scans,
                                          const int4* items, int n_items, unsigned* next, int* err, int smem_bytes,
                                          int grid, cudaStream_t s) {
 #define WFBP_B32(C, U, N, S) \
-  if (cpw == C && cu == U && nw == N && slab == S) return launch_batch_one<uint32_t, C, U, N, S>(scans, items, n_items, next, err, smem_bytes, grid, s);
+  if (cpw == C && cu == U && nw == N && slab == S) return launch_batch_one<uint32_t, C, U, N, S>(zc, scans, items, n_items, next, err, smem_bytes, grid, s);
 #define WFBP_BF(C, U, N, S) \
-  if (cpw == C && cu == U && nw == N && slab == S) return launch_batch_one<float, C, U, N, S>(scans, items, n_items, next, err, smem_bytes, grid, s);
+  if (cpw == C && cu == U && nw == N && slab == S) return launch_batch_one<float, C, U, N, S>(zc, scans, items, n_items, next, err, smem_bytes, grid, s);
   if (elem_half2) {
     WFBP_BP_SHAPES(WFBP_B32)
   } else {

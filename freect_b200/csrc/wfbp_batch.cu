@@ -32,6 +32,7 @@ struct wfbp_batch {
   int n_items = 0;
   unsigned* d_next = nullptr;
   int* d_err = nullptr;
+  int zc = 1;                       // record layout of the persistent launch (BPTile::zc of every scan)
   int smem = 0, grid = 0;
   cudaStream_t own = nullptr;
   cudaGraph_t graph = nullptr;
@@ -124,6 +125,10 @@ int build_plan(wfbp_batch* b) {
     double cost;
   };
   std::vector<Item> items;
+  // one launch, one record layout: with the table-position cull's row range
+  // if any scan's cull can bind
+  b->zc = 0;
+  for (int i = 0; i < n; i++) b->zc |= b->ctx[i]->bp_zcull;
   for (int i = 0; i < n; i++) {
     wfbp_ctx* c = b->ctx[i];
     BPTile bt;
@@ -133,6 +138,12 @@ int build_plan(wfbp_batch* b) {
                                                 std::to_string(b->cfg.tile_y) + "/" +
                                                 std::to_string(b->cfg.cols_per_step) + " does not fit scan " +
                                                 std::to_string(i));
+    if (bt.zc != b->zc) {
+      bt.zc = b->zc;
+      bt.smem_bytes = (int)bp_tma_smem_bytes(bt, 4);
+      if (bt.smem_bytes > 220 * 1024)
+        return bfail(b, WFBP_ERR_UNSUPPORTED, "backprojection configuration does not fit scan " + std::to_string(i));
+    }
     b->tiles[i] = bt;
     smem = std::max(smem, bt.smem_bytes);
     memset(&hs[i], 0, sizeof(BpScan));
@@ -351,7 +362,7 @@ WFBP_API int wfbp_batch_run(wfbp_batch* b, const float* const* raws, float* cons
     if (!st && !e) {
       const int cpw = b->cfg.tile_x * b->cfg.tile_y / b->cfg.consumer_warps;
       e = launch_backproject_tma_batch(b->precision == WFBP_PRECISION_MIXED ? 1 : 0, cpw, b->cfg.cols_per_step,
-                                       b->cfg.consumer_warps, b->cfg.slab,
+                                       b->cfg.consumer_warps, b->cfg.slab, b->zc,
                                        b->d_scans, b->d_items, b->n_items, b->d_next, b->d_err, b->smem, b->grid, s);
     }
     for (int i = 0; i < n && !st && !e; i++) {
@@ -489,7 +500,7 @@ WFBP_API int wfbp_batch_run_host(wfbp_batch* b, const float* const* raws_host, f
     if (n_items > 0) {
       BCUDA(b, cudaMemsetAsync(b->d_next, 0, sizeof(unsigned), s));
       BCUDA(b, launch_backproject_tma_batch(b->precision == WFBP_PRECISION_MIXED ? 1 : 0, cpw, b->cfg.cols_per_step,
-                                            b->cfg.consumer_warps, b->cfg.slab, b->d_scans, items, n_items,
+                                            b->cfg.consumer_warps, b->cfg.slab, b->zc, b->d_scans, items, n_items,
                                             b->d_next, b->d_err, b->smem, b->grid, s));
     }
     for (int i = i0; i < i1; i++) {

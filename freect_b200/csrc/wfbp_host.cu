@@ -310,6 +310,10 @@ void bp_reach(wfbp_ctx* ctx, const std::vector<float>& table) {
   }
   ctx->bp_reach = (float)reach;
   ctx->bp_nv_max = std::max(1, nv_max);
+  // A sample with its row in [0, nr - 2] has |z - z_j| <= cone; below z_rot
+  // by a margin for rounding, the cull of cuda_kernels.cuh:232 never removes
+  // one and the backprojection's records drop its row range
+  ctx->bp_zcull = cone < (double)ctx->cg.z_rot * (1.0 - 1e-3) ? 0 : 1;
 }
 
 // Sizes one TMA backprojection configuration; false if it does not fit.
@@ -323,6 +327,7 @@ bool size_bp_tile(const wfbp_ctx* ctx, int tx, int ty, int cu, int nw, int slab,
   b.slab = slab;
   b.zb0 = 0;
   b.nzb = 0;
+  b.zc = ctx->bp_zcull;
   const double ext = sqrt(pow((b.tx - 1) * vx, 2) + pow((b.ty - 1) * vy, 2));
   b.W = (int)ceil(ext * ctx->gp.pixel_scale) + 5;
   b.W = std::max(4, std::min(b.W, 256));

@@ -50,6 +50,7 @@ struct BPTile {
   int nw;            // consumer warps per CTA (16, 20 or 24; one more warp produces)
   int slab;          // native slices per slab (32, or 16 with two column groups per warp)
   int zb0, nzb;      // slabs [zb0, zb0 + nzb) of this launch (nzb 0: all)
+  int zc;            // 1: geometry records carry the table-position cull's row range (it can bind)
 };
 
 // Bits of the device-side error word besides WFBP_ERR_TIMEOUT (which a
@@ -65,6 +66,8 @@ constexpr int WFBP_ERRBIT_F16_RANGE = 0x800;  // filter: |filtered row / pair_sc
 constexpr int BT_CWARPS = 16;  // default consumer warps of the TMA backprojection
 constexpr int BT_STAGES = 2;   // view-window ring depth
 constexpr int BT_FUSE_WORDS = 384;  // shared-memory words for one slab's fused-thickening records
+constexpr int BP_GEO_BYTES_ZCULL = 48;  // column-pair record with the row range of the table-position cull
+constexpr int BP_GEO_BYTES = 32;        // column-pair record when that cull never binds
 struct BpSmem {
   unsigned slots, vinfo, geo, fuse, total;
 };
@@ -79,7 +82,7 @@ __host__ __device__ inline BpSmem bp_smem_layout(const BPTile& bt, int cpw) {
   o += (unsigned)(BT_STAGES * bt.nv_max * 8);
   o = (o + 15u) & ~15u;
   L.geo = o;
-  o += (unsigned)(bt.nw * bt.nv_max * (cpw / 2) * 48);  // column-pair geometry records
+  o += (unsigned)(bt.nw * bt.nv_max * (cpw / 2) * (bt.zc ? BP_GEO_BYTES_ZCULL : BP_GEO_BYTES));  // column-pair records
   L.fuse = o;
   o += (unsigned)(BT_FUSE_WORDS * 4);  // the slab's fused-thickening records (ThickFuse)
   L.total = o;
@@ -174,6 +177,8 @@ struct wfbp_ctx {
   BPTile bpt;
   float bp_reach = 0.0f;            // slab-level view prefilter half width (mm)
   int bp_nv_max = 1;                // most views of one theta~ reaching a slab
+  int bp_zcull = 1;                 // 0: the table-position cull (|z - z_j| > z_rot) never removes a
+                                    // sample whose row lies in [0, nr - 2] (cone shorter than z_rot)
 
   // context-owned scratch for wfbp_run / wfbp_run_host
   void* s_rebinned = nullptr;
@@ -263,7 +268,7 @@ struct alignas(64) BpScan {
   ThickFuse tf;                 // fused thickening (tf.out == nullptr: none)
 };
 cudaError_t bp_tma_encode_map(const void* D, int elem_half2, const BPParams& p, const BPTile& bt, CUtensorMap* map);
-cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, const BpScan* scans,
+cudaError_t launch_backproject_tma_batch(int elem_half2, int cpw, int cu, int nw, int slab, int zc, const BpScan* scans,
                                          const int4* items, int n_items, unsigned* next, int* err, int smem_bytes,
                                          int grid, cudaStream_t s);
 size_t bp_tma_smem_bytes(const BPTile& bt, int elem_bytes);

@@ -102,12 +102,16 @@ def test_mixed_requires_row_scales(orc):
     assert e.value.status == 1
 
 
-@pytest.mark.parametrize("which", ["tiny", "odd"])
+@pytest.mark.parametrize("which", ["tiny", "odd", "lowpitch"])
 def test_mixed_backprojection_layout_stages(orc, which):
-    # split-FP16 filter writing FP16 row pairs with per-view scales, read by the
-    # TMA-staged backprojection; against the FP64 oracle
+    # split-FP16 filter writing FP16 row pairs with one scale per scan, read by
+    # the TMA-staged backprojection; against the FP64 oracle ("lowpitch": the
+    # table-position cull binds, 4 mm table feed per rotation)
     if which == "tiny":
         spec = scans.tiny()
+    elif which == "lowpitch":
+        spec = scans.tiny()
+        spec.feed = 4.0
     else:
         spec = scans.tiny(nch=90, nr=5, P=100, rotations=2.57, nx=33, n_slices=3)
         spec.ny = 17

@@ -289,13 +289,19 @@ def test_fp32_form_vs_reference_kernels(orc, path):
     assert rms <= 0.5 and mx <= 2.0, (rms, mx)
 
 
-@pytest.mark.parametrize("which", ["tiny", "odd", "small128"])
+@pytest.mark.parametrize("which", ["tiny", "odd", "small128", "lowpitch"])
 def test_backprojection_layout_stages(orc, which):
     # FP32 form through the stage API with the backprojection layout: the
     # transposed filter output equals the reference-layout one, and the
     # TMA-staged backprojection equals the transcript on the same rows.
+    # "lowpitch": a table feed (4 mm per rotation) below the detector cone's
+    # height, so the table-position cull (cuda_kernels.cuh:232) removes
+    # samples the rows would admit and the records carry its row range.
     if which == "tiny":
         spec = scans.tiny()
+    elif which == "lowpitch":
+        spec = scans.tiny()
+        spec.feed = 4.0
     elif which == "odd":
         spec = scans.tiny(nch=90, nr=5, P=100, rotations=2.57, nx=33, n_slices=3)
         spec.ny = 17
