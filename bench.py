@@ -37,12 +37,21 @@ METRIC = "backproj voxel-view updates/s & s/volume at <=1 HU RMSE vs FP64; mixed
 # launch, from the ncu captures of rows64_short (2.3819501378e10 updates; profiles/
 # k_bp_tma_rows64_short.md), by precision form and slab height (16-slice slabs stage each view
 # window in twice as many CTAs); the kernel's binding limit is instruction issue
-DRAM_BYTES_PER_UPDATE = {("fp32", 32): 14.42e9 / 2.3819501378e10,
-                         ("mixed", 16): 14.39e9 / 2.3819501378e10,
-                         ("fp32", 16): 21.08e9 / 2.3819501378e10,
-                         ("mixed", 32): 13.18e9 / 2.3819501378e10}
-WARP_INST_PER_UPDATE = {("fp32", 32): 3.537e10 / 2.3819501378e10, ("mixed", 16): 3.428e10 / 2.3819501378e10,
-                        ("fp32", 16): 3.475e10 / 2.3819501378e10, ("mixed", 32): 3.631e10 / 2.3819501378e10}
+# ncu captures of k_bp_tma on rows64_short (2.3819501378e10 updates per launch;
+# profiles/k_bp_tma_rows64_short.md): DRAM bytes and warp instructions per
+# update, keyed by (form, configuration) for the shapes the autotuner picks on
+# rows64, else by (form, slab height)
+_SHORT_UPDATES = 2.3819501378e10
+DRAM_BYTES_PER_UPDATE = {("fp32", 32): 14.42e9 / _SHORT_UPDATES,
+                         ("mixed", 16): 14.39e9 / _SHORT_UPDATES,
+                         ("fp32", 16): 21.08e9 / _SHORT_UPDATES,
+                         ("mixed", 32): 13.18e9 / _SHORT_UPDATES,
+                         ("mixed", "16x8/4w8s16"): 34.85e9 / _SHORT_UPDATES,
+                         ("fp32", "16x8/8w8s32"): 15.24e9 / _SHORT_UPDATES}
+WARP_INST_PER_UPDATE = {("fp32", 32): 3.537e10 / _SHORT_UPDATES, ("mixed", 16): 3.428e10 / _SHORT_UPDATES,
+                        ("fp32", 16): 3.475e10 / _SHORT_UPDATES, ("mixed", 32): 3.631e10 / _SHORT_UPDATES,
+                        ("mixed", "16x8/4w8s16"): 3.4788e10 / _SHORT_UPDATES,
+                        ("fp32", "16x8/8w8s32"): 3.4167e10 / _SHORT_UPDATES}
 SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"
 
@@ -709,11 +718,13 @@ def stage_rooflines(form, ctx, d, updates, stage, clk):
     form: 2 (V nr) nch^2 FLOP against 148 SMs x 128 lanes x 2 x clock)."""
     hbm, bf16, bf16_sus, peak_src = load_peaks()
     mhz = (clk or {}).get("sm_mhz") or 1965.0
-    slab = ctx.bp_config().slab
+    bpc = ctx.bp_config()
+    slab, shape = bpc.slab, autotune_name(bpc.key())
     t_bp = stage["backproject"] / 1000.0
-    wipu = WARP_INST_PER_UPDATE.get((form, slab))
+    wipu = WARP_INST_PER_UPDATE.get((form, shape), WARP_INST_PER_UPDATE.get((form, slab)))
     ipeak = SMS * SCHEDULERS_PER_SM * mhz * 1e6
-    dram_per_update = DRAM_BYTES_PER_UPDATE.get((form, slab))
+    dram_per_update = DRAM_BYTES_PER_UPDATE.get((form, shape), DRAM_BYTES_PER_UPDATE.get((form, slab)))
+    src = "configuration %s" % shape if (form, shape) in WARP_INST_PER_UPDATE else "slab height %d" % slab
     traffic = dram_per_update * updates if dram_per_update else None
     compulsory = d.filtered_bytes + d.native_volume_bytes
     bp = {"bound": "issue", "kernel": "backproject", "achieved": wipu * updates / t_bp if wipu else None,
@@ -726,9 +737,9 @@ def stage_rooflines(form, ctx, d, updates, stage, clk):
           "updates_per_s": updates / t_bp,
           "warp_inst_per_update": wipu,
           "note": "warp instructions per update and DRAM bytes per update from the ncu capture of the same "
-                  "kernel and slab height on rows64_short (profiles/), scaled by this launch's updates; peak = "
+                  "kernel and %s on rows64_short (profiles/), scaled by this launch's updates; peak = "
                   "%d SMs x %d schedulers x %.0f MHz (sampled); taps are shared-memory reads after one TMA "
-                  "staging per view window" % (SMS, SCHEDULERS_PER_SM, mhz)}
+                  "staging per view window" % (src, SMS, SCHEDULERS_PER_SM, mhz)}
     samples = d.n_views * d.n_rows * d.n_channels
     rebin_bytes = d.raw_bytes + samples * 4  # FP32 rows, or the two FP16 operand planes
     t_rb = stage["rebin"] / 1000.0

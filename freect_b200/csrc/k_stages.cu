@@ -80,10 +80,28 @@ k_rebin_f32_rows(const float* __restrict__ raw, float* __restrict__ out, const f
   }
 }
 
+namespace {
+// The view-chunk kernels serve scans without a flying focal spot whose raw
+// frames fit 31-bit element offsets.
+bool use_vchunk_rebin(const RebinParams& p) { return p.G == 1 && (long long)p.V * p.nr * p.nch < (1ll << 31); }
+}  // namespace
+
+template <bool SPLIT, bool F64>
+__global__ void k_rebin_vchunk(const float* __restrict__ raw, float* __restrict__ out, __half* __restrict__ a_hi,
+                               __half* __restrict__ a_lo, unsigned* __restrict__ rowmax,
+                               const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
+                               const double2* __restrict__ chan64, RebinParams p, int kp, int nrv, int vb, int ve);
+
 cudaError_t launch_rebin_f32(const float* raw, float* out, const float* d_beta, const float* d_bidx,
                              const RebinParams& p, cudaStream_t s, int vb, int ve) {
   if (ve < 0) ve = p.V;
   if (vb < 0 || vb >= ve || ve > p.V) return cudaErrorInvalidValue;
+  if (use_vchunk_rebin(p)) {
+    const dim3 g((unsigned)((p.nch + RV_CW - 1) / RV_CW), (unsigned)((ve - vb + RV_NY - 1) / RV_NY));
+    k_rebin_vchunk<false, false><<<g, RV_CW, 0, s>>>(raw, out, nullptr, nullptr, nullptr, d_beta, d_bidx, nullptr, p,
+                                                      0, 0, vb, ve);
+    return cudaGetLastError();
+  }
   dim3 g((unsigned)((p.nch + RBR_CH - 1) / RBR_CH), (unsigned)(ve - vb));
   if (p.G == 1)
     k_rebin_f32_rows<false><<<g, RBR_CH, 0, s>>>(raw, out, d_beta, d_bidx, p, vb);
@@ -462,6 +480,160 @@ k_rebin_split_pairs(const float* __restrict__ raw, __half* __restrict__ a_hi, __
   }
 }
 
+// ---------------------------------------------------------------------------
+// view-chunk rebin (no flying focal spot)
+// ---------------------------------------------------------------------------
+//
+// Output sample (v, i, c) blends readings y0(v, c) and y1(v, c) = y0 + 1
+// (clamped), and y0(v + 1, c) = y1(v, c) except where the rounding of the
+// sample coordinates or the clamp at the scan's ends says otherwise. In the
+// per-view kernels above every texel row is fetched twice from L2, once as
+// y1 of view v and once as y0 of view v + 1, by CTAs of different views.
+// Here a thread owns one channel of RV_NY consecutive views and loads, per
+// detector row, the RV_NY + 1 readings y0(v0), y1(v0), ..., y1(v0 + RV_NY - 1)
+// once (a separate y0 load only where the chain breaks): (RV_NY + 1) / (2
+// RV_NY) of the texel traffic. The lanes of a warp are consecutive channels
+// of the same view (full-line stores). Taps and sample arithmetic are the
+// per-view kernels' (rebin_taps_x / rebin_taps_y or their FP64 forms,
+// rebin_bilinear), so the samples are the same bit for bit.
+// SPLIT writes the two FP16 planes with o = 1 and the row maxima (one warp
+// reduction per view and row, the CTA's warps merged in shared memory, then
+// into the global maxima: bits of |x| in row_scale, zeroed before the
+// launch); k_rebin_split_scales turns them into the scales.
+template <bool SPLIT, bool F64>
+__global__ void __launch_bounds__(RV_CW)
+k_rebin_vchunk(const float* __restrict__ raw, float* __restrict__ out, __half* __restrict__ a_hi,
+               __half* __restrict__ a_lo, unsigned* __restrict__ rowmax, const float* __restrict__ beta_t,
+               const float* __restrict__ bidx_t, const double2* __restrict__ chan64, RebinParams p, int kp, int nrv,
+               int vb, int ve) {
+  extern __shared__ unsigned s_max[];  // SPLIT: [RV_NY][nrv] largest |sample| (bits; >= 0 orders as values)
+  const int lane = threadIdx.x % 32;
+  const int c = blockIdx.x * RV_CW + threadIdx.x;
+  const int v0 = vb + (int)blockIdx.y * RV_NY;
+  const int nv = min(RV_NY, ve - v0);
+  const int ncw = SPLIT ? kp : p.nch;  // channels written (the planes' padding channels hold zeros)
+  const int cc = min(c, p.nch - 1);
+  RebinTapsX tx;
+  tx.ok = false;
+  tx.c0 = tx.c1 = 0;
+  tx.ax = 0.0f;
+  if (c < p.nch) tx = F64 ? rebin_taps64_x(p.nch, __ldg(chan64 + c)) : rebin_taps_x(p.nch, __ldg(bidx_t + c), p.q8);
+  const float beta = F64 ? 0.0f : __ldg(beta_t + cc);
+  const double2 ch = F64 ? __ldg(chan64 + cc) : make_double2(0.0, 0.0);
+  // element offsets (reading y, sheet row 0, channel c0) from the last raw row:
+  // r[k] = y0 of view k for k = 0, else y1 of view k - 1; b[k] = y0 of view k
+  // where it differs from y1 of view k - 1 (brk bit k)
+  const int vs = p.nr * p.nch;
+  int r[RV_NY + 1], yb[RV_NY];
+  float ay[RV_NY];
+  unsigned brk = 0u;
+#pragma unroll
+  for (int k = 0; k < RV_NY; k++) {
+    RebinTapsY ty;
+    ty.y0 = ty.y1 = 0;
+    ty.ay = 0.0f;
+    if (k < nv && c < p.nch)
+      ty = F64 ? rebin_taps64_y(p.V, ch, v0 + k, p.voff) : rebin_taps_y(p.V, beta, v0 + k, p.dth, p.q8, p.voff);
+    const int o0 = ty.y0 * vs + tx.c0, o1 = ty.y1 * vs + tx.c0;
+    if (k == 0) r[0] = o0;
+    yb[k] = o0;
+    if (k > 0 && o0 != r[k]) brk |= 1u << k;
+    r[k + 1] = o1;
+    ay[k] = ty.ay;
+  }
+  const int dc = tx.c1 - tx.c0;  // -1, or 0 at the detector's last channel (c0 = 0)
+  if constexpr (SPLIT) {
+    for (int e = threadIdx.x; e < RV_NY * nrv; e += RV_CW) s_max[e] = 0u;
+    __syncthreads();
+  }
+  const bool wr = c < ncw;
+  const float* last = raw + (size_t)(p.nr - 1) * p.nch;
+  const int nrows = SPLIT ? nrv : p.nr;
+  for (int i = 0; i < nrows; i++) {
+    const float* row = last - (size_t)min(i, p.nr - 1) * p.nch;  // rows >= nr: padding, written as zeros
+    float ta[RV_NY + 1], tb[RV_NY + 1];
+#pragma unroll
+    for (int k = 0; k <= RV_NY; k++) {
+      ta[k] = tb[k] = 0.0f;
+      if (k <= nv) {
+        ta[k] = __ldg(row + r[k]);
+        tb[k] = __ldg(row + (r[k] + dc));
+      }
+    }
+    float x[RV_NY];
+#pragma unroll
+    for (int k = 0; k < RV_NY; k++) {
+      float t00 = ta[k], t10 = tb[k];
+      if ((brk >> k) & 1u) {
+        t00 = __ldg(row + yb[k]);
+        t10 = __ldg(row + (yb[k] + dc));
+      }
+      x[k] = tx.ok && i < p.nr ? rebin_bilinear(t00, t10, ta[k + 1], tb[k + 1], tx.ax, ay[k]) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < RV_NY; k++) {
+      if (k < nv && wr) {
+        if constexpr (SPLIT) {
+          const size_t o = ((size_t)(v0 + k) * nrv + i) * kp + c;
+          split_f16(x[k], 1.0f, a_hi + o, a_lo + o);
+        } else {
+          out[((size_t)(v0 + k) * p.nr + i) * p.nch + c] = x[k];
+        }
+      }
+    }
+    if constexpr (SPLIT) {
+#pragma unroll
+      for (int k = 0; k < RV_NY; k++) {
+        // fmaxf semantics: a NaN sample does not raise the maximum
+        const float a = wr && k < nv && !isnan(x[k]) ? fabsf(x[k]) : 0.0f;
+        const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(a));
+        if (lane == 0 && m) atomicMax(&s_max[k * nrv + i], m);
+      }
+    }
+  }
+  if constexpr (SPLIT) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < nv * nrv; e += RV_CW) {
+      const unsigned m = s_max[e];
+      if (m) atomicMax(rowmax + (size_t)(v0 + e / nrv) * nrv + e % nrv, m);
+    }
+  }
+}
+
+// The scales of the mixed rebin's views from the row maxima that
+// k_rebin_vchunk left in row_scale (split_view_scales, one CTA per view); a
+// view whose largest sample exceeds 16384 has its planes written again with
+// the operand scale o < 1 (the samples recomputed, as the per-view kernels'
+// second pass).
+template <bool F64>
+__global__ void __launch_bounds__(RS_THREADS)
+k_rebin_split_scales(const float* __restrict__ raw, __half* __restrict__ a_hi, __half* __restrict__ a_lo,
+                     float* __restrict__ row_scale, float* __restrict__ view_scale, float* __restrict__ op_scale,
+                     const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
+                     const double2* __restrict__ chan64, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
+  extern __shared__ float s_rowmax[];  // [nrv]
+  const int v = vb + blockIdx.x;
+  for (int i = threadIdx.x; i < nrv; i += blockDim.x) s_rowmax[i] = row_scale[(size_t)v * nrv + i];
+  __syncthreads();
+  const float o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
+  if (o == 1.0f) return;  // block-uniform
+  for (int c = threadIdx.x; c < kp; c += blockDim.x) {
+    RebinTaps t;
+    t.ok = false;
+    t.raw0 = t.raw1 = raw;
+    t.c0 = t.c1 = 0;
+    t.ax = t.ay = 0.0f;
+    if (c < p.nch)
+      t = F64 ? rebin_taps64(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, __ldg(chan64 + c), v, p.voff)
+              : wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
+    for (int i = 0; i < nrv; i++) {
+      const float x = i < p.nr ? rebin_taps_sample(t, i, p.nch) : 0.0f;
+      const size_t row = (size_t)v * nrv + i;
+      split_f16(x, o, a_hi + row * kp + c, a_lo + row * kp + c);
+    }
+  }
+}
+
 cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale, float* view_scale,
                                float* op_scale, const float* d_beta, const float* d_bidx, const double2* d_chan64,
                                const RebinParams& p, int kp, int nrv, float taps_l1, cudaStream_t s, int vb, int ve) {
@@ -471,7 +643,24 @@ cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale,
   __half* hi = reinterpret_cast<__half*>(planes);
   __half* lo = hi + rows * kp;
   if (kp % 64 != 0) return cudaErrorInvalidValue;  // whole warps per channel run (the row maxima's reduction)
-  if (p.G == 1 && kp <= 4 * RS_THREADS)
+  if (use_vchunk_rebin(p)) {
+    cudaError_t e = cudaMemsetAsync(row_scale + (size_t)vb * nrv, 0, sizeof(float) * (size_t)(ve - vb) * nrv, s);
+    if (e != cudaSuccess) return e;
+    const dim3 g((unsigned)((kp + RV_CW - 1) / RV_CW), (unsigned)((ve - vb + RV_NY - 1) / RV_NY));
+    const size_t sm = sizeof(unsigned) * (size_t)RV_NY * nrv;
+    unsigned* rmax = reinterpret_cast<unsigned*>(row_scale);
+    if (d_chan64) {
+      k_rebin_vchunk<true, true><<<g, RV_CW, sm, s>>>(raw, nullptr, hi, lo, rmax, d_beta, d_bidx, d_chan64, p, kp,
+                                                       nrv, vb, ve);
+      k_rebin_split_scales<true><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
+          raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
+    } else {
+      k_rebin_vchunk<true, false><<<g, RV_CW, sm, s>>>(raw, nullptr, hi, lo, rmax, d_beta, d_bidx, nullptr, p,
+                                                        kp, nrv, vb, ve);
+      k_rebin_split_scales<false><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
+          raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, nullptr, p, kp, nrv, taps_l1, vb);
+    }
+  } else if (p.G == 1 && kp <= 4 * RS_THREADS)
     k_rebin_split_pairs<2><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
         raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   else if (p.G == 1)

@@ -26,32 +26,63 @@ struct RebinTaps {
   bool ok;     // false: the fan sample is outside the detector (bidx NaN), value 0
 };
 
-__device__ __forceinline__ RebinTaps rebin_taps(const float* __restrict__ raw, size_t view_stride, int V, int nr,
-                                                int nch, float bidx, float beta, int v, float dth, int q8, int voff) {
-  RebinTaps t;
+// The channel part of rebin_taps: the clamped raw channels of the two texel
+// columns, the channel weight and whether the fan sample lies on the detector.
+struct RebinTapsX {
+  int c0, c1;
+  float ax;
+  bool ok;
+};
+__device__ __forceinline__ RebinTapsX rebin_taps_x(int nch, float bidx, int q8) {
+  RebinTapsX t;
   t.ok = !isnan(bidx);
-  float theta = (float)(v + voff) * dth;
-  float alpha = theta - beta;
-  float aidx = alpha / dth;
   float xb = (bidx + 0.5f) - 0.5f;
-  float yb = (aidx + 0.5f) - 0.5f;
-  float fx = floorf(xb), fy = floorf(yb);
-  float ax = xb - fx, ay = yb - fy;
-  if (q8) {
-    ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
-    ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
-  }
-  int x0 = t.ok ? (int)fx : 0, y0 = (int)fy - voff;
-  int x1 = min(max(x0 + 1, 0), nch - 1), y1 = min(max(y0 + 1, 0), V - 1);
+  float fx = floorf(xb);
+  float ax = xb - fx;
+  if (q8) ax = rintf(ax * 256.0f) * (1.0f / 256.0f);
+  int x0 = t.ok ? (int)fx : 0;
+  int x1 = min(max(x0 + 1, 0), nch - 1);
   x0 = min(max(x0, 0), nch - 1);
-  y0 = min(max(y0, 0), V - 1);
-  const float* last = raw + (size_t)(nr - 1) * nch;
-  t.raw0 = last + (size_t)y0 * view_stride;
-  t.raw1 = last + (size_t)y1 * view_stride;
   t.c0 = nch - 1 - x0;
   t.c1 = nch - 1 - x1;
   t.ax = ax;
+  return t;
+}
+// The reading part: the clamped window-relative readings of the two texel
+// rows and the reading weight of output view v.
+struct RebinTapsY {
+  int y0, y1;
+  float ay;
+};
+__device__ __forceinline__ RebinTapsY rebin_taps_y(int V, float beta, int v, float dth, int q8, int voff) {
+  RebinTapsY t;
+  float theta = (float)(v + voff) * dth;
+  float alpha = theta - beta;
+  float aidx = alpha / dth;
+  float yb = (aidx + 0.5f) - 0.5f;
+  float fy = floorf(yb);
+  float ay = yb - fy;
+  if (q8) ay = rintf(ay * 256.0f) * (1.0f / 256.0f);
+  int y0 = (int)fy - voff;
+  t.y1 = min(max(y0 + 1, 0), V - 1);
+  t.y0 = min(max(y0, 0), V - 1);
   t.ay = ay;
+  return t;
+}
+
+__device__ __forceinline__ RebinTaps rebin_taps(const float* __restrict__ raw, size_t view_stride, int V, int nr,
+                                                int nch, float bidx, float beta, int v, float dth, int q8, int voff) {
+  const RebinTapsX x = rebin_taps_x(nch, bidx, q8);
+  const RebinTapsY y = rebin_taps_y(V, beta, v, dth, q8, voff);
+  RebinTaps t;
+  t.ok = x.ok;
+  const float* last = raw + (size_t)(nr - 1) * nch;
+  t.raw0 = last + (size_t)y.y0 * view_stride;
+  t.raw1 = last + (size_t)y.y1 * view_stride;
+  t.c0 = x.c0;
+  t.c1 = x.c1;
+  t.ax = x.ax;
+  t.ay = y.ay;
   return t;
 }
 
@@ -61,24 +92,47 @@ __device__ __forceinline__ RebinTaps rebin_taps(const float* __restrict__ raw, s
 // both fractional weights are formed in double (the FP64 oracle's
 // arithmetic, oracle/wfbp_oracle.c rb64_body) and only the weights rounded to
 // FP32. Exact weights (no 8-bit texture fractions).
-__device__ __forceinline__ RebinTaps rebin_taps64(const float* __restrict__ raw, size_t view_stride, int V, int nr,
-                                                  int nch, double2 ch, int v, int voff) {
-  RebinTaps t;
+__device__ __forceinline__ RebinTapsX rebin_taps64_x(int nch, double2 ch) {
+  RebinTapsX t;
   t.ok = !isnan(ch.x);
-  const double aidx = (double)(v + voff) - ch.y;
-  const double fx = t.ok ? floor(ch.x) : 0.0, fy = floor(aidx);
-  int x0 = (int)fx, y0 = (int)fy - voff;
-  int x1 = min(max(x0 + 1, 0), nch - 1), y1 = min(max(y0 + 1, 0), V - 1);
+  const double fx = t.ok ? floor(ch.x) : 0.0;
+  int x0 = (int)fx;
+  int x1 = min(max(x0 + 1, 0), nch - 1);
   x0 = min(max(x0, 0), nch - 1);
-  y0 = min(max(y0, 0), V - 1);
-  const float* last = raw + (size_t)(nr - 1) * nch;
-  t.raw0 = last + (size_t)y0 * view_stride;
-  t.raw1 = last + (size_t)y1 * view_stride;
   t.c0 = nch - 1 - x0;
   t.c1 = nch - 1 - x1;
   t.ax = t.ok ? (float)(ch.x - fx) : 0.0f;
+  return t;
+}
+__device__ __forceinline__ RebinTapsY rebin_taps64_y(int V, double2 ch, int v, int voff) {
+  RebinTapsY t;
+  const double aidx = (double)(v + voff) - ch.y;
+  const double fy = floor(aidx);
+  int y0 = (int)fy - voff;
+  t.y1 = min(max(y0 + 1, 0), V - 1);
+  t.y0 = min(max(y0, 0), V - 1);
   t.ay = (float)(aidx - fy);
   return t;
+}
+__device__ __forceinline__ RebinTaps rebin_taps64(const float* __restrict__ raw, size_t view_stride, int V, int nr,
+                                                  int nch, double2 ch, int v, int voff) {
+  const RebinTapsX x = rebin_taps64_x(nch, ch);
+  const RebinTapsY y = rebin_taps64_y(V, ch, v, voff);
+  RebinTaps t;
+  t.ok = x.ok;
+  const float* last = raw + (size_t)(nr - 1) * nch;
+  t.raw0 = last + (size_t)y.y0 * view_stride;
+  t.raw1 = last + (size_t)y.y1 * view_stride;
+  t.c0 = x.c0;
+  t.c1 = x.c1;
+  t.ax = x.ax;
+  t.ay = y.ay;
+  return t;
+}
+
+// The bilinear texel blend of rebin_kernel's linear texture filter.
+__device__ __forceinline__ float rebin_bilinear(float t00, float t10, float t01, float t11, float ax, float ay) {
+  return (1.0f - ax) * (1.0f - ay) * t00 + ax * (1.0f - ay) * t10 + (1.0f - ax) * ay * t01 + ax * ay * t11;
 }
 
 // The bilinear sample of sheet row i (raw row nr-1-i) at the taps.
@@ -86,10 +140,9 @@ __device__ __forceinline__ float rebin_taps_sample(const RebinTaps& t, int i, in
   if (!t.ok) return 0.0f;
   const float* r0 = t.raw0 - (size_t)i * nch;
   const float* r1 = t.raw1 - (size_t)i * nch;
-  const float ax = t.ax, ay = t.ay;
   float t00 = __ldg(r0 + t.c0), t10 = __ldg(r0 + t.c1);
   float t01 = __ldg(r1 + t.c0), t11 = __ldg(r1 + t.c1);
-  return (1.0f - ax) * (1.0f - ay) * t00 + ax * (1.0f - ay) * t10 + (1.0f - ax) * ay * t01 + ax * ay * t11;
+  return rebin_bilinear(t00, t10, t01, t11, t.ax, t.ay);
 }
 
 // Flying focal spot (no counterpart in the reference's WFBP): readings cycle

@@ -104,6 +104,10 @@ struct RebinParams {
   int voff;                  // index of the first view within the whole scan (wfbp_set_reading_offset / G)
 };
 
+// Chunk shape of the view-chunk rebin (k_rebin_vchunk): channels per CTA and
+// consecutive views per thread.
+constexpr int RV_CW = 128, RV_NY = 4;
+
 struct wfbp_ctx {
   CTGeometry cg;                    // geometry of the views the stages work on (effective one with FFS)
   CTGeometry cg_read;               // geometry of the raw readings (== cg without FFS)
