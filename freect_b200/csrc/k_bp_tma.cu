@@ -206,6 +206,7 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
   const BpSmem L = bp_smem_layout(bt, CPW);  // bt.zc == ZC (the launch picks the instantiation)
   uint8_t* slots = smem + L.slots;                            // [STAGES][nv_max][slot_bytes]
   int2* vinfo = reinterpret_cast<int2*>(smem + L.vinfo);      // [STAGES][nv_max] (view, first channel)
+  BpViewGeo* vgeo = reinterpret_cast<BpViewGeo*>(smem + L.vgeo);  // [STAGES][nv_max] the views' angle and z
   int* nvs = reinterpret_cast<int*>(smem + BT_OFF_NVS);       // [STAGES] views, [8] failure flag
   Geo* geo = reinterpret_cast<Geo*>(smem + L.geo);            // [warps][nv_max][NPW]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -290,10 +291,12 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
         const int j = t + k * p.P2;
         bool sel = false;
         int c_lo = 0;
+        float4 vf = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // FP32 form: the view's sin, cos, z for the records
         if (k < p.K) {
           const float zt = __ldg(view_z + j);
+          const float2 sc = __ldg(view_sc + j);
+          vf = make_float4(sc.x, sc.y, zt, 0.0f);
           if (!(zt < zlo || zt > zhi)) {
-            const float2 sc = __ldg(view_sc + j);
             const float p1 = xa * sc.x - ya * sc.y, p2 = xa * sc.x - yb * sc.y;
             const float p3 = xb * sc.x - ya * sc.y, p4 = xb * sc.x - yb * sc.y;
             const float pmax = fmaxf(fmaxf(p1, p2), fmaxf(p3, p4));
@@ -316,6 +319,18 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
         if (sel) {
           if (pos < bt.nv_max) {
             vinfo[s * bt.nv_max + pos] = make_int2(j, c_lo);
+            // the view's angle and z for the consumers' record pass (the
+            // mixed form's FP64 tables; the FP32 form's values of the test)
+            BpViewGeo* g = vgeo + s * bt.nv_max + pos;
+            if constexpr (HALF) {
+              const double2 sc64 = __ldg(p.sc64 + j);
+              const double z64 = __ldg(p.z64 + j);
+              g->s = sc64.x;
+              g->c = sc64.y;
+              g->z = z64;
+            } else {
+              *reinterpret_cast<float4*>(g) = vf;
+            }
           } else {
             atomicOr(err, WFBP_ERRBIT_BP_SLOTS);  // more views than slots: host sizing violated
           }
@@ -384,20 +399,23 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
     // geometry of (column gc, view v) for v = gv, gv + VPP, ...
     for (int v = gv; v < nv; v += VPP) {
       const int2 vi = vinfo[s * bt.nv_max + v];
+      const BpViewGeo& vg = vgeo[s * bt.nv_max + v];  // the view's angle and z, staged by the producer
       float p_hat, t_hat, zt;
       if constexpr (HALF) {
         // the mixed form's per-view geometry is FP64 (sin, cos and table
         // position of the view, from the FP64 tables of wfbp_set_views)
-        const double2 sc = __ldg(p.sc64 + vi.x);
+        const double2 sc = make_double2(vg.s, vg.c);
         const double gxd = (double)gx, gyd = (double)gy;
         p_hat = (float)fma(gxd, sc.x, -gyd * sc.y);
         t_hat = (float)fma(gxd, sc.y, gyd * sc.x);
-        zt = (float)__ldg(p.z64 + vi.x);
+        zt = (float)vg.z;
       } else {
-        const float2 sc = __ldg(view_sc + vi.x);
-        p_hat = gx * sc.x - gy * sc.y;
-        t_hat = gx * sc.y + gy * sc.x;
-        zt = __ldg(view_z + vi.x);
+        const float4 vf = *reinterpret_cast<const float4*>(&vg);
+        // x sin - y cos and x cos + y sin (cuda_kernels.cuh:235-238) with one
+        // rounding of the second product each, as the FP64 form's
+        p_hat = fmaf(gx, vf.x, -(gy * vf.y));
+        t_hat = fmaf(gx, vf.y, gy * vf.x);
+        zt = vf.z;
       }
       const float l_hat = bp_sqrt(p.R2 - p_hat * p_hat) - t_hat;
       const float A = p.zr2pi * bp_asin(p.rR * p_hat);
@@ -558,9 +576,19 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
   return p.P2;
 }
 
+// CTAs per SM the launch bounds of the one-tile kernel ask for: three 9-warp
+// CTAs of the FP16 pairs form (their registers, at most 75 per thread, and
+// shared memory fit; eight columns per pass over 32-slice slabs would spill at
+// that budget), two of the other 9-warp shapes, one of the wider ones. (The
+// persistent batch kernel keeps two: it holds more state per thread.)
+template <typename T, int NW, int CU, int SL>
+constexpr int bp_min_ctas() {
+  return NW > 8 ? 1 : (!std::is_same<T, float>::value && (CU == 4 || SL == 16)) ? 3 : 2;
+}
+
 // One tile per CTA: grid (tiles x, tiles y, SL-slice slabs).
 template <typename T, int CPW, int CU, int NW, int SL, bool ZC, bool COUNT>
-__global__ void __launch_bounds__((NW + 1) * 32, NW <= 8 ? 2 : 1)
+__global__ void __launch_bounds__((NW + 1) * 32, bp_min_ctas<T, NW, CU, SL>())
 k_bp_tma(const __grid_constant__ CUtensorMap map, float* __restrict__ vol, const float2* __restrict__ view_sc,
          const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, BPTile bt,
          unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {

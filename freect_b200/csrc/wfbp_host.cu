@@ -1507,6 +1507,11 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
   // each waits only for the views it reads (filtered on s).
   cudaEvent_t ev_done = ctx->ev_copy[kChunks + 1], ev_filt = ctx->ev_copy[kChunks + 2];
   int nlaunch = 0;
+  // Once the readings are all on the device most slabs become ready at
+  // once; a launch takes at most an eighth of them, so that the copy-back of
+  // each launch's slices overlaps the next launches and only the last
+  // launch's copy remains at the end.
+  const int max_run = std::max(1, (nslab + 7) / 8);
   auto launch_ready = [&](int filtered_upto) -> int {
     for (int sl = 0; sl < nslab;) {
       if (done[sl] || need[sl] >= filtered_upto) {
@@ -1514,7 +1519,7 @@ int run_host_pipelined(wfbp_ctx* ctx, const float* raw_host, float* vol_host, cu
         continue;
       }
       int e = sl;  // a run of ready slabs in one launch
-      while (e < nslab && !done[e] && need[e] < filtered_upto) e++;
+      while (e < nslab && e - sl < max_run && !done[e] && need[e] < filtered_upto) e++;
       BPTile bt = ctx->bpt;
       bt.zb0 = sl;
       bt.nzb = e - sl;

@@ -69,7 +69,13 @@ constexpr int BT_FUSE_WORDS = 384;  // shared-memory words for one slab's fused-
 constexpr int BP_GEO_BYTES_ZCULL = 48;  // column-pair record with the row range of the table-position cull
 constexpr int BP_GEO_BYTES = 32;        // column-pair record when that cull never binds
 struct BpSmem {
-  unsigned slots, vinfo, geo, fuse, total;
+  unsigned slots, vinfo, vgeo, geo, fuse, total;
+};
+// Per staged view, the geometry the consumers' record pass reads (copied by
+// the producer lane that selects the view): sin and cos of the tube angle and
+// the table position, FP64 (mixed form) or FP32 (the first three floats).
+struct __align__(16) BpViewGeo {
+  double s, c, z, pad;
 };
 // Bytes 0..127 hold the ring's mbarriers and a few words (fixed across the
 // tiles of a persistent launch); the per-scan regions follow.
@@ -81,6 +87,8 @@ __host__ __device__ inline BpSmem bp_smem_layout(const BPTile& bt, int cpw) {
   L.vinfo = o;
   o += (unsigned)(BT_STAGES * bt.nv_max * 8);
   o = (o + 15u) & ~15u;
+  L.vgeo = o;
+  o += (unsigned)(BT_STAGES * bt.nv_max * sizeof(BpViewGeo));
   L.geo = o;
   o += (unsigned)(bt.nw * bt.nv_max * (cpw / 2) * (bt.zc ? BP_GEO_BYTES_ZCULL : BP_GEO_BYTES));  // column-pair records
   L.fuse = o;
