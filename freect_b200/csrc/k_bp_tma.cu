@@ -577,21 +577,19 @@ __device__ __forceinline__ int bp_tile(const CUtensorMap* map, float* __restrict
 }
 
 // CTAs per SM the launch bounds of the one-tile kernel ask for: three 9-warp
-// CTAs of the FP16 pairs form (their registers, at most 75 per thread, and
-// shared memory fit; eight columns per pass over 32-slice slabs would spill at
-// that budget), two of the other 9-warp shapes, one of the wider ones. (The
-// persistent batch kernel holds more state per thread: three only for four
-// columns per pass over 16-slice slabs.)
-template <typename T, int NW, int CU, int SL, bool BATCH = false>
+// CTAs (their registers, at most 75 per thread, and shared memory fit) for
+// four columns per pass or 16-slice slabs, in both forms; eight columns per
+// pass over 32-slice slabs would spill at that budget and keep two; the wider
+// shapes one. (The persistent batch kernel holds more state per thread:
+// three only for four columns per pass over 16-slice slabs.)
+template <int NW, int CU, int SL, bool BATCH = false>
 constexpr int bp_min_ctas() {
-  return NW > 8 ? 1
-                : (!std::is_same<T, float>::value && (BATCH ? (CU == 4 && SL == 16) : (CU == 4 || SL == 16))) ? 3
-                                                                                                              : 2;
+  return NW > 8 ? 1 : (BATCH ? (CU == 4 && SL == 16) : (CU == 4 || SL == 16)) ? 3 : 2;
 }
 
 // One tile per CTA: grid (tiles x, tiles y, SL-slice slabs).
 template <typename T, int CPW, int CU, int NW, int SL, bool ZC, bool COUNT>
-__global__ void __launch_bounds__((NW + 1) * 32, bp_min_ctas<T, NW, CU, SL>())
+__global__ void __launch_bounds__((NW + 1) * 32, bp_min_ctas<NW, CU, SL>())
 k_bp_tma(const __grid_constant__ CUtensorMap map, float* __restrict__ vol, const float2* __restrict__ view_sc,
          const float* __restrict__ view_z, const float* __restrict__ zslices, BPParams p, BPTile bt,
          unsigned long long* __restrict__ count, int* __restrict__ err, ThickFuse tf) {
@@ -607,7 +605,7 @@ k_bp_tma(const __grid_constant__ CUtensorMap map, float* __restrict__ vol, const
 // the next work item (scan, tile x, tile y, slab) from a global counter until
 // the list is exhausted. Items are listed by decreasing estimated cost.
 template <typename T, int CPW, int CU, int NW, int SL, bool ZC>
-__global__ void __launch_bounds__((NW + 1) * 32, bp_min_ctas<T, NW, CU, SL, true>())
+__global__ void __launch_bounds__((NW + 1) * 32, bp_min_ctas<NW, CU, SL, true>())
 k_bp_tma_batch(const BpScan* __restrict__ scans, const int4* __restrict__ items, int n_items,
                unsigned* __restrict__ next, int* __restrict__ err) {
   extern __shared__ __align__(128) uint8_t smem[];
