@@ -82,7 +82,8 @@ k_rebin_f32_rows(const float* __restrict__ raw, float* __restrict__ out, const f
 
 namespace {
 // The view-chunk kernels serve scans without a flying focal spot whose raw
-// frames fit 31-bit element offsets.
+// frames fit 31-bit element offsets; longer ones (over 2^31 samples) take
+// the per-view kernels k_rebin_f32_rows / k_rebin_split_rows.
 bool use_vchunk_rebin(const RebinParams& p) { return p.G == 1 && (long long)p.V * p.nr * p.nch < (1ll << 31); }
 }  // namespace
 
@@ -389,97 +390,6 @@ k_rebin_split_rows(const float* __restrict__ raw, __half* __restrict__ a_hi, __h
   }
 }
 
-// Without a flying focal spot the same samples with more work per thread:
-// thread t owns the channel pairs t + k * RS_THREADS (k < NP) of the view,
-// keeps their taps in registers and walks the rows two at a time with all its
-// samples' loads (NP x 2 channels x 2 rows x 4 texels) issued before their
-// use; each row's two channels go out as one 4-byte FP16x2 word per plane,
-// and the row maximum takes one warp reduction per row (over the thread's
-// channels first). Same sample arithmetic, planes and scales bit for bit.
-template <int NP>
-__global__ void __launch_bounds__(RS_THREADS)
-k_rebin_split_pairs(const float* __restrict__ raw, __half* __restrict__ a_hi, __half* __restrict__ a_lo,
-                    float* __restrict__ row_scale, float* __restrict__ view_scale, float* __restrict__ op_scale,
-                    const float* __restrict__ beta_t, const float* __restrict__ bidx_t,
-                    const double2* __restrict__ chan64, RebinParams p, int kp, int nrv, float taps_l1, int vb) {
-  extern __shared__ float s_rowmax[];  // [nrv]
-  const int v = vb + blockIdx.x;
-  const int lane = threadIdx.x % 32;
-  for (int i = threadIdx.x; i < nrv; i += blockDim.x) s_rowmax[i] = 0.0f;
-  RebinTaps t[NP][2];
-  bool pv[NP];  // the pair lies inside [0, kp)
-#pragma unroll
-  for (int k = 0; k < NP; k++) {
-    const int c0 = 2 * ((int)threadIdx.x + k * RS_THREADS);
-    pv[k] = c0 < kp;
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int c = c0 + h;
-      t[k][h].ok = false;
-      t[k][h].raw0 = t[k][h].raw1 = raw;
-      t[k][h].c0 = t[k][h].c1 = 0;
-      t[k][h].ax = t[k][h].ay = 0.0f;
-      if (c < p.nch) {
-        if (chan64) t[k][h] = rebin_taps64(raw, (size_t)p.nr * p.nch, p.V, p.nr, p.nch, __ldg(chan64 + c), v, p.voff);
-        else t[k][h] = wfbp_rebin_taps(raw, p, __ldg(bidx_t + c), __ldg(beta_t + c), v);
-      }
-    }
-  }
-  __syncthreads();
-  for (int pass = 0; pass < 2; pass++) {
-    // pass 0: the planes with o = 1 and the row maxima; pass 1 (only a view
-    // whose largest sample exceeds 16384): the planes again with o < 1
-    float o = 1.0f;
-    if (pass == 1) {
-      o = split_view_scales(s_rowmax, nrv, v, taps_l1, row_scale, view_scale, op_scale);
-      if (o == 1.0f) break;  // block-uniform
-    }
-    for (int i0 = 0; i0 < nrv; i0 += 2) {
-      float x[NP][2][2];  // [pair][row][channel]
-#pragma unroll
-      for (int k = 0; k < NP; k++)
-#pragma unroll
-        for (int u = 0; u < 2; u++)
-#pragma unroll
-          for (int h = 0; h < 2; h++)
-            x[k][u][h] = i0 + u >= p.nr ? 0.0f  // 0 off the detector and in the padding
-                                        : rebin_taps_sample(t[k][h], i0 + u, p.nch);
-#pragma unroll
-      for (int u = 0; u < 2; u++) {
-        const int i = i0 + u;
-        if (i >= nrv) break;  // warp-uniform
-        const size_t row = (size_t)v * nrv + i;
-        if (pass == 0) {
-          float m = 0.0f;
-#pragma unroll
-          for (int k = 0; k < NP; k++) {
-            if (!pv[k]) continue;
-            // fmaxf semantics: a NaN sample does not raise the maximum
-            m = fmaxf(m, fmaxf(isnan(x[k][u][0]) ? 0.0f : fabsf(x[k][u][0]),
-                               isnan(x[k][u][1]) ? 0.0f : fabsf(x[k][u][1])));
-          }
-          const unsigned mm = __reduce_max_sync(0xffffffffu, __float_as_uint(m));  // m >= 0: bits order as values
-          if (lane == 0 && mm) atomicMax(reinterpret_cast<int*>(&s_rowmax[i]), (int)mm);
-        }
-        {
-#pragma unroll
-          for (int k = 0; k < NP; k++) {
-            if (!pv[k]) continue;
-            const int c0 = 2 * ((int)threadIdx.x + k * RS_THREADS);
-            const float y0 = x[k][u][0] * o, y1 = x[k][u][1] * o;  // o: a power of two, exact
-            const __half2 hi = __floats2half2_rn(y0, y1);
-            const float2 hf = __half22float2(hi);
-            const __half2 lo = __floats2half2_rn(y0 - hf.x, y1 - hf.y);
-            *reinterpret_cast<__half2*>(a_hi + row * kp + c0) = hi;
-            *reinterpret_cast<__half2*>(a_lo + row * kp + c0) = lo;
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // ---------------------------------------------------------------------------
 // view-chunk rebin (no flying focal spot)
 // ---------------------------------------------------------------------------
@@ -660,10 +570,7 @@ cudaError_t launch_rebin_split(const float* raw, void* planes, float* row_scale,
       k_rebin_split_scales<false><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
           raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, nullptr, p, kp, nrv, taps_l1, vb);
     }
-  } else if (p.G == 1 && kp <= 4 * RS_THREADS)
-    k_rebin_split_pairs<2><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
-        raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
-  else if (p.G == 1)
+  } else if (p.G == 1)
     k_rebin_split_rows<false><<<(unsigned)(ve - vb), RS_THREADS, sizeof(float) * nrv, s>>>(
         raw, hi, lo, row_scale, view_scale, op_scale, d_beta, d_bidx, d_chan64, p, kp, nrv, taps_l1, vb);
   else
