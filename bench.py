@@ -47,11 +47,13 @@ DRAM_BYTES_PER_UPDATE = {("fp32", 32): 14.42e9 / _SHORT_UPDATES,
                          ("fp32", 16): 21.08e9 / _SHORT_UPDATES,
                          ("mixed", 32): 13.18e9 / _SHORT_UPDATES,
                          ("mixed", "16x8/4w8s16"): 34.96e9 / _SHORT_UPDATES,
-                         ("fp32", "16x8/8w8s32"): 15.38e9 / _SHORT_UPDATES}
+                         ("fp32", "16x8/8w8s32"): 15.38e9 / _SHORT_UPDATES,
+                         ("fp32", "8x16/8w8s16"): 22.55e9 / _SHORT_UPDATES}
 WARP_INST_PER_UPDATE = {("fp32", 32): 3.537e10 / _SHORT_UPDATES, ("mixed", 16): 3.428e10 / _SHORT_UPDATES,
                         ("fp32", 16): 3.475e10 / _SHORT_UPDATES, ("mixed", 32): 3.631e10 / _SHORT_UPDATES,
                         ("mixed", "16x8/4w8s16"): 3.6336e10 / _SHORT_UPDATES,
-                        ("fp32", "16x8/8w8s32"): 3.4076e10 / _SHORT_UPDATES}
+                        ("fp32", "16x8/8w8s32"): 3.4076e10 / _SHORT_UPDATES,
+                        ("fp32", "8x16/8w8s16"): 3.4219e10 / _SHORT_UPDATES}
 SMS, SCHEDULERS_PER_SM = 148, 4
 UNIT = "voxel-view updates/s"
 
