@@ -153,20 +153,24 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
     const float nxm = 0.5f * ((float)p.nx - 1.0f), nym = 0.5f * ((float)p.ny - 1.0f);
     const bool along_y = fabsf(sc.x) >= fabsf(sc.y);  // p_hat = x sin - y cos: solve for x per row y
     const int n_outer = along_y ? p.ny : p.nx;
+    // the candidate range of each row through reciprocals computed once: their
+    // rounding (a few 1e-5 mm) stays far inside the margin, and the exact
+    // channel test below decides which voxels the thread owns
+    const float r_sc = 1.0f / (along_y ? sc.x : sc.y), r_sx = 1.0f / sx, r_sy = 1.0f / sy;
     for (int o = 0; o < n_outer; o++) {
       int i_lo, i_hi;
       if (along_y) {
         const float y = ycoord(p, o);
-        float xa = (plo + y * sc.y) / sc.x, xb = (phi + y * sc.y) / sc.x;
+        float xa = (plo + y * sc.y) * r_sc, xb = (phi + y * sc.y) * r_sc;
         if (xa > xb) { const float tt = xa; xa = xb; xb = tt; }
-        i_lo = max(0, (int)floorf((xa - p.x0) / sx + nxm));
-        i_hi = min(p.nx - 1, (int)ceilf((xb - p.x0) / sx + nxm));
+        i_lo = max(0, (int)floorf((xa - p.x0) * r_sx + nxm));
+        i_hi = min(p.nx - 1, (int)ceilf((xb - p.x0) * r_sx + nxm));
       } else {
         const float x = xcoord(p, o);
-        float ya = (x * sc.x - phi) / sc.y, yb = (x * sc.x - plo) / sc.y;
+        float ya = (x * sc.x - phi) * r_sc, yb = (x * sc.x - plo) * r_sc;
         if (ya > yb) { const float tt = ya; ya = yb; yb = tt; }
-        i_lo = max(0, (int)floorf((ya - p.y0) / sy + nym));
-        i_hi = min(p.ny - 1, (int)ceilf((yb - p.y0) / sy + nym));
+        i_lo = max(0, (int)floorf((ya - p.y0) * r_sy + nym));
+        i_hi = min(p.ny - 1, (int)ceilf((yb - p.y0) * r_sy + nym));
       }
       for (int in = i_lo; in <= i_hi; in++) {
         const int ix = along_y ? in : o, iy = along_y ? o : in;
