@@ -10,6 +10,7 @@
 
 #include <math.h>
 
+#include "bp_math.cuh"
 #include "rebin_sample.cuh"
 
 namespace {
@@ -50,7 +51,7 @@ __device__ __forceinline__ float ycoord(const BPParams& p, int iy) {
 }
 
 struct ViewGeo {
-  float zt, A, inv, p_idx;
+  float zt, A, lt, inv, p_idx;  // lt = l_hat tan(cone), inv = 1 / lt
   bool valid_p;
 };
 
@@ -58,9 +59,12 @@ __device__ __forceinline__ ViewGeo view_geo(const BPParams& p, float x, float y,
   ViewGeo g;
   g.zt = zt;
   const float p_hat = x * sc.x - y * sc.y;
-  const float l_hat = sqrtf(p.R2 - p_hat * p_hat) - x * sc.y - y * sc.x;
-  g.A = p.zr2pi * asinf(p.rR * p_hat);
-  g.inv = 1.0f / (l_hat * p.tanc);
+  // the forward's short forms (bp_math.cuh): hardware square root and
+  // reciprocal, arcsine from its series
+  const float l_hat = bp_sqrt(p.R2 - p_hat * p_hat) - x * sc.y - y * sc.x;
+  g.A = p.zr2pi * bp_asin(p.rR * p_hat);
+  g.lt = l_hat * p.tanc;
+  g.inv = bp_rcp(g.lt);
   g.p_idx = p.kp - (p_hat * p.ps + p.c0);
   const float pf = floorf(g.p_idx);
   g.valid_p = pf >= 0.0f && ceilf(g.p_idx) <= p.ncm2;
@@ -189,7 +193,7 @@ k_bp_adjoint(const float* __restrict__ gvol, const float* __restrict__ G, float*
         const float h0 = 1.0f - wp;  // channel c; channel c + 1 gets wp
         // slices that can pass this view's tests: |z - zt| <= z_rot and
         // q_idx in [0, nr-2], a z interval around zt - A
-        const float za = zt - g.A - 1.0f / g.inv, zb = zt - g.A + (p.nrm2 / p.hn - 1.0f) / g.inv;
+        const float za = zt - g.A - g.lt, zb = zt - g.A + (p.nrm2 / p.hn - 1.0f) * g.lt;
         const float zlo = fmaxf(fminf(za, zb), zt - p.z_rot), zhi = fminf(fmaxf(za, zb), zt + p.z_rot);
         if (zlo > zhi) continue;
         int s_lo, s_hi;
