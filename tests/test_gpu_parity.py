@@ -4,7 +4,8 @@ against the oracle on the same seeded inputs.
 Tolerances: stages are compared elementwise relative to the data's scale
 (FP32 arithmetic in a different order); volumes in HU (1 HU = 1.9e-5 /mm):
 the FP32 form must stay within 0.5 HU RMS / 2 HU max of the reference
-transcript (the north-star parity gate).
+transcript (the parity gate of the FP32 form against the reference's
+algorithm).
 """
 import numpy as np
 import pytest
